@@ -1,0 +1,143 @@
+"""Python handle on the LST reference CPU backend built in oracle/_ref/.
+
+Test infrastructure only (parity checks, golden fixtures, the reference arm of
+bench.py).  ``RefLST(variant)`` loads ``oracle/_ref/liblstref_<variant>.so``
+(see oracle/ref/Makefile for the variants), ``run_event`` feeds one event
+through ``SDL::Event`` in the order bin/sdl.cc:451-458 calls the stages, and
+``field`` returns any internal array of the event as a numpy view.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+STAGES = {
+    "md": 1,
+    "ls": 2,
+    "t3": 3,
+    "t5": 4,
+    "pls_clean": 5,
+    "pt5": 6,
+    "pt3": 7,
+    "tc": 8,
+}
+STAGE_ORDER = ("md", "ls", "t3", "t5", "pls_clean", "pt5", "pt3", "tc")
+
+_INT_DTYPES = {1: np.int8, 2: np.uint16, 4: np.uint32, 8: np.uint64}
+
+
+def library_path(variant: str = "cr") -> str:
+    return os.path.join(REF_DIR, f"liblstref_{variant}.so")
+
+
+def available(variant: str = "cr") -> bool:
+    return os.path.exists(library_path(variant))
+
+
+class RefLST:
+    """One loaded reference library plus its event setup."""
+
+    def __init__(self, variant: str = "cr", es_base: str | None = None):
+        from tracklooper_b200 import geometry
+
+        path = library_path(variant)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference library not built: {path}")
+        lib = ctypes.CDLL(path)
+        vp = ctypes.c_void_p
+        lib.lstref_es_load.restype = vp
+        lib.lstref_es_load.argtypes = [ctypes.c_char_p]
+        lib.lstref_es_free.argtypes = [vp]
+        lib.lstref_es_counts.restype = ctypes.c_uint
+        lib.lstref_es_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
+        lib.lstref_event_create.restype = vp
+        lib.lstref_event_create.argtypes = [vp]
+        lib.lstref_event_destroy.argtypes = [vp]
+        lib.lstref_event_reset.argtypes = [vp]
+        lib.lstref_event_add_hits.argtypes = [vp, ctypes.c_uint] + [vp] * 5
+        lib.lstref_event_add_pixel_segments.argtypes = [vp, ctypes.c_uint] + [vp] * 18
+        lib.lstref_event_run_stage.restype = ctypes.c_int
+        lib.lstref_event_run_stage.argtypes = [vp, ctypes.c_int]
+        lib.lstref_event_field.restype = vp
+        lib.lstref_event_field.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
+        self.lib = lib
+        geometry.geometry_dir()
+        self.es = lib.lstref_es_load((es_base or geometry.ES_BASE).encode())
+        if not self.es:
+            raise RuntimeError("reference failed to load the event setup")
+        nm, nl = ctypes.c_uint(), ctypes.c_uint()
+        self.n_pixels = lib.lstref_es_counts(self.es, ctypes.byref(nm), ctypes.byref(nl))
+        self.n_modules, self.n_lower = nm.value, nl.value
+        self.ev = lib.lstref_event_create(self.es)
+
+    def close(self):
+        if self.ev:
+            self.lib.lstref_event_destroy(self.ev)
+            self.ev = None
+        if self.es:
+            self.lib.lstref_es_free(self.es)
+            self.es = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ event
+    def reset(self):
+        self.lib.lstref_event_reset(self.ev)
+
+    def add_inputs(self, inp):
+        keep = []
+
+        def p(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a.ctypes.data
+
+        self.lib.lstref_event_add_hits(
+            self.ev,
+            inp.n_hits,
+            p(inp.x, np.float32),
+            p(inp.y, np.float32),
+            p(inp.z, np.float32),
+            p(inp.detId, np.uint32),
+            p(inp.idxInNtuple, np.uint32),
+        )
+        from tracklooper_b200.gen import PLS_FIELDS
+
+        self.lib.lstref_event_add_pixel_segments(
+            self.ev, inp.n_pls, *[p(inp.pls[name], dt) for name, dt in PLS_FIELDS]
+        )
+
+    def run_stage(self, stage: str):
+        rc = self.lib.lstref_event_run_stage(self.ev, STAGES[stage])
+        if rc != 0:
+            raise RuntimeError(f"unknown stage {stage}")
+
+    def run_event(self, inp, upto: str = "tc"):
+        self.reset()
+        self.add_inputs(inp)
+        for st in STAGE_ORDER:
+            self.run_stage(st)
+            if st == upto:
+                break
+
+    def field(self, name: str, dtype=None, copy: bool = True) -> np.ndarray | None:
+        n, sz = ctypes.c_longlong(), ctypes.c_int()
+        ptr = self.lib.lstref_event_field(self.ev, name.encode(), ctypes.byref(n), ctypes.byref(sz))
+        if not ptr:
+            return None
+        if dtype is None:
+            dtype = _INT_DTYPES[sz.value]
+        dtype = np.dtype(dtype)
+        count = n.value * sz.value // dtype.itemsize
+        buf = (ctypes.c_char * (n.value * sz.value)).from_address(ptr)
+        arr = np.frombuffer(buf, dtype=dtype, count=count)
+        return arr.copy() if copy else arr
