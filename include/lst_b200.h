@@ -1,0 +1,217 @@
+/* C ABI of the B200 LST object-building chain (hits -> mini-doublets ->
+ * line segments -> triplets -> quintuplets -> pixel triplets/quintuplets ->
+ * track candidates).
+ *
+ * The reference exposes this path only as C++ classes templated on Alpaka
+ * types: SDL::Event<Acc> (SDL/Event.h:31-205, SDL/Event.cc) and the
+ * event-setup loaders (SDL/LSTESData.h:79-80).  Each entry point below states
+ * the reference member it replaces.  Conventions:
+ *   - every function returns an int status: 0 = ok, < 0 = error (the message
+ *     is available from lst_last_error()), > 0 = the event's status bits
+ *     (LST_STATUS_*) where a function reports them;
+ *   - no C++ exceptions cross this boundary;
+ *   - a handle is used by one host thread at a time; an event set owns its
+ *     CUDA stream (or borrows the caller's) and all its device memory;
+ *   - an event setup (lst_es) is read-only once loaded and may be shared by
+ *     any number of event sets on the same device.
+ *
+ * Event sets hold N event slots.  The per-event calls take a slot index and
+ * behave as the matching SDL::Event member on that event.  The batched calls
+ * (lst_batch_*) run a stage for slots [first, first + count) in one launch per
+ * kernel.
+ */
+#ifndef LST_B200_H
+#define LST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lst_es lst_es;
+typedef struct lst_event lst_event;
+
+/* Status bits an event can report (returned by stage calls and in counts). */
+#define LST_STATUS_UNKNOWN_DETID 0x1u        /* a hit's detId is not in the geometry */
+#define LST_STATUS_UNKNOWN_ENDCAP_DETID 0x2u /* 2S endcap hit without strip orientation */
+#define LST_STATUS_HIT_CAPACITY 0x4u         /* more hits than the slot holds: event rejected */
+#define LST_STATUS_PLS_TRUNCATED 0x8u        /* more than 50000 pLS: the rest dropped (as the reference) */
+#define LST_STATUS_TC_TRUNCATED 0x10u        /* a track-candidate cap was reached (as the reference) */
+#define LST_STATUS_CAP_OVERFLOW 0x20u        /* an occupancy cap dropped objects (as the reference) */
+#define LST_STATUS_INVALID_INPUT 0x40u       /* a pLS hit index >= nHits (replaced by hit 0), or pLS without hits */
+
+/* Stage identifiers for lst_batch_run / lst_event_run_stage. */
+enum lst_stage {
+  LST_STAGE_MINI_DOUBLETS = 1,     /* Event::createMiniDoublets            SDL/Event.cc:393 */
+  LST_STAGE_SEGMENTS = 2,          /* Event::createSegmentsWithModuleMap   SDL/Event.cc:469 */
+  LST_STAGE_TRIPLETS = 3,          /* Event::createTriplets                SDL/Event.cc:512 */
+  LST_STAGE_QUINTUPLETS = 4,       /* Event::createQuintuplets             SDL/Event.cc:903 */
+  LST_STAGE_PLS_CLEANING = 5,      /* Event::pixelLineSegmentCleaning      SDL/Event.cc:993 */
+  LST_STAGE_PIXEL_QUINTUPLETS = 6, /* Event::createPixelQuintuplets        SDL/Event.cc:1009 */
+  LST_STAGE_PIXEL_TRIPLETS = 7,    /* Event::createPixelTriplets           SDL/Event.cc:784 */
+  LST_STAGE_TRACK_CANDIDATES = 8   /* Event::createTrackCandidates         SDL/Event.cc:620 */
+};
+
+/* T5 selection method used by LST_STAGE_QUINTUPLETS. */
+enum lst_t5_method {
+  LST_T5_DNN = 0,     /* reference default: rz chi2 + DNN (USE_RZCHI2, USE_T5_DNN) */
+  LST_T5_CUTS = 1     /* cut-only: rz chi2 + r-phi chi2 (USE_RZCHI2, USE_RPHICHI2) */
+};
+
+/* Object counts of one event (SDL/Event.cc:1263-1487 getNumberOf*). */
+typedef struct lst_counts {
+  uint32_t nHits;
+  uint32_t nPixelSegments;
+  uint32_t status;
+  uint32_t nMiniDoublets;     /* summed over lower modules, as getNumberOfMiniDoublets */
+  uint32_t nSegments;         /* as getNumberOfSegments */
+  uint32_t nTriplets;         /* as getNumberOfTriplets */
+  uint32_t nQuintuplets;      /* as getNumberOfQuintuplets */
+  uint32_t nPixelTriplets;    /* as getNumberOfPixelTriplets (stored, <= 5000) */
+  uint32_t nPixelQuintuplets; /* as getNumberOfPixelQuintuplets (stored, <= 15000) */
+  uint32_t nTrackCandidates;
+  uint32_t nTrackCandidatesPT5;
+  uint32_t nTrackCandidatesPT3;
+  uint32_t nTrackCandidatesPLS;
+  uint32_t nTrackCandidatesT5;
+  uint32_t nPixelTripletsFound;    /* before the 5000 cap */
+  uint32_t nPixelQuintupletsFound; /* before the 15000 cap */
+  uint32_t mdBarrel[6], mdEndcap[5]; /* getNumberOfMiniDoubletsByLayer{Barrel,Endcap} */
+  uint32_t lsBarrel[6], lsEndcap[5]; /* getNumberOfSegmentsByLayer{Barrel,Endcap} */
+  uint32_t t3Barrel[6], t3Endcap[5]; /* getNumberOfTripletsByLayer{Barrel,Endcap} */
+  uint32_t t5Barrel[6], t5Endcap[5]; /* getNumberOfQuintupletsByLayer{Barrel,Endcap} */
+  uint32_t reserved[4];
+} lst_counts;
+
+/* Static sizes of an event setup. */
+typedef struct lst_es_info {
+  uint32_t nModules;
+  uint32_t nLowerModules;
+  uint32_t pixelModule;
+  uint32_t nConnectedPixels;
+  uint32_t nTotalMDs;      /* MD arena length per event (incl. 100000 pixel MDs) */
+  uint32_t nTotalSegments; /* LS arena length per event (incl. 50000 pLS) */
+  uint32_t maxTriplets;    /* T3 arena length per event */
+  uint32_t maxQuintuplets; /* T5 arena length per event */
+} lst_es_info;
+
+/* Last error message of the calling thread (empty if none). */
+const char* lst_last_error(void);
+
+/* ------------------------------------------------------------------ ES */
+/* Loads the geometry directory (the OT800_IT615_pt0.8 layout: sensor
+ * centroids, module connection map, pixel maps, endcap and tilted-barrel
+ * orientation) and uploads it to `device`, with the T5 DNN weights from
+ * `t5dnn_weights_path` (2337 little-endian float32: w0[38][32], b0[32],
+ * w2[32][32], b2[32], w4[32], b4[1]; NULL disables the DNN method).
+ * Replaces SDL::loadAndFillESHost + SDL::loadAndFillESDevice
+ * (SDL/LSTESData.h:79-80, SDL/LSTESData.cc:79-126). */
+int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out);
+void lst_es_free(lst_es* es);
+int lst_es_get_info(const lst_es* es, lst_es_info* out);
+/* Replaces the T5 DNN weights (same layout as the file).  The weights live
+ * in constant memory of the ES's device and are shared by every event set on
+ * that device; call between events. */
+int lst_es_set_t5dnn_weights(lst_es* es, const float* weights, size_t n);
+
+/* --------------------------------------------------------------- events */
+/* Creates an event set of `n_slots` events holding at most `max_hits` hits
+ * each, on the ES's device.  `stream` is a cudaStream_t to run on (NULL: the
+ * set creates its own non-blocking stream).  All device memory is allocated
+ * here, once.  Replaces the constructor SDL::Event(bool, Queue, ESDeviceData*)
+ * (SDL/Event.h:100-111), whose arenas are allocated per event. */
+int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, lst_event** out);
+void lst_event_destroy(lst_event* ev);
+/* Device memory held by the set, in bytes. */
+int lst_event_memory(const lst_event* ev, size_t* bytes);
+/* Synchronises the set's stream. */
+int lst_event_sync(lst_event* ev);
+/* The CUDA stream the set runs on (a cudaStream_t). */
+void* lst_event_stream(lst_event* ev);
+/* Selects the T5 method (default LST_T5_DNN when weights were loaded). */
+int lst_event_set_t5_method(lst_event* ev, int method);
+
+/* Event::resetEvent (SDL/Event.cc:45): clears slot `slot`'s objects.  Adding
+ * hits resets the slot as well. */
+int lst_event_reset(lst_event* ev, int slot);
+
+/* Event::addHitToEvent (SDL/Event.cc:151): resets the slot, copies the hits
+ * (host or device pointers) and runs the hit preparation and module-range
+ * kernels.  Returns LST_STATUS_HIT_CAPACITY (>0) without touching the slot if
+ * n > max_hits. */
+int lst_event_add_hits(lst_event* ev, int slot, uint32_t n, const float* x, const float* y, const float* z,
+                       const uint32_t* detId, const uint32_t* idxInNtuple);
+
+/* Event::addPixelSegmentToEvent (SDL/Event.cc:217; argument order of
+ * SDL/Event.h:120-137): copies the pixel line segments and builds their
+ * mini-doublets and segment records.  More than 50000 segments are truncated
+ * as in the reference (LST_STATUS_PLS_TRUNCATED). */
+int lst_event_add_pixel_segments(lst_event* ev, int slot, uint32_t n, const uint32_t* hitIndices0,
+                                 const uint32_t* hitIndices1, const uint32_t* hitIndices2,
+                                 const uint32_t* hitIndices3, const float* dPhiChange, const float* ptIn,
+                                 const float* ptErr, const float* px, const float* py, const float* pz,
+                                 const float* eta, const float* etaErr, const float* phi, const int32_t* charge,
+                                 const uint32_t* seedIdx, const int32_t* superbin, const int8_t* pixelType,
+                                 const int8_t* isQuad);
+
+/* Runs one stage (enum lst_stage) on one slot (the Event::create* members). */
+int lst_event_run_stage(lst_event* ev, int slot, int stage);
+int lst_event_create_mini_doublets(lst_event* ev, int slot);
+int lst_event_create_segments(lst_event* ev, int slot);
+int lst_event_create_triplets(lst_event* ev, int slot);
+int lst_event_create_quintuplets(lst_event* ev, int slot);
+int lst_event_pixel_line_segment_cleaning(lst_event* ev, int slot);
+int lst_event_create_pixel_quintuplets(lst_event* ev, int slot);
+int lst_event_create_pixel_triplets(lst_event* ev, int slot);
+int lst_event_create_track_candidates(lst_event* ev, int slot);
+
+/* Copies the counts of one slot to the host (synchronises the stream).
+ * Returns the slot's status bits. */
+int lst_event_get_counts(lst_event* ev, int slot, lst_counts* out);
+
+/* Copies one object-store field of a slot to host memory `dst` (synchronises
+ * the stream).  `name` is "<store>.<field>" with the reference's store and
+ * field names (hits.xs, md.anchorHitIndices, ls.mdIndices, t3.hitIndices,
+ * t5.score_rphisum, pt3.hitIndices, pt5.T5Indices, tc.hitIndices,
+ * ranges.quintupletModuleIndices, ...).  The full array (its arena length)
+ * is described by *n_elems and *elem_size; min(n_elems, capacity) elements
+ * are copied.  dst may be NULL to query the length.  Replaces the getters
+ * getHits() ... getTrackCandidates() (SDL/Event.cc:1489-1805). */
+int lst_event_get_field(lst_event* ev, int slot, const char* name, void* dst, size_t capacity, size_t* n_elems,
+                        size_t* elem_size);
+/* Device address of a field of a slot (for zero-copy consumers). */
+int lst_event_field_device_ptr(lst_event* ev, int slot, const char* name, void** dptr, size_t* n_elems,
+                               size_t* elem_size);
+/* Number of fields, the i-th name, and its element type: *elem_size bytes of
+ * kind 'f' (IEEE float), 'i' (signed integer) or 'u' (unsigned integer). */
+int lst_field_count(void);
+const char* lst_field_name(int i);
+int lst_field_info(int i, const char** name, size_t* elem_size, char* kind);
+
+/* --------------------------------------------------------------- batches */
+/* Packed per-event input, one contiguous little-endian blob per event:
+ *   uint32 nHits, uint32 nPLS, uint32 reserved[2],
+ *   float x[nHits], y[nHits], z[nHits], uint32 detId[nHits], idxInNtuple[nHits],
+ *   uint32 hitIndices0..3[nPLS], float dPhiChange, ptIn, ptErr, px, py, pz, eta,
+ *   etaErr, phi [nPLS each], int32 charge[nPLS], uint32 seedIdx[nPLS],
+ *   int32 superbin[nPLS], int8 pixelType[nPLS], int8 isQuad[nPLS]
+ * (lst_packed_size gives the byte size).  `blob_offsets[i]` is the byte
+ * offset of event i's blob inside `blobs`; each offset is a multiple of 16.
+ * lst_batch_upload copies `total_bytes` of host (preferably pinned) memory in
+ * one transfer and unpacks events into slots [first, first + count), i.e. it
+ * performs addHitToEvent + addPixelSegmentToEvent for all of them. */
+size_t lst_packed_size(uint32_t n_hits, uint32_t n_pls);
+int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                     const uint64_t* blob_offsets);
+/* Runs stages [first_stage, last_stage] for slots [first, first + count). */
+int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage);
+/* Copies the counts of slots [first, first + count) into out[count]. */
+int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LST_B200_H */

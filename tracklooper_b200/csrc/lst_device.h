@@ -1,0 +1,87 @@
+// Device-side views of the event setup and of one event's object stores.
+#pragma once
+
+#include "lst_b200.h"
+#include "lst_pixel.h"
+
+namespace lst {
+
+  // Event setup resident on the device (read-only during an event).
+  struct DeviceES {
+    Modules m;
+    const unsigned int* cpIndex;
+    const unsigned int* cpSizes;
+    const unsigned int* cpIndexPos;
+    const unsigned int* cpSizesPos;
+    const unsigned int* cpIndexNeg;
+    const unsigned int* cpSizesNeg;
+    unsigned int pixelIndexOffsetPos;
+    unsigned int pixelIndexOffsetNeg;
+    const int* mdOffset;
+    const int* mdCap;
+    const int* lsOffset;
+    const int* lsCap;
+    const int* t3CapIfUsed;
+    const int* t5CapIfEligible;
+    unsigned int nTotalMDs;
+    unsigned int nTotalSegments;
+    unsigned int maxTriplets;
+    unsigned int maxQuintuplets;
+    uint16_t nModules;
+    uint16_t nLowerModules;
+    uint16_t pixelModule;
+  };
+
+  // Status bits reported per event.
+  enum StatusBits : unsigned int {
+    kStatusUnknownDetId = 1u << 0,       // a hit's detId is not in the geometry
+    kStatusUnknownEndcapDetId = 1u << 1,  // a 2S endcap hit without strip orientation
+    kStatusHitCapacity = 1u << 2,        // more hits than the event store holds
+    kStatusPLSTruncated = 1u << 3,       // more than 50000 pLS: the rest were dropped (as the reference does)
+    kStatusTCTruncated = 1u << 4,        // a track-candidate cap was reached
+    kStatusCapOverflow = 1u << 5,        // an occupancy cap dropped objects (as the reference does)
+    kStatusInvalidInput = 1u << 6,       // a pLS hit index beyond the event's hits (replaced by hit 0)
+  };
+
+  // Per-event scalars in device memory.
+  struct EventScalars {
+    unsigned int nHits;
+    unsigned int nPLS;
+    unsigned int status;
+    unsigned int nPT5Total;
+    unsigned int nPT3Total;
+    unsigned int pad[3];
+  };
+
+  // All device pointers of one event.
+  struct EventView {
+    Hits hits;
+    Ranges rg;
+    MiniDoublets md;
+    Segments ls;
+    Triplets t3;
+    Quintuplets t5;
+    PixelTriplets pt3;
+    PixelQuintuplets pt5;
+    TrackCandidates tc;
+    EventScalars* sc;
+    lst_counts* counts;
+    // pLS inputs that are not stored in the segment store
+    unsigned int* plsHit0;
+    unsigned int* plsHit1;
+    unsigned int* plsHit2;
+    unsigned int* plsHit3;
+    float* plsDPhiChange;
+    // scratch
+    unsigned int* plsConnIndex;
+    unsigned int* plsConnSize;
+    unsigned int* plsCount;
+    unsigned int* plsOffset;
+    unsigned int* moduleCount;
+    unsigned int* moduleOffset;
+    uint8_t* t5Flag;   // removal marks of the cross-module T5 cleaning
+    uint8_t* plsFlag;  // removal marks of the second pLS cleaning pass
+    unsigned int maxHits;
+  };
+
+}  // namespace lst

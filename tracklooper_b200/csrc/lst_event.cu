@@ -1,0 +1,856 @@
+// Host runtime and C ABI of the LST object-building chain on one GPU.
+//
+// An event set (lst_event) owns one device arena holding N event slots; each
+// slot carries the complete object stores of one event at their static
+// capacities, so nothing is allocated while events run.  Stages are launched
+// with gridDim.y = number of events, so the per-event calls (one slot) and the
+// batched calls (many slots) run the same kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <new>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "es.h"
+#include "lst_b200.h"
+#include "lst_fields.h"
+#include "lst_kernels.cuh"
+
+namespace {
+
+  thread_local std::string g_lastError;
+
+  int setError(const std::string& msg) {
+    g_lastError = msg;
+    return -1;
+  }
+
+  int cudaFail(cudaError_t e, const char* what) {
+    return setError(std::string(what) + ": " + cudaGetErrorString(e));
+  }
+
+#define LST_CUDA(call)                 \
+  do {                                 \
+    cudaError_t e_ = (call);           \
+    if (e_ != cudaSuccess)             \
+      return cudaFail(e_, #call);      \
+  } while (0)
+
+  // Carves 256-byte-aligned sub-arrays out of one allocation.  With a null
+  // base it only measures.
+  struct Carver {
+    char* base = nullptr;
+    size_t off = 0;
+    template <typename T>
+    T* take(size_t n) {
+      off = (off + 255) & ~size_t(255);
+      T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+      off += n * sizeof(T);
+      return p;
+    }
+  };
+
+  struct Sizes {
+    size_t H, M, L, MD, LS, P, T3, T5, P3, P5, TC;
+  };
+
+  void carveEvent(Carver& c, lst::EventView& v, const Sizes& s) {
+    const size_t H = s.H, M = s.M, L = s.L, MD = s.MD, LS = s.LS, P = s.P, T3 = s.T3, T5 = s.T5, P3 = s.P3,
+                 P5 = s.P5, TC = s.TC;
+    (void)H;
+#define LST_CARVE(prefix, member, field, type, count) v.member.field = c.take<type>(count);
+    LST_EVENT_FIELDS(LST_CARVE)
+#undef LST_CARVE
+#define LST_CARVE_SCRATCH(field, type, count) v.field = c.take<type>(count);
+    LST_SCRATCH_FIELDS(LST_CARVE_SCRATCH)
+#undef LST_CARVE_SCRATCH
+    v.sc = c.take<lst::EventScalars>(1);
+  }
+
+  struct FieldInfo {
+    std::string name;
+    size_t elemSize;
+    char kind;
+  };
+
+  template <typename T>
+  constexpr char kindOf() {
+    return std::is_floating_point<T>::value ? 'f' : (std::is_signed<T>::value ? 'i' : 'u');
+  }
+
+  // Field names ("store.field") and element types in table order.
+  const std::vector<FieldInfo>& fieldTable() {
+    static const std::vector<FieldInfo> table = [] {
+      std::vector<FieldInfo> t;
+#define LST_NAME(prefix, member, field, type, count) \
+  t.push_back(FieldInfo{std::string(prefix) + #field, sizeof(type), kindOf<type>()});
+      LST_EVENT_FIELDS(LST_NAME)
+#undef LST_NAME
+      return t;
+    }();
+    return table;
+  }
+
+  // Device pointer, length and element size of a named field of one view.
+  bool findField(const lst::EventView& v, const Sizes& s, const std::string& name, void*& ptr, size_t& n,
+                 size_t& esz) {
+    const size_t H = s.H, M = s.M, L = s.L, MD = s.MD, LS = s.LS, P = s.P, T3 = s.T3, T5 = s.T5, P3 = s.P3,
+                 P5 = s.P5, TC = s.TC;
+    (void)H;
+#define LST_FIND(prefix, member, field, type, count) \
+  if (name == prefix #field) {                       \
+    ptr = (void*)v.member.field;                     \
+    n = (count);                                     \
+    esz = sizeof(type);                              \
+    return true;                                     \
+  }
+    LST_EVENT_FIELDS(LST_FIND)
+#undef LST_FIND
+    return false;
+  }
+
+  unsigned int ceilDiv(size_t a, size_t b) { return static_cast<unsigned int>((a + b - 1) / b); }
+
+}  // namespace
+
+// ------------------------------------------------------------------ ES
+struct lst_es {
+  int device = 0;
+  lst::EsHost host;
+  lst::DeviceES view{};
+  void* arena = nullptr;
+  size_t arenaBytes = 0;
+  bool haveDnn = false;
+  unsigned int nEligibleMax = 0;  // lower modules that can seed T5s
+  std::vector<float> dnn;
+};
+
+namespace {
+
+  template <typename T>
+  const T* upload(Carver& c, const std::vector<T>& v, std::vector<std::pair<void*, const void*>>& copies,
+                  std::vector<size_t>& sizes) {
+    T* p = c.take<T>(std::max<size_t>(v.size(), 1));
+    if (c.base && !v.empty()) {
+      copies.emplace_back(p, v.data());
+      sizes.push_back(v.size() * sizeof(T));
+    }
+    return p;
+  }
+
+  // Lays out (or, with a base, fills) the device copy of the event setup.
+  void layoutES(Carver& c, lst_es& es, std::vector<std::pair<void*, const void*>>& copies, std::vector<size_t>& sizes) {
+    const lst::EsHost& h = es.host;
+    lst::DeviceES& d = es.view;
+    lst::Modules& m = d.m;
+    m.detIds = upload(c, h.detIds, copies, sizes);
+    m.moduleMap = upload(c, h.moduleMap, copies, sizes);
+    m.mapdetId = upload(c, h.mapdetId, copies, sizes);
+    m.mapIdx = upload(c, h.mapIdx, copies, sizes);
+    m.nConnectedModules = upload(c, h.nConnectedModules, copies, sizes);
+    m.drdzs = upload(c, h.drdzs, copies, sizes);
+    m.dxdys = upload(c, h.dxdys, copies, sizes);
+    m.partnerModuleIndices = upload(c, h.partnerModuleIndices, copies, sizes);
+    m.layers = upload(c, h.layers, copies, sizes);
+    m.rings = upload(c, h.rings, copies, sizes);
+    m.modules = upload(c, h.modules, copies, sizes);
+    m.rods = upload(c, h.rods, copies, sizes);
+    m.subdets = upload(c, h.subdets, copies, sizes);
+    m.sides = upload(c, h.sides, copies, sizes);
+    m.eta = upload(c, h.eta, copies, sizes);
+    m.r = upload(c, h.r, copies, sizes);
+    m.isInverted = upload(c, h.isInverted, copies, sizes);
+    m.isLower = upload(c, h.isLower, copies, sizes);
+    m.isAnchor = upload(c, h.isAnchor, copies, sizes);
+    m.moduleType = upload(c, h.moduleType, copies, sizes);
+    m.moduleLayerType = upload(c, h.moduleLayerType, copies, sizes);
+    m.sdlLayers = upload(c, h.sdlLayers, copies, sizes);
+    m.connectedPixels = upload(c, h.connectedPixels, copies, sizes);
+    m.geoMapDetId = upload(c, h.geoMapDetId, copies, sizes);
+    m.geoMapPhi = upload(c, h.geoMapPhi, copies, sizes);
+    m.nEndCapMap = static_cast<unsigned int>(h.geoMapDetId.size());
+    m.nModules = h.nModules;
+    m.nLowerModules = h.nLowerModules;
+    d.cpIndex = upload(c, h.connectedPixelsIndex, copies, sizes);
+    d.cpSizes = upload(c, h.connectedPixelsSizes, copies, sizes);
+    d.cpIndexPos = upload(c, h.connectedPixelsIndexPos, copies, sizes);
+    d.cpSizesPos = upload(c, h.connectedPixelsSizesPos, copies, sizes);
+    d.cpIndexNeg = upload(c, h.connectedPixelsIndexNeg, copies, sizes);
+    d.cpSizesNeg = upload(c, h.connectedPixelsSizesNeg, copies, sizes);
+    d.mdOffset = upload(c, h.mdOffset, copies, sizes);
+    d.mdCap = upload(c, h.mdCap, copies, sizes);
+    d.lsOffset = upload(c, h.lsOffset, copies, sizes);
+    d.lsCap = upload(c, h.lsCap, copies, sizes);
+    d.t3CapIfUsed = upload(c, h.t3CapIfUsed, copies, sizes);
+    d.t5CapIfEligible = upload(c, h.t5CapIfEligible, copies, sizes);
+    // The positive- and negative-z pixel maps follow the inclusive one in
+    // connectedPixels (SDL/Event.cc:1049-1052).
+    const size_t last = lst::kSizeSuperbins - 1;
+    d.pixelIndexOffsetPos = h.connectedPixelsIndex[last] + h.connectedPixelsSizes[last];
+    d.pixelIndexOffsetNeg = h.connectedPixelsIndexPos[last] + h.connectedPixelsSizesPos[last] + d.pixelIndexOffsetPos;
+    d.nTotalMDs = h.nTotalMDs;
+    d.nTotalSegments = h.nTotalSegments;
+    d.maxTriplets = h.maxTriplets;
+    d.maxQuintuplets = h.maxQuintuplets;
+    d.nModules = h.nModules;
+    d.nLowerModules = h.nLowerModules;
+    d.pixelModule = h.pixelModuleIndex;
+  }
+
+  int loadWeightsFile(const char* path, std::vector<float>& w) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f.is_open())
+      return setError(std::string("cannot open T5 DNN weights ") + path);
+    std::streamsize n = f.tellg();
+    if (n != static_cast<std::streamsize>(lst::kT5DnnParams * sizeof(float)))
+      return setError(std::string("T5 DNN weight file has the wrong size: ") + path);
+    f.seekg(0);
+    w.resize(lst::kT5DnnParams);
+    f.read(reinterpret_cast<char*>(w.data()), n);
+    return 0;
+  }
+
+  int uploadWeights(lst_es* es) {
+    if (es->dnn.size() != lst::kT5DnnParams)
+      return setError("T5 DNN weights must hold 2337 values");
+    lst::T5DnnWeights w;
+    static_assert(sizeof(lst::T5DnnWeights) == lst::kT5DnnParams * sizeof(float), "packed weight struct");
+    std::memcpy(&w, es->dnn.data(), sizeof(w));
+    LST_CUDA(cudaSetDevice(es->device));
+    LST_CUDA(cudaMemcpyToSymbol(lst::c_t5dnn, &w, sizeof(w)));
+    LST_CUDA(cudaDeviceSynchronize());
+    es->haveDnn = true;
+    return 0;
+  }
+
+}  // namespace
+
+// ---------------------------------------------------------------- events
+struct lst_event {
+  lst_es* es = nullptr;
+  int nSlots = 0;
+  unsigned int maxHits = 0;
+  cudaStream_t stream = nullptr;
+  bool ownStream = false;
+  char* arena = nullptr;
+  size_t slotBytes = 0;
+  size_t totalBytes = 0;
+  Sizes sizes{};
+  std::vector<lst::EventView> hv;
+  lst::EventView* dv = nullptr;
+  int t5Method = LST_T5_DNN;
+  // batched-input staging
+  unsigned char* inbox = nullptr;
+  size_t inboxBytes = 0;
+  unsigned long long* dOffsets = nullptr;
+  // per-slot counts, contiguous on the device and in pinned host memory
+  lst_counts* dCounts = nullptr;
+  lst_counts* hCounts = nullptr;
+};
+
+namespace {
+
+  constexpr unsigned int kThreads = 256;
+  constexpr unsigned int kResidentBlocks = 148 * 8;
+
+  // Blocks per event for a grid-stride kernel over n items.
+  unsigned int blocksFor(size_t n, int count, unsigned int threads = kThreads) {
+    unsigned int want = std::max(1u, ceilDiv(n, threads));
+    unsigned int cap = std::max(1u, ceilDiv(2 * kResidentBlocks, static_cast<size_t>(std::max(count, 1))));
+    return std::min(want, cap);
+  }
+
+  int checkSlots(lst_event* ev, int first, int count) {
+    if (!ev)
+      return setError("null event set");
+    if (first < 0 || count < 0 || first + count > ev->nSlots)
+      return setError("slot range outside the event set");
+    return 0;
+  }
+
+  int launchStatus(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+      return cudaFail(e, what);
+    return 0;
+  }
+
+  int runReset(lst_event* ev, int first, int count) {
+    const lst_es* es = ev->es;
+    dim3 g(blocksFor(2 * size_t(es->view.nModules), count), count);
+    lst::kResetEvent<<<g, kThreads, 0, ev->stream>>>(es->view, ev->dv + first);
+    return launchStatus("kResetEvent");
+  }
+
+  int runHitKernels(lst_event* ev, int first, int count) {
+    const lst::DeviceES& d = ev->es->view;
+    lst::kHitPrep<<<dim3(blocksFor(ev->maxHits, count), count), kThreads, 0, ev->stream>>>(d, ev->dv + first);
+    lst::kModuleRanges<<<dim3(blocksFor(d.nLowerModules, count), count), kThreads, 0, ev->stream>>>(d, ev->dv + first);
+    return launchStatus("hit kernels");
+  }
+
+  int runPixelIngest(lst_event* ev, int first, int count) {
+    const lst::DeviceES& d = ev->es->view;
+    lst::kPixelIngest<<<dim3(blocksFor(lst::kMaxPixelSegments, count), count), kThreads, 0, ev->stream>>>(
+        d, ev->dv + first);
+    return launchStatus("kPixelIngest");
+  }
+
+  // Warp-per-object kernels: blocks of `warps` warps.
+  dim3 warpGrid(size_t nObjects, int warps, int count) {
+    return dim3(blocksFor(nObjects, count, 32u * warps) , count);
+  }
+
+  int runStage(lst_event* ev, int first, int count, int stage) {
+    const lst::DeviceES& d = ev->es->view;
+    const lst::EventView* v = ev->dv + first;
+    cudaStream_t s = ev->stream;
+    const size_t nLower = d.nLowerModules;
+    const size_t P = lst::kMaxPixelSegments;
+    const dim3 one(1, count);
+    switch (stage) {
+      case LST_STAGE_MINI_DOUBLETS:
+        lst::kCreateMD<<<warpGrid(nLower, 8, count), 256, 0, s>>>(d, v);
+        lst::kMDRanges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        break;
+      case LST_STAGE_SEGMENTS:
+        lst::kCreateLS<<<warpGrid(nLower, lst::kLSWarps, count), 32 * lst::kLSWarps, 0, s>>>(d, v);
+        lst::kLSRanges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        break;
+      case LST_STAGE_TRIPLETS:
+        lst::kT3Offsets<<<one, 1024, 0, s>>>(d, v);
+        lst::kCreateT3<<<warpGrid(nLower, lst::kT3Warps, count), 32 * lst::kT3Warps, 0, s>>>(d, v);
+        lst::kT3Ranges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        break;
+      case LST_STAGE_QUINTUPLETS: {
+        if (ev->t5Method == LST_T5_DNN && !ev->es->haveDnn)
+          return setError("the DNN T5 method needs weights (lst_es_load or lst_es_set_t5dnn_weights)");
+        bool useDnn = ev->t5Method == LST_T5_DNN;
+        lst::kT5Eligible<<<one, 1024, 0, s>>>(d, v);
+        lst::kCreateT5<<<warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, 0, s>>>(
+            d, v, useDnn);
+        lst::kT5DedupAfterBuild<<<dim3(ceilDiv(nLower * 32, 256), count), 256, 0, s>>>(d, v);
+        lst::kT5Ranges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        break;
+      }
+      case LST_STAGE_PLS_CLEANING:
+        lst::kPLSClean<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v, false);
+        break;
+      case LST_STAGE_PIXEL_QUINTUPLETS:
+        lst::kPixelConnect<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
+        lst::kPT5Count<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
+        lst::kPLSScan<<<one, 1024, 0, s>>>(d, v, 0);
+        lst::kPT5Emit<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
+        lst::kPT5Dedup<<<dim3(blocksFor(lst::kMaxPixelQuintuplets, count), count), kThreads, 0, s>>>(d, v);
+        lst::kAddPT5TC<<<one, 1024, 0, s>>>(d, v);
+        break;
+      case LST_STAGE_PIXEL_TRIPLETS:
+        lst::kPixelConnect<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
+        lst::kPT3Count<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
+        lst::kPLSScan<<<one, 1024, 0, s>>>(d, v, 1);
+        lst::kPT3Emit<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
+        lst::kPT3Dedup<<<dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, 0, s>>>(d, v);
+        break;
+      case LST_STAGE_TRACK_CANDIDATES: {
+        const size_t nE = ev->es->nEligibleMax;
+        const dim3 eligGrid(ceilDiv(std::max<size_t>(nE, 1) * 32, 256), count);
+        lst::kCrossCleanPT3<<<dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, 0, s>>>(d, v);
+        lst::kAddPT3TC<<<one, 1024, 0, s>>>(d, v);
+        lst::kT5DedupBeforeTC<<<eligGrid, 256, 0, s>>>(d, v);
+        lst::kMergeT5Flag<<<eligGrid, 256, 0, s>>>(d, v);
+        lst::kCrossCleanT5<<<eligGrid, 256, 0, s>>>(d, v);
+        lst::kT5TCCount<<<eligGrid, 256, 0, s>>>(d, v);
+        lst::kT5TCScan<<<one, 1024, 0, s>>>(d, v);
+        lst::kT5TCEmit<<<eligGrid, 256, 0, s>>>(d, v);
+        lst::kT5TCFinish<<<one, 32, 0, s>>>(d, v);
+        lst::kPLSClean<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v, true);
+        lst::kMergePLSFlag<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
+        lst::kCrossCleanPLS<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
+        lst::kAddPLSTC<<<one, 1024, 0, s>>>(d, v);
+        break;
+      }
+      default:
+        return setError("unknown stage " + std::to_string(stage));
+    }
+    return launchStatus("stage kernels");
+  }
+
+  int runCounts(lst_event* ev, int first, int count) {
+    lst::kCounts<<<dim3(1, count), 256, 0, ev->stream>>>(ev->es->view, ev->dv + first);
+    return launchStatus("kCounts");
+  }
+
+  int readCounts(lst_event* ev, int first, int count, lst_counts* out) {
+    int rc = runCounts(ev, first, count);
+    if (rc)
+      return rc;
+    LST_CUDA(cudaMemcpyAsync(ev->hCounts, ev->dCounts + first, sizeof(lst_counts) * count, cudaMemcpyDeviceToHost,
+                             ev->stream));
+    LST_CUDA(cudaStreamSynchronize(ev->stream));
+    std::memcpy(out, ev->hCounts, sizeof(lst_counts) * count);
+    return 0;
+  }
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+const char* lst_last_error(void) { return g_lastError.c_str(); }
+
+int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out) {
+  if (!geometry_dir || !out)
+    return setError("lst_es_load: null argument");
+  *out = nullptr;
+  std::unique_ptr<lst_es> es(new (std::nothrow) lst_es());
+  if (!es)
+    return setError("out of host memory");
+  es->device = device;
+  std::string err = lst::loadEsHost(geometry_dir, es->host);
+  if (!err.empty())
+    return setError(err);
+  for (int v : es->host.t5CapIfEligible)
+    if (v >= 0)
+      es->nEligibleMax++;
+  LST_CUDA(cudaSetDevice(device));
+  std::vector<std::pair<void*, const void*>> copies;
+  std::vector<size_t> sizes;
+  Carver measure;
+  layoutES(measure, *es, copies, sizes);
+  es->arenaBytes = measure.off;
+  LST_CUDA(cudaMalloc(&es->arena, es->arenaBytes));
+  Carver fill;
+  fill.base = static_cast<char*>(es->arena);
+  layoutES(fill, *es, copies, sizes);
+  for (size_t i = 0; i < copies.size(); ++i)
+    LST_CUDA(cudaMemcpy(copies[i].first, copies[i].second, sizes[i], cudaMemcpyHostToDevice));
+  if (t5dnn_weights_path) {
+    int rc = loadWeightsFile(t5dnn_weights_path, es->dnn);
+    if (rc) {
+      cudaFree(es->arena);
+      return rc;
+    }
+    rc = uploadWeights(es.get());
+    if (rc) {
+      cudaFree(es->arena);
+      return rc;
+    }
+  }
+  *out = es.release();
+  return 0;
+}
+
+void lst_es_free(lst_es* es) {
+  if (!es)
+    return;
+  if (es->arena) {
+    cudaSetDevice(es->device);
+    cudaFree(es->arena);
+  }
+  delete es;
+}
+
+int lst_es_get_info(const lst_es* es, lst_es_info* out) {
+  if (!es || !out)
+    return setError("lst_es_get_info: null argument");
+  out->nModules = es->host.nModules;
+  out->nLowerModules = es->host.nLowerModules;
+  out->pixelModule = es->host.pixelModuleIndex;
+  out->nConnectedPixels = es->host.nPixels;
+  out->nTotalMDs = es->host.nTotalMDs;
+  out->nTotalSegments = es->host.nTotalSegments;
+  out->maxTriplets = es->host.maxTriplets;
+  out->maxQuintuplets = es->host.maxQuintuplets;
+  return 0;
+}
+
+int lst_es_set_t5dnn_weights(lst_es* es, const float* weights, size_t n) {
+  if (!es || !weights)
+    return setError("lst_es_set_t5dnn_weights: null argument");
+  if (n != lst::kT5DnnParams)
+    return setError("T5 DNN weights must hold 2337 values");
+  es->dnn.assign(weights, weights + n);
+  return uploadWeights(es);
+}
+
+int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, lst_event** out) {
+  if (!es || !out || n_slots <= 0 || max_hits == 0)
+    return setError("lst_event_create: bad argument");
+  *out = nullptr;
+  std::unique_ptr<lst_event> ev(new (std::nothrow) lst_event());
+  if (!ev)
+    return setError("out of host memory");
+  ev->es = es;
+  ev->nSlots = n_slots;
+  ev->maxHits = max_hits;
+  ev->t5Method = es->haveDnn ? LST_T5_DNN : LST_T5_CUTS;
+  const lst::EsHost& h = es->host;
+  ev->sizes = Sizes{max_hits,
+                    h.nModules,
+                    h.nLowerModules,
+                    h.nTotalMDs,
+                    h.nTotalSegments,
+                    lst::kMaxPixelSegments,
+                    std::max<size_t>(h.maxTriplets, 1),
+                    std::max<size_t>(h.maxQuintuplets, 1),
+                    lst::kMaxPixelTriplets,
+                    lst::kMaxPixelQuintuplets,
+                    lst::kMaxTrackCandidates};
+  LST_CUDA(cudaSetDevice(es->device));
+  Carver measure;
+  lst::EventView tmp{};
+  carveEvent(measure, tmp, ev->sizes);
+  ev->slotBytes = (measure.off + 4095) & ~size_t(4095);
+  ev->totalBytes = ev->slotBytes * n_slots;
+  if (stream) {
+    ev->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    LST_CUDA(cudaStreamCreateWithFlags(&ev->stream, cudaStreamNonBlocking));
+    ev->ownStream = true;
+  }
+  cudaError_t e = cudaMalloc(&ev->arena, ev->totalBytes);
+  if (e != cudaSuccess) {
+    if (ev->ownStream)
+      cudaStreamDestroy(ev->stream);
+    return cudaFail(e, "event arena");
+  }
+  LST_CUDA(cudaMalloc(&ev->dCounts, sizeof(lst_counts) * n_slots));
+  ev->hv.resize(n_slots);
+  for (int i = 0; i < n_slots; ++i) {
+    Carver c;
+    c.base = ev->arena + ev->slotBytes * i;
+    carveEvent(c, ev->hv[i], ev->sizes);
+    ev->hv[i].maxHits = max_hits;
+    ev->hv[i].counts = ev->dCounts + i;
+  }
+  LST_CUDA(cudaMalloc(&ev->dv, sizeof(lst::EventView) * n_slots));
+  LST_CUDA(cudaMemcpy(ev->dv, ev->hv.data(), sizeof(lst::EventView) * n_slots, cudaMemcpyHostToDevice));
+  LST_CUDA(cudaMalloc(&ev->dOffsets, sizeof(unsigned long long) * n_slots));
+  LST_CUDA(cudaMallocHost(&ev->hCounts, sizeof(lst_counts) * n_slots));
+  // Start every slot empty.
+  int rc = runReset(ev.get(), 0, n_slots);
+  if (rc)
+    return rc;
+  LST_CUDA(cudaStreamSynchronize(ev->stream));
+  *out = ev.release();
+  return 0;
+}
+
+void lst_event_destroy(lst_event* ev) {
+  if (!ev)
+    return;
+  cudaSetDevice(ev->es->device);
+  cudaStreamSynchronize(ev->stream);
+  cudaFree(ev->arena);
+  cudaFree(ev->dv);
+  cudaFree(ev->dOffsets);
+  cudaFree(ev->dCounts);
+  if (ev->inbox)
+    cudaFree(ev->inbox);
+  cudaFreeHost(ev->hCounts);
+  if (ev->ownStream)
+    cudaStreamDestroy(ev->stream);
+  delete ev;
+}
+
+int lst_event_memory(const lst_event* ev, size_t* bytes) {
+  if (!ev || !bytes)
+    return setError("lst_event_memory: null argument");
+  *bytes = ev->totalBytes + ev->inboxBytes;
+  return 0;
+}
+
+int lst_event_sync(lst_event* ev) {
+  if (!ev)
+    return setError("null event set");
+  LST_CUDA(cudaStreamSynchronize(ev->stream));
+  return 0;
+}
+
+void* lst_event_stream(lst_event* ev) { return ev ? static_cast<void*>(ev->stream) : nullptr; }
+
+int lst_event_set_t5_method(lst_event* ev, int method) {
+  if (!ev)
+    return setError("null event set");
+  if (method != LST_T5_DNN && method != LST_T5_CUTS)
+    return setError("unknown T5 method");
+  if (method == LST_T5_DNN && !ev->es->haveDnn)
+    return setError("the DNN T5 method needs weights");
+  ev->t5Method = method;
+  return 0;
+}
+
+int lst_event_reset(lst_event* ev, int slot) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  return runReset(ev, slot, 1);
+}
+
+int lst_event_add_hits(lst_event* ev, int slot, uint32_t n, const float* x, const float* y, const float* z,
+                       const uint32_t* detId, const uint32_t* idxInNtuple) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  if (n > ev->maxHits)
+    return LST_STATUS_HIT_CAPACITY;
+  if (n > 0 && (!x || !y || !z || !detId || !idxInNtuple))
+    return setError("lst_event_add_hits: null array");
+  rc = runReset(ev, slot, 1);
+  if (rc)
+    return rc;
+  const lst::EventView& v = ev->hv[slot];
+  cudaStream_t s = ev->stream;
+  if (n > 0) {
+    LST_CUDA(cudaMemcpyAsync(v.hits.xs, x, n * sizeof(float), cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.hits.ys, y, n * sizeof(float), cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.hits.zs, z, n * sizeof(float), cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.hits.detid, detId, n * sizeof(uint32_t), cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.hits.idxs, idxInNtuple, n * sizeof(uint32_t), cudaMemcpyDefault, s));
+  }
+  lst::kSetInputCounts<<<1, 1, 0, s>>>(ev->dv, slot, 1, n, 1, 0u, 0u);
+  rc = launchStatus("kSetInputCounts");
+  if (rc)
+    return rc;
+  return runHitKernels(ev, slot, 1);
+}
+
+int lst_event_add_pixel_segments(lst_event* ev, int slot, uint32_t n, const uint32_t* hitIndices0,
+                                 const uint32_t* hitIndices1, const uint32_t* hitIndices2,
+                                 const uint32_t* hitIndices3, const float* dPhiChange, const float* ptIn,
+                                 const float* ptErr, const float* px, const float* py, const float* pz,
+                                 const float* eta, const float* etaErr, const float* phi, const int32_t* charge,
+                                 const uint32_t* seedIdx, const int32_t* superbin, const int8_t* pixelType,
+                                 const int8_t* isQuad) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  unsigned int status = 0;
+  uint32_t size = n;
+  if (size > lst::kMaxPixelSegments) {
+    size = lst::kMaxPixelSegments;
+    status |= LST_STATUS_PLS_TRUNCATED;
+  }
+  if (size > 0 && (!hitIndices0 || !hitIndices1 || !hitIndices2 || !hitIndices3 || !dPhiChange || !ptIn || !ptErr ||
+                   !px || !py || !pz || !eta || !etaErr || !phi || !charge || !seedIdx || !superbin || !pixelType ||
+                   !isQuad))
+    return setError("lst_event_add_pixel_segments: null array");
+  const lst::EventView& v = ev->hv[slot];
+  cudaStream_t s = ev->stream;
+  if (size > 0) {
+    LST_CUDA(cudaMemcpyAsync(v.plsHit0, hitIndices0, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.plsHit1, hitIndices1, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.plsHit2, hitIndices2, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.plsHit3, hitIndices3, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.plsDPhiChange, dPhiChange, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.ptIn, ptIn, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.ptErr, ptErr, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.px, px, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.py, py, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.pz, pz, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.etaErr, etaErr, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.isQuad, isQuad, size, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.eta, eta, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.phi, phi, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.charge, charge, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.seedIdx, seedIdx, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.superbin, superbin, size * 4, cudaMemcpyDefault, s));
+    LST_CUDA(cudaMemcpyAsync(v.ls.pixelType, pixelType, size, cudaMemcpyDefault, s));
+  }
+  lst::kSetInputCounts<<<1, 1, 0, s>>>(ev->dv, slot, 0, 0u, 1, size, status);
+  rc = launchStatus("kSetInputCounts");
+  if (rc)
+    return rc;
+  return runPixelIngest(ev, slot, 1);
+}
+
+int lst_event_run_stage(lst_event* ev, int slot, int stage) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  return runStage(ev, slot, 1, stage);
+}
+
+int lst_event_create_mini_doublets(lst_event* ev, int slot) {
+  return lst_event_run_stage(ev, slot, LST_STAGE_MINI_DOUBLETS);
+}
+int lst_event_create_segments(lst_event* ev, int slot) { return lst_event_run_stage(ev, slot, LST_STAGE_SEGMENTS); }
+int lst_event_create_triplets(lst_event* ev, int slot) { return lst_event_run_stage(ev, slot, LST_STAGE_TRIPLETS); }
+int lst_event_create_quintuplets(lst_event* ev, int slot) {
+  return lst_event_run_stage(ev, slot, LST_STAGE_QUINTUPLETS);
+}
+int lst_event_pixel_line_segment_cleaning(lst_event* ev, int slot) {
+  return lst_event_run_stage(ev, slot, LST_STAGE_PLS_CLEANING);
+}
+int lst_event_create_pixel_quintuplets(lst_event* ev, int slot) {
+  return lst_event_run_stage(ev, slot, LST_STAGE_PIXEL_QUINTUPLETS);
+}
+int lst_event_create_pixel_triplets(lst_event* ev, int slot) {
+  return lst_event_run_stage(ev, slot, LST_STAGE_PIXEL_TRIPLETS);
+}
+int lst_event_create_track_candidates(lst_event* ev, int slot) {
+  return lst_event_run_stage(ev, slot, LST_STAGE_TRACK_CANDIDATES);
+}
+
+int lst_event_get_counts(lst_event* ev, int slot, lst_counts* out) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  if (!out)
+    return setError("lst_event_get_counts: null output");
+  rc = readCounts(ev, slot, 1, out);
+  if (rc)
+    return rc;
+  return static_cast<int>(out->status & 0x7fffffffu);
+}
+
+int lst_event_get_field(lst_event* ev, int slot, const char* name, void* dst, size_t capacity, size_t* n_elems,
+                        size_t* elem_size) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  if (!name)
+    return setError("lst_event_get_field: null name");
+  void* ptr = nullptr;
+  size_t n = 0, esz = 0;
+  if (!findField(ev->hv[slot], ev->sizes, name, ptr, n, esz))
+    return setError(std::string("unknown field ") + name);
+  if (n_elems)
+    *n_elems = n;
+  if (elem_size)
+    *elem_size = esz;
+  if (dst && capacity) {
+    size_t k = std::min(n, capacity);
+    LST_CUDA(cudaMemcpyAsync(dst, ptr, k * esz, cudaMemcpyDeviceToHost, ev->stream));
+    LST_CUDA(cudaStreamSynchronize(ev->stream));
+  }
+  return 0;
+}
+
+int lst_event_field_device_ptr(lst_event* ev, int slot, const char* name, void** dptr, size_t* n_elems,
+                               size_t* elem_size) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  if (!name || !dptr)
+    return setError("lst_event_field_device_ptr: null argument");
+  size_t n = 0, esz = 0;
+  if (!findField(ev->hv[slot], ev->sizes, name, *dptr, n, esz))
+    return setError(std::string("unknown field ") + name);
+  if (n_elems)
+    *n_elems = n;
+  if (elem_size)
+    *elem_size = esz;
+  return 0;
+}
+
+int lst_field_count(void) { return static_cast<int>(fieldTable().size()); }
+
+const char* lst_field_name(int i) {
+  const auto& t = fieldTable();
+  if (i < 0 || i >= static_cast<int>(t.size()))
+    return nullptr;
+  return t[i].name.c_str();
+}
+
+int lst_field_info(int i, const char** name, size_t* elem_size, char* kind) {
+  const auto& t = fieldTable();
+  if (i < 0 || i >= static_cast<int>(t.size()))
+    return setError("field index out of range");
+  if (name)
+    *name = t[i].name.c_str();
+  if (elem_size)
+    *elem_size = t[i].elemSize;
+  if (kind)
+    *kind = t[i].kind;
+  return 0;
+}
+
+size_t lst_packed_size(uint32_t n_hits, uint32_t n_pls) { return lst::packedLayout(n_hits, n_pls).end; }
+
+int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                     const uint64_t* blob_offsets) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (count == 0)
+    return 0;
+  if (!blobs || !blob_offsets)
+    return setError("lst_batch_upload: null argument");
+  for (int i = 0; i < count; ++i) {
+    if (blob_offsets[i] % 16 != 0 || blob_offsets[i] + 16 > total_bytes)
+      return setError("lst_batch_upload: blob offset misaligned or outside the buffer");
+  }
+  if (total_bytes > ev->inboxBytes) {
+    LST_CUDA(cudaStreamSynchronize(ev->stream));
+    if (ev->inbox)
+      LST_CUDA(cudaFree(ev->inbox));
+    ev->inbox = nullptr;
+    ev->inboxBytes = 0;
+    size_t want = (total_bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
+    LST_CUDA(cudaMalloc(&ev->inbox, want));
+    ev->inboxBytes = want;
+  }
+  cudaStream_t s = ev->stream;
+  LST_CUDA(cudaMemcpyAsync(ev->inbox, blobs, total_bytes, cudaMemcpyDefault, s));
+  LST_CUDA(cudaMemcpyAsync(ev->dOffsets + first, blob_offsets, sizeof(uint64_t) * count, cudaMemcpyDefault, s));
+  rc = runReset(ev, first, count);
+  if (rc)
+    return rc;
+  lst::kUnpack<<<dim3(blocksFor(ev->maxHits, count), count), kThreads, 0, s>>>(ev->dv + first, ev->inbox,
+                                                                             ev->dOffsets + first);
+  rc = launchStatus("kUnpack");
+  if (rc)
+    return rc;
+  rc = runHitKernels(ev, first, count);
+  if (rc)
+    return rc;
+  return runPixelIngest(ev, first, count);
+}
+
+int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (count == 0)
+    return 0;
+  if (first_stage < LST_STAGE_MINI_DOUBLETS || last_stage > LST_STAGE_TRACK_CANDIDATES || first_stage > last_stage)
+    return setError("lst_batch_run: bad stage range");
+  // Stage order of a full event (SDL/LST.cc:34-81): the pT5 stage runs
+  // before the pT3 stage.
+  static const int order[] = {LST_STAGE_MINI_DOUBLETS,
+                              LST_STAGE_SEGMENTS,
+                              LST_STAGE_TRIPLETS,
+                              LST_STAGE_QUINTUPLETS,
+                              LST_STAGE_PLS_CLEANING,
+                              LST_STAGE_PIXEL_QUINTUPLETS,
+                              LST_STAGE_PIXEL_TRIPLETS,
+                              LST_STAGE_TRACK_CANDIDATES};
+  for (int st : order) {
+    if (st < first_stage || st > last_stage)
+      continue;
+    rc = runStage(ev, first, count, st);
+    if (rc)
+      return rc;
+  }
+  return 0;
+}
+
+int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (!out)
+    return setError("lst_batch_get_counts: null output");
+  if (count == 0)
+    return 0;
+  return readCounts(ev, first, count, out);
+}
+
+}  // extern "C"

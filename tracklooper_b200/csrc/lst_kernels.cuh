@@ -1,0 +1,1677 @@
+// CUDA kernels of the LST object-building chain.  Every kernel takes the
+// device event setup by value and an array of per-event views; blockIdx.y
+// selects the event, so one launch processes a whole batch of events.
+//
+// Ordering.  The reference appends objects with atomic counters; its serial
+// CPU backend therefore stores them in loop-nest order, and per-module
+// occupancy caps keep the first N in that order.  Here each module (or pixel
+// seed) is owned by one warp that walks the flattened loop nest in order,
+// 32 candidates at a time, and places accepted objects with a warp ballot
+// prefix, so object indices equal the reference CPU backend's.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lst_device.h"
+
+namespace lst {
+
+  constexpr unsigned int kFullMask = 0xffffffffu;
+
+  // T5 classifier weights (uploaded once per process from the weight file).
+  __constant__ T5DnnWeights c_t5dnn;
+
+  struct ConstDnn {
+    __device__ __forceinline__ const T5DnnWeights& get() const { return c_t5dnn; }
+  };
+
+  __device__ __forceinline__ unsigned int laneId() { return threadIdx.x & 31u; }
+  __device__ __forceinline__ unsigned int lanesBelowMask() { return (1u << laneId()) - 1u; }
+
+  // Rank of this lane's flag among the set flags of lower lanes; total = set flags in the warp.
+  __device__ __forceinline__ unsigned int warpRank(bool flag, unsigned int& total) {
+    unsigned int b = __ballot_sync(kFullMask, flag);
+    total = __popc(b);
+    return __popc(b & lanesBelowMask());
+  }
+
+  // Exclusive prefix sums of countOf(0..n-1) into pre[0..n] (pre[n] = total),
+  // computed by one warp.  pre must be warp-private shared memory.
+  template <typename F>
+  __device__ __forceinline__ unsigned int warpPrefix(unsigned int* pre, int n, F countOf) {
+    unsigned int carry = 0;
+    for (int base = 0; base < n; base += 32) {
+      int i = base + int(laneId());
+      unsigned int c = (i < n) ? countOf(i) : 0u;
+      unsigned int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(kFullMask, incl, o);
+        if (int(laneId()) >= o)
+          incl += y;
+      }
+      if (i < n)
+        pre[i] = carry + incl - c;
+      carry += __shfl_sync(kFullMask, incl, 31);
+    }
+    if (laneId() == 0)
+      pre[n] = carry;
+    __syncwarp();
+    return carry;
+  }
+
+  // Largest k in [0, n) with pre[k] <= f (pre[n] > f).
+  __device__ __forceinline__ int findSlot(const unsigned int* pre, int n, unsigned int f) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (pre[mid] <= f)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    return lo;
+  }
+
+  // Block-wide exclusive scan (blockDim.x a multiple of 32, <= 1024).
+  __device__ __forceinline__ unsigned int blockExclusiveScan(unsigned int v, unsigned int& total) {
+    __shared__ unsigned int sWarp[32];
+    __shared__ unsigned int sTotal;
+    unsigned int lane = laneId(), wid = threadIdx.x >> 5;
+    unsigned int nw = blockDim.x >> 5;
+    unsigned int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned int y = __shfl_up_sync(kFullMask, incl, o);
+      if (int(lane) >= o)
+        incl += y;
+    }
+    if (lane == 31)
+      sWarp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      unsigned int w = (lane < nw) ? sWarp[lane] : 0u;
+      unsigned int wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(kFullMask, wi, o);
+        if (int(lane) >= o)
+          wi += y;
+      }
+      if (lane < nw)
+        sWarp[lane] = wi - w;
+      if (lane == 31)
+        sTotal = wi;
+    }
+    __syncthreads();
+    unsigned int excl = sWarp[wid] + incl - v;
+    total = sTotal;
+    __syncthreads();
+    return excl;
+  }
+
+  // =============================================================== reset
+  __global__ void kResetEvent(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nMod = es.nModules, nLower = es.nLowerModules;
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2u * nMod; i += gridDim.x * blockDim.x) {
+      ev.hits.hitRanges[i] = -1;
+      ev.rg.mdRanges[i] = -1;
+      ev.rg.segmentRanges[i] = -1;
+      ev.rg.tripletRanges[i] = -1;
+      ev.rg.quintupletRanges[i] = -1;
+      if (i < nMod) {
+        ev.hits.hitRangesLower[i] = -1;
+        ev.hits.hitRangesUpper[i] = -1;
+        ev.hits.hitRangesnLower[i] = -1;
+        ev.hits.hitRangesnUpper[i] = -1;
+      }
+      if (i <= nLower) {
+        ev.md.nMDs[i] = 0;
+        ev.md.totOccupancyMDs[i] = 0;
+        ev.ls.nSegments[i] = 0;
+        ev.ls.totOccupancySegments[i] = 0;
+        ev.rg.miniDoubletModuleIndices[i] = es.mdOffset[i];
+        ev.rg.miniDoubletModuleOccupancy[i] = es.mdCap[i];
+        ev.rg.segmentModuleIndices[i] = es.lsOffset[i];
+        ev.rg.segmentModuleOccupancy[i] = es.lsCap[i];
+      }
+      if (i < nLower) {
+        ev.t3.nTriplets[i] = 0;
+        ev.t3.totOccupancyTriplets[i] = 0;
+        ev.t5.nQuintuplets[i] = 0;
+        ev.t5.totOccupancyQuintuplets[i] = 0;
+        ev.rg.quintupletModuleIndices[i] = -1;
+        ev.rg.quintupletModuleOccupancy[i] = 0;
+        ev.rg.tripletModuleIndices[i] = 0;
+        ev.rg.tripletModuleOccupancy[i] = 0;
+      }
+      if (i == 0) {
+        ev.sc->status = 0;
+        ev.sc->nPT5Total = 0;
+        ev.sc->nPT3Total = 0;
+        *ev.pt3.nPixelTriplets = 0;
+        *ev.pt3.totOccupancyPixelTriplets = 0;
+        *ev.pt5.nPixelQuintuplets = 0;
+        *ev.pt5.totOccupancyPixelQuintuplets = 0;
+        *ev.tc.nTrackCandidates = 0;
+        *ev.tc.nTrackCandidatespT3 = 0;
+        *ev.tc.nTrackCandidatespT5 = 0;
+        *ev.tc.nTrackCandidatespLS = 0;
+        *ev.tc.nTrackCandidatesT5 = 0;
+        *ev.rg.nEligibleT5Modules = 0;
+        *ev.rg.device_nTotalMDs = es.mdOffset[nLower];
+        *ev.rg.device_nTotalSegs = es.lsOffset[nLower];
+        *ev.rg.device_nTotalTrips = 0;
+        *ev.rg.device_nTotalQuints = 0;
+      }
+    }
+  }
+
+  // ================================================================ hits
+  // SDL/Hit.h:217-269
+  __global__ void kHitPrep(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nHits = ev.sc->nHits;
+    const Modules& m = es.m;
+    Hits h = ev.hits;
+    for (unsigned int ihit = blockIdx.x * blockDim.x + threadIdx.x; ihit < nHits; ihit += gridDim.x * blockDim.x) {
+      float x = h.xs[ihit], y = h.ys[ihit], z = h.zs[ihit];
+      unsigned int detId = h.detid[ihit];
+      float rt = fsqrt(x * x + y * y);
+      h.rts[ihit] = rt;
+      h.phis[ihit] = phiOf(x, y);
+      h.etas[ihit] = ((z > 0) - (z < 0)) * facosh(fsqrt(x * x + y * y + z * z) / rt);
+      float hex = 0.f, hey = 0.f, lex = 0.f, ley = 0.f;
+      int found = sortedFind(m.mapdetId, detId, es.nModules);
+      if (found < 0) {
+        atomicOr(&ev.sc->status, kStatusUnknownDetId);
+        h.moduleIndices[ihit] = 0xffff;
+        h.highEdgeXs[ihit] = hex;
+        h.highEdgeYs[ihit] = hey;
+        h.lowEdgeXs[ihit] = lex;
+        h.lowEdgeYs[ihit] = ley;
+        continue;
+      }
+      uint16_t mi = m.mapIdx[found];
+      h.moduleIndices[ihit] = mi;
+      if (m.subdets[mi] == Endcap && m.moduleType[mi] == TwoS) {
+        int f = sortedFind(m.geoMapDetId, detId, m.nEndCapMap);
+        if (f < 0) {
+          atomicOr(&ev.sc->status, kStatusUnknownEndcapDetId);
+        } else {
+          float phi = m.geoMapPhi[f];
+          float cos_phi = fcos(phi);
+          hex = x + 2.5f * cos_phi;
+          lex = x - 2.5f * cos_phi;
+          float sin_phi = fsin(phi);
+          hey = y + 2.5f * sin_phi;
+          ley = y - 2.5f * sin_phi;
+        }
+      }
+      h.highEdgeXs[ihit] = hex;
+      h.highEdgeYs[ihit] = hey;
+      h.lowEdgeXs[ihit] = lex;
+      h.lowEdgeYs[ihit] = ley;
+      int old = atomicCAS(&h.hitRanges[mi * 2], -1, static_cast<int>(ihit));
+      if (old != -1)
+        atomicMin(&h.hitRanges[mi * 2], static_cast<int>(ihit));
+      atomicMax(&h.hitRanges[mi * 2 + 1], static_cast<int>(ihit));
+    }
+  }
+
+  // SDL/Hit.h:194-215
+  __global__ void kModuleRanges(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    Hits h = ev.hits;
+    for (unsigned int lower = blockIdx.x * blockDim.x + threadIdx.x; lower < es.nLowerModules;
+         lower += gridDim.x * blockDim.x) {
+      uint16_t upper = es.m.partnerModuleIndices[lower];
+      if (h.hitRanges[lower * 2] != -1 && h.hitRanges[upper * 2] != -1) {
+        h.hitRangesLower[lower] = h.hitRanges[lower * 2];
+        h.hitRangesUpper[lower] = h.hitRanges[upper * 2];
+        h.hitRangesnLower[lower] = static_cast<int8_t>(h.hitRanges[lower * 2 + 1] - h.hitRanges[lower * 2] + 1);
+        h.hitRangesnUpper[lower] = static_cast<int8_t>(h.hitRanges[upper * 2 + 1] - h.hitRanges[upper * 2] + 1);
+      }
+    }
+  }
+
+  // ========================================================= pixel segments
+  // SDL/Segment.h:1031-1117
+  __global__ void kPixelIngest(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nPLS = ev.sc->nPLS;
+    const uint16_t pix = es.pixelModule;
+    MiniDoublets md = ev.md;
+    Segments ls = ev.ls;
+    const unsigned int mdBase = es.mdOffset[es.nLowerModules];
+    const unsigned int lsBase = es.lsOffset[es.nLowerModules];
+    const unsigned int nHits = ev.sc->nHits;
+    for (unsigned int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < nPLS; tid += gridDim.x * blockDim.x) {
+      unsigned int hit[4] = {ev.plsHit0[tid], ev.plsHit1[tid], ev.plsHit2[tid], ev.plsHit3[tid]};
+      // The reference indexes the hit store with these unchecked; an index
+      // outside the event is flagged and replaced by hit 0 (the host rejects
+      // pixel segments for events without hits).
+      for (int k = 0; k < 4; ++k)
+        if (hit[k] >= nHits) {
+          atomicOr(&ev.sc->status, kStatusInvalidInput);
+          hit[k] = 0;
+        }
+      storePixelSegment(
+          es.m, ev.hits, md, ls, pix, mdBase, lsBase, tid, hit[0], hit[1], hit[2], hit[3], ev.plsDPhiChange[tid]);
+      ls.partOfPT5[tid] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      md.nMDs[pix] = 2 * nPLS;
+      md.totOccupancyMDs[pix] = 2 * nPLS;
+      ls.nSegments[pix] = nPLS;
+      ls.totOccupancySegments[pix] = nPLS;
+    }
+  }
+
+  // ======================================================== mini-doublets
+  // One warp per lower module (SDL/MiniDoublet.h:896-992).
+  __device__ __forceinline__ void mdModule(DeviceES const& es, const EventView& ev, uint16_t lm) {
+    const Hits& h = ev.hits;
+    if (h.hitRangesLower[lm] == -1)
+      return;
+    const int nLowerHits = h.hitRangesnLower[lm];
+    const int nUpperHits = h.hitRangesnUpper[lm];
+    const unsigned int upHit0 = h.hitRangesUpper[lm];
+    const unsigned int loHit0 = h.hitRangesLower[lm];
+    const int limit = nUpperHits * nLowerHits;
+    const int cap = es.mdCap[lm];
+    const unsigned int base = es.mdOffset[lm];
+    MiniDoublets md = ev.md;
+    unsigned int count = 0;
+    for (int start = 0; start < limit; start += 32) {
+      int hitIndex = start + int(laneId());
+      bool ok = false;
+      MDValues v;
+      unsigned int lowerIdx = 0, upperIdx = 0;
+      if (hitIndex < limit) {
+        int lowerHitIndex = hitIndex / nUpperHits;
+        int upperHitIndex = hitIndex % nUpperHits;
+        if (!(upperHitIndex >= nUpperHits) && !(lowerHitIndex >= nLowerHits)) {
+          lowerIdx = loHit0 + lowerHitIndex;
+          upperIdx = upHit0 + upperHitIndex;
+          ok = mdSelect(es.m,
+                        lm,
+                        h.xs[lowerIdx],
+                        h.ys[lowerIdx],
+                        h.zs[lowerIdx],
+                        h.rts[lowerIdx],
+                        h.xs[upperIdx],
+                        h.ys[upperIdx],
+                        h.zs[upperIdx],
+                        h.rts[upperIdx],
+                        v);
+        }
+      }
+      unsigned int tot;
+      unsigned int r = count + warpRank(ok, tot);
+      if (ok && int(r) < cap)
+        storeMD(es.m, h, md, lowerIdx, upperIdx, lm, v, base + r);
+      count += tot;
+    }
+    if (laneId() == 0) {
+      md.nMDs[lm] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
+      md.totOccupancyMDs[lm] = count;
+      if (int(count) > cap)
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
+    }
+  }
+
+  __global__ void kCreateMD(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const int wpb = blockDim.x >> 5;
+    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < es.nLowerModules; w += gridDim.x * wpb) {
+      __syncwarp();
+      mdModule(es, ev, static_cast<uint16_t>(w));
+    }
+  }
+
+  // SDL/MiniDoublet.h:1084-1104
+  __global__ void kMDRanges(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < es.nLowerModules; i += gridDim.x * blockDim.x) {
+      if (ev.md.nMDs[i] == 0 or ev.hits.hitRanges[i * 2] == -1) {
+        ev.rg.mdRanges[i * 2] = -1;
+        ev.rg.mdRanges[i * 2 + 1] = -1;
+      } else {
+        ev.rg.mdRanges[i * 2] = es.mdOffset[i];
+        ev.rg.mdRanges[i * 2 + 1] = es.mdOffset[i] + ev.md.nMDs[i] - 1;
+      }
+    }
+  }
+
+  // ======================================================== line segments
+  // One warp per inner lower module walking (connected module, inner MD,
+  // outer MD) in order (SDL/Segment.h:798-910).
+  constexpr int kLSWarps = 4;
+  __device__ __forceinline__ void lsModule(
+      DeviceES const& es, const EventView& ev, uint16_t lm, unsigned int* pre, uint16_t* outer) {
+    const unsigned int nInnerMDs = ev.md.nMDs[lm];
+    if (nInnerMDs == 0)
+      return;
+    const Modules& m = es.m;
+    const int nConn = m.nConnectedModules[lm];
+    for (int k = laneId(); k < nConn; k += 32)
+      outer[k] = m.moduleMap[lm * kMaxConnectedModules + k];
+    __syncwarp();
+    const unsigned int total =
+        warpPrefix(pre, nConn, [&](int k) { return nInnerMDs * ev.md.nMDs[outer[k]]; });
+    const int cap = es.lsCap[lm];
+    const unsigned int base = es.lsOffset[lm];
+    const unsigned int innerBase = es.mdOffset[lm];
+    Segments ls = ev.ls;
+    unsigned int count = 0;
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      LSValues v;
+      unsigned int innerMD = 0, outerMD = 0;
+      uint16_t outerLM = 0;
+      if (f < total) {
+        int k = findSlot(pre, nConn, f);
+        outerLM = outer[k];
+        unsigned int nOuterMDs = ev.md.nMDs[outerLM];
+        unsigned int local = f - pre[k];
+        innerMD = innerBase + local / nOuterMDs;
+        outerMD = es.mdOffset[outerLM] + local % nOuterMDs;
+        ok = lsSelect(m, ev.md, lm, outerLM, innerMD, outerMD, v);
+      }
+      unsigned int tot;
+      unsigned int r = count + warpRank(ok, tot);
+      if (ok && int(r) < cap)
+        storeLS(ls, ev.md, innerMD, outerMD, lm, outerLM, v, base + r);
+      count += tot;
+    }
+    if (laneId() == 0) {
+      ls.nSegments[lm] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
+      ls.totOccupancySegments[lm] = count;
+      if (int(count) > cap)
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
+    }
+  }
+
+  __global__ void kCreateLS(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sPre[kLSWarps][kMaxConnectedModules + 1];
+    __shared__ uint16_t sOuter[kLSWarps][kMaxConnectedModules];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    for (int w = blockIdx.x * kLSWarps + wib; w < es.nLowerModules; w += gridDim.x * kLSWarps) {
+      __syncwarp();
+      lsModule(es, ev, static_cast<uint16_t>(w), sPre[wib], sOuter[wib]);
+    }
+  }
+
+  // SDL/Segment.h:1010-1029
+  __global__ void kLSRanges(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < es.nLowerModules; i += gridDim.x * blockDim.x) {
+      if (ev.ls.nSegments[i] == 0) {
+        ev.rg.segmentRanges[i * 2] = -1;
+        ev.rg.segmentRanges[i * 2 + 1] = -1;
+      } else {
+        ev.rg.segmentRanges[i * 2] = es.lsOffset[i];
+        ev.rg.segmentRanges[i * 2 + 1] = es.lsOffset[i] + ev.ls.nSegments[i] - 1;
+      }
+    }
+  }
+
+  // ============================================================ triplets
+  // Per-module triplet offsets (SDL/Triplet.h:1007-1102); one block per event.
+  __global__ void kT3Offsets(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int occ = 0;
+      bool valid = i < es.nLowerModules;
+      if (valid && ev.ls.nSegments[i] != 0)
+        occ = static_cast<unsigned int>(es.t3CapIfUsed[i]);
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(occ, tot);
+      if (valid) {
+        ev.rg.tripletModuleIndices[i] = static_cast<int>(carry + ex);
+        ev.rg.tripletModuleOccupancy[i] = static_cast<int>(occ);
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0)
+      *ev.rg.device_nTotalTrips = carry;
+  }
+
+  // One warp per inner-inner lower module walking (inner segment, outer
+  // segment of the middle module) in order (SDL/Triplet.h:874-1005).
+  constexpr int kT3Warps = 4;
+  constexpr int kT3MaxInner = 1024;
+  __device__ __forceinline__ void t3Module(DeviceES const& es, const EventView& ev, uint16_t lm1, unsigned int* pre) {
+    const Modules& m = es.m;
+    if (m.nConnectedModules[lm1] == 0)
+      return;
+    const unsigned int nInner = ev.ls.nSegments[lm1];
+    if (nInner == 0)
+      return;
+    const unsigned int segBase = es.lsOffset[lm1];
+    const Segments& ls = ev.ls;
+    const unsigned int total = warpPrefix(pre, int(nInner), [&](int i) {
+      uint16_t middle = ls.outerLowerModuleIndices[segBase + i];
+      return ls.nSegments[middle];
+    });
+    const int cap = ev.rg.tripletModuleOccupancy[lm1];
+    const unsigned int base = ev.rg.tripletModuleIndices[lm1];
+    Triplets t3 = ev.t3;
+    unsigned int count = 0;
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      T3Values v;
+      unsigned int innerSeg = 0, outerSeg = 0;
+      uint16_t middle = 0, outerOuter = 0;
+      if (f < total) {
+        int i = findSlot(pre, int(nInner), f);
+        innerSeg = segBase + i;
+        middle = ls.outerLowerModuleIndices[innerSeg];
+        outerSeg = es.lsOffset[middle] + (f - pre[i]);
+        outerOuter = ls.outerLowerModuleIndices[outerSeg];
+        ok = t3Select(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg, v);
+      }
+      unsigned int tot;
+      unsigned int r = count + warpRank(ok, tot);
+      if (ok && int(r) < cap)
+        storeT3(m, ev.md, ls, t3, innerSeg, outerSeg, lm1, middle, outerOuter, v, base + r);
+      count += tot;
+    }
+    if (laneId() == 0) {
+      t3.nTriplets[lm1] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
+      t3.totOccupancyTriplets[lm1] = count;
+      if (int(count) > cap)
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
+    }
+  }
+
+  __global__ void kCreateT3(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sPre[kT3Warps][kT3MaxInner + 1];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    for (int w = blockIdx.x * kT3Warps + wib; w < es.nLowerModules; w += gridDim.x * kT3Warps) {
+      __syncwarp();
+      t3Module(es, ev, static_cast<uint16_t>(w), sPre[wib]);
+    }
+  }
+
+  // SDL/Triplet.h:1104-1122
+  __global__ void kT3Ranges(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < es.nLowerModules; i += gridDim.x * blockDim.x) {
+      if (ev.t3.nTriplets[i] == 0) {
+        ev.rg.tripletRanges[i * 2] = -1;
+        ev.rg.tripletRanges[i * 2 + 1] = -1;
+      } else {
+        ev.rg.tripletRanges[i * 2] = ev.rg.tripletModuleIndices[i];
+        ev.rg.tripletRanges[i * 2 + 1] = ev.rg.tripletModuleIndices[i] + ev.t3.nTriplets[i] - 1;
+      }
+    }
+  }
+
+  // ========================================================= quintuplets
+  // Eligible T5 seed modules and their offsets (SDL/Quintuplet.h:3117-3213).
+  __global__ void kT5Eligible(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    unsigned int carryN = 0, carryQ = 0;
+    for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      bool valid = i < es.nLowerModules;
+      bool elig = valid && ev.t3.nTriplets[i] != 0 && es.t5CapIfEligible[i] >= 0;
+      unsigned int occ = elig ? static_cast<unsigned int>(es.t5CapIfEligible[i]) : 0u;
+      unsigned int totN, totQ;
+      unsigned int exN = blockExclusiveScan(elig ? 1u : 0u, totN);
+      unsigned int exQ = blockExclusiveScan(occ, totQ);
+      if (elig) {
+        ev.rg.indicesOfEligibleT5Modules[carryN + exN] = static_cast<uint16_t>(i);
+        ev.rg.quintupletModuleIndices[i] = static_cast<int>(carryQ + exQ);
+        ev.rg.quintupletModuleOccupancy[i] = static_cast<int>(occ);
+      }
+      carryN += totN;
+      carryQ += totQ;
+    }
+    if (threadIdx.x == 0) {
+      *ev.rg.nEligibleT5Modules = static_cast<uint16_t>(carryN);
+      *ev.rg.device_nTotalQuints = carryQ;
+    }
+  }
+
+  // One warp per eligible module walking (inner T3, outer T3) in order
+  // (SDL/Quintuplet.h:2988-3115).
+  constexpr int kT5Warps = 4;
+  constexpr int kT5MaxInner = 1024;
+  __device__ __forceinline__ void t5Module(
+      DeviceES const& es, const EventView& ev, uint16_t lm1, unsigned int* pre, bool useDnn) {
+    const Modules& m = es.m;
+    const int layer = m.layers[lm1];
+    if (layer != 1 && layer != 2)
+      return;
+    const unsigned int nInner = ev.t3.nTriplets[lm1];
+    const unsigned int t3Base = ev.rg.tripletModuleIndices[lm1];
+    const Triplets& t3r = ev.t3;
+    const unsigned int total = warpPrefix(pre, int(nInner), [&](int i) {
+      uint16_t lm3 = t3r.lowerModuleIndices[3 * (t3Base + i) + 2];
+      return t3r.nTriplets[lm3];
+    });
+    const int cap = ev.rg.quintupletModuleOccupancy[lm1];
+    const unsigned int base = ev.rg.quintupletModuleIndices[lm1];
+    Triplets t3 = ev.t3;
+    Quintuplets t5 = ev.t5;
+    ConstDnn dnn;
+    unsigned int count = 0;
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      T5Values v;
+      unsigned int innerT3 = 0, outerT3 = 0;
+      uint16_t lm[5] = {lm1, 0, 0, 0, 0};
+      if (f < total) {
+        int i = findSlot(pre, int(nInner), f);
+        innerT3 = t3Base + i;
+        lm[1] = t3.lowerModuleIndices[3 * innerT3 + 1];
+        lm[2] = t3.lowerModuleIndices[3 * innerT3 + 2];
+        outerT3 = ev.rg.tripletModuleIndices[lm[2]] + (f - pre[i]);
+        lm[3] = t3.lowerModuleIndices[3 * outerT3 + 1];
+        lm[4] = t3.lowerModuleIndices[3 * outerT3 + 2];
+        ok = t5Select(m, ev.md, ev.ls, t3, dnn.get(), useDnn, lm, innerT3, outerT3, v);
+      }
+      unsigned int tot;
+      unsigned int r = count + warpRank(ok, tot);
+      if (ok && int(r) < cap)
+        storeT5(ev.md, ev.ls, t3, t5, innerT3, outerT3, lm, layer, v, base + r);
+      count += tot;
+    }
+    if (laneId() == 0) {
+      t5.nQuintuplets[lm1] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
+      t5.totOccupancyQuintuplets[lm1] = count;
+      if (int(count) > cap)
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
+    }
+  }
+
+  __global__ void kCreateT5(DeviceES es, const EventView* evs, bool useDnn) {
+    __shared__ unsigned int sPre[kT5Warps][kT5MaxInner + 1];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    for (int w = blockIdx.x * kT5Warps + wib; w < nE; w += gridDim.x * kT5Warps) {
+      __syncwarp();
+      t5Module(es, ev, ev.rg.indicesOfEligibleT5Modules[w], sPre[wib], useDnn);
+    }
+  }
+
+  // Number of hits two T5s share (SDL/Kernels.h:42-84).
+  LST_DEV int sharedHitsT5(const Quintuplets& q, unsigned int ix, unsigned int jx) {
+    int nMatched = 0;
+    for (int i = 0; i < 10; i++) {
+      unsigned int a = q.hitIndices[10 * ix + i];
+      bool matched = false;
+      for (int j = 0; j < 10; j++)
+        if (a == q.hitIndices[10 * jx + j]) {
+          matched = true;
+          break;
+        }
+      if (matched)
+        nMatched++;
+    }
+    return nMatched;
+  }
+
+  // Duplicate removal among the T5s of one module (SDL/Kernels.h:202-249);
+  // one warp per module, only ever setting bit 1.
+  __global__ void kT5DedupAfterBuild(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= es.nLowerModules)
+      return;
+    const unsigned int n = ev.t5.nQuintuplets[warp];
+    if (n < 2)
+      return;
+    const unsigned int base = ev.rg.quintupletModuleIndices[warp];
+    Quintuplets q = ev.t5;
+    for (unsigned int ix1 = laneId(); ix1 < n; ix1 += 32) {
+      unsigned int ix = base + ix1;
+      float eta1 = q.eta[ix], phi1 = q.phi[ix], score1 = q.score_rphisum[ix];
+      for (unsigned int jx1 = ix1 + 1; jx1 < n; jx1++) {
+        unsigned int jx = base + jx1;
+        float eta2 = q.eta[jx], phi2 = q.phi[jx];
+        float dEta = fabs_(eta1 - eta2);
+        float dPhi = wrapDPhi(phi1, phi2);
+        float score2 = q.score_rphisum[jx];
+        if (dEta > 0.1f)
+          continue;
+        if (fabs_(dPhi) > 0.1f)
+          continue;
+        if (sharedHitsT5(q, ix, jx) >= 7) {
+          if (score1 >= score2)
+            q.isDup[ix] = 1;
+          else
+            q.isDup[jx] = 1;
+        }
+      }
+    }
+  }
+
+  // SDL/Quintuplet.h:3215-3235
+  __global__ void kT5Ranges(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < es.nLowerModules; i += gridDim.x * blockDim.x) {
+      if (ev.t5.nQuintuplets[i] == 0 or ev.rg.quintupletModuleIndices[i] == -1) {
+        ev.rg.quintupletRanges[i * 2] = -1;
+        ev.rg.quintupletRanges[i * 2 + 1] = -1;
+      } else {
+        ev.rg.quintupletRanges[i * 2] = ev.rg.quintupletModuleIndices[i];
+        ev.rg.quintupletRanges[i * 2 + 1] = ev.rg.quintupletModuleIndices[i] + ev.t5.nQuintuplets[i] - 1;
+      }
+    }
+  }
+
+  // ==================================================== pLS cleaning
+  // SDL/Kernels.h:384-473.  Pass 1 sets bit 1 of isDup directly; pass 2 marks
+  // plsFlag and kMergePLSFlag folds it into bit 2 afterwards, so that pass 2
+  // reads the pass-1 bit while other threads mark removals.
+  __global__ void kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
+    const EventView& ev = evs[blockIdx.y];
+    unsigned int nPix = ev.ls.nSegments[es.pixelModule];
+    if (nPix > kMaxPixelSegments)
+      nPix = kMaxPixelSegments;
+    const Segments& s = ev.ls;
+    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < nPix; ix += gridDim.x * blockDim.x) {
+      if (secondpass && (!s.isQuad[ix] || (s.isDup[ix] & 1)))
+        continue;
+      unsigned int phits1[4] = {s.pLSHitsIdxs[4 * ix], s.pLSHitsIdxs[4 * ix + 1], s.pLSHitsIdxs[4 * ix + 2],
+                                s.pLSHitsIdxs[4 * ix + 3]};
+      float eta_pix1 = s.eta[ix];
+      float phi_pix1 = s.phi[ix];
+      for (unsigned int jx = ix + 1; jx < nPix; jx++) {
+        float eta_pix2 = s.eta[jx];
+        float phi_pix2 = s.phi[jx];
+        if (fabs_(eta_pix2 - eta_pix1) > 0.1f)
+          continue;
+        if (secondpass && (!s.isQuad[jx] || (s.isDup[jx] & 1)))
+          continue;
+        int8_t quad_diff = s.isQuad[ix] - s.isQuad[jx];
+        float score_diff = s.score[ix] - s.score[jx];
+        unsigned int idxToRemove;
+        if (quad_diff > 0)
+          idxToRemove = jx;
+        else if (quad_diff < 0)
+          idxToRemove = ix;
+        else if (score_diff < 0)
+          idxToRemove = jx;
+        else if (score_diff > 0)
+          idxToRemove = ix;
+        else
+          idxToRemove = ix;
+        int npMatched = 0;
+        for (int i = 0; i < 4; i++) {
+          bool pmatched = false;
+          for (int j = 0; j < 4; j++) {
+            if (phits1[i] == s.pLSHitsIdxs[4 * jx + j]) {
+              pmatched = true;
+              break;
+            }
+          }
+          if (pmatched) {
+            npMatched++;
+            if (secondpass)
+              break;
+          }
+        }
+        bool remove = npMatched >= 3;
+        if (secondpass) {
+          float dEta = fabs_(eta_pix1 - eta_pix2);
+          float dPhi = wrapDPhi(phi_pix1, phi_pix2);
+          float dR2 = dEta * dEta + dPhi * dPhi;
+          if ((npMatched >= 1) || (dR2 < 1e-5f))
+            remove = true;
+        }
+        if (remove) {
+          if (secondpass)
+            ev.plsFlag[idxToRemove] = 1;
+          else
+            s.isDup[idxToRemove] = 1;
+        }
+      }
+    }
+  }
+
+  __global__ void kMergePLSFlag(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    unsigned int nPix = ev.ls.nSegments[es.pixelModule];
+    if (nPix > kMaxPixelSegments)
+      nPix = kMaxPixelSegments;
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPix; i += gridDim.x * blockDim.x) {
+      if (ev.plsFlag[i]) {
+        ev.ls.isDup[i] |= 2;
+        ev.plsFlag[i] = 0;
+      }
+    }
+  }
+
+  // ============================================ pixel-map slices per pLS
+  // SDL/Event.cc:1055-1080
+  __global__ void kPixelConnect(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPLS; i += gridDim.x * blockDim.x) {
+      int8_t pixelType = ev.ls.pixelType[i];
+      int superbin = ev.ls.superbin[i];
+      unsigned int size = 0, index = 0;
+      if (!((superbin < 0) or (superbin >= int(kSizeSuperbins)) or (pixelType > 2) or (pixelType < 0))) {
+        if (pixelType == 0) {
+          size = es.cpSizes[superbin];
+          index = es.cpIndex[superbin];
+        } else if (pixelType == 1) {
+          size = es.cpSizesPos[superbin];
+          index = es.cpIndexPos[superbin] + es.pixelIndexOffsetPos;
+        } else {
+          size = es.cpSizesNeg[superbin];
+          index = es.cpIndexNeg[superbin] + es.pixelIndexOffsetNeg;
+        }
+      }
+      ev.plsConnSize[i] = size;
+      ev.plsConnIndex[i] = index;
+    }
+  }
+
+  // ============================================================== pT5
+  // Candidate modules of a pLS for pT5 (SDL/PixelTriplet.h:2697-2716).
+  __device__ __forceinline__ unsigned int pt5ModuleCount(DeviceES const& es, const EventView& ev, uint16_t mod) {
+    if (mod >= es.nLowerModules)
+      return 0;
+    if (es.m.moduleType[mod] == TwoS)
+      return 0;
+    return ev.t5.nQuintuplets[mod];
+  }
+
+  // Walks the pT5 candidates of one pLS in order; emit selects the pass:
+  // count passing candidates, or store those with global rank < cap.
+  constexpr int kPixWarps = 4;
+  template <bool kEmit>
+  __device__ __forceinline__ void pt5Walk(DeviceES const& es, const EventView& ev, unsigned int iPLS, unsigned int* pre,
+                                          uint16_t* mods) {
+    if (ev.ls.isDup[iPLS])
+      return;
+    const unsigned int nConn = ev.plsConnSize[iPLS];
+    const unsigned int cidx = ev.plsConnIndex[iPLS];
+    for (unsigned int k = laneId(); k < nConn; k += 32)
+      mods[k] = static_cast<uint16_t>(es.m.connectedPixels[cidx + k]);
+    __syncwarp();
+    const unsigned int total = warpPrefix(pre, int(nConn), [&](int k) { return pt5ModuleCount(es, ev, mods[k]); });
+    const unsigned int plsIndex = es.lsOffset[es.nLowerModules] + iPLS;
+    unsigned int count = 0;
+    unsigned int rankBase = kEmit ? ev.plsOffset[iPLS] : 0u;
+    Segments ls = ev.ls;
+    Triplets t3 = ev.t3;
+    Quintuplets t5 = ev.t5;
+    PixelQuintuplets pt5 = ev.pt5;
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      PT5Values v;
+      unsigned int t5i = 0;
+      if (f < total) {
+        int k = findSlot(pre, int(nConn), f);
+        t5i = ev.rg.quintupletModuleIndices[mods[k]] + (f - pre[k]);
+        if (!t5.isDup[t5i])
+          ok = pt5Select(es.m, ev.rg, ev.md, ls, t3, t5, plsIndex, t5i, iPLS, v);
+      }
+      unsigned int tot;
+      unsigned int r = rankBase + count + warpRank(ok, tot);
+      if (kEmit && ok && r < kMaxPixelQuintuplets)
+        storePT5(ev.md, ls, t3, t5, pt5, plsIndex, iPLS, t5i, v, r);
+      count += tot;
+    }
+    if (!kEmit && laneId() == 0)
+      ev.plsCount[iPLS] = count;
+  }
+
+  __global__ void kPT5Count(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
+    __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
+      __syncwarp();
+      if (laneId() == 0)
+        ev.plsCount[i] = 0;
+      pt5Walk<false>(es, ev, i, sPre[wib], sMods[wib]);
+    }
+  }
+
+  __global__ void kPT5Emit(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
+    __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
+      __syncwarp();
+      if (ev.plsCount[i] == 0 || ev.plsOffset[i] >= kMaxPixelQuintuplets)
+        continue;
+      pt5Walk<true>(es, ev, i, sPre[wib], sMods[wib]);
+    }
+  }
+
+  // Exclusive scan of the per-pLS pass counts; one block per event.
+  // which = 0: pT5 (cap 15000), 1: pT3 (cap 5000).
+  __global__ void kPLSScan(DeviceES es, const EventView* evs, int which) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = ev.ls.nSegments[es.pixelModule];
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int c = (i < n) ? ev.plsCount[i] : 0u;
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(c, tot);
+      if (i < n)
+        ev.plsOffset[i] = carry + ex;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      if (which == 0) {
+        ev.sc->nPT5Total = carry;
+        *ev.pt5.totOccupancyPixelQuintuplets = carry;
+        *ev.pt5.nPixelQuintuplets = carry < kMaxPixelQuintuplets ? carry : kMaxPixelQuintuplets;
+      } else {
+        ev.sc->nPT3Total = carry;
+        *ev.pt3.totOccupancyPixelTriplets = carry;
+        *ev.pt3.nPixelTriplets = carry < kMaxPixelTriplets ? carry : kMaxPixelTriplets;
+      }
+      if ((which == 0 && carry > kMaxPixelQuintuplets) || (which == 1 && carry > kMaxPixelTriplets))
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
+    }
+  }
+
+  // Number of hits two pT5s share (SDL/Kernels.h:86-136).
+  LST_DEV int sharedHitsPT5(const PixelQuintuplets& p, unsigned int ix, unsigned int jx) {
+    int nMatched = 0;
+    for (int i = 0; i < 14; i++) {
+      unsigned int a = p.hitIndices[14 * ix + i];
+      bool matched = false;
+      for (int j = 0; j < 14; j++)
+        if (a == p.hitIndices[14 * jx + j]) {
+          matched = true;
+          break;
+        }
+      if (matched)
+        nMatched++;
+    }
+    return nMatched;
+  }
+
+  // SDL/Kernels.h:358-382
+  __global__ void kPT5Dedup(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.pt5.nPixelQuintuplets;
+    PixelQuintuplets p = ev.pt5;
+    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < n; ix += gridDim.x * blockDim.x) {
+      float score1 = p.score[ix];
+      for (unsigned int jx = 0; jx < n; jx++) {
+        if (ix == jx)
+          continue;
+        int nMatched = sharedHitsPT5(p, ix, jx);
+        float score2 = p.score[jx];
+        if (nMatched >= 7) {
+          if (score1 > score2 or ((score1 == score2) and (ix > jx))) {
+            p.isDup[ix] = 1;
+            break;
+          }
+        }
+      }
+    }
+  }
+
+  // Writes a track candidate built from a pT3 / T5 / pT5 record
+  // (SDL/TrackCandidate.h:130-163); unused slots are zeroed.
+  LST_DEV void storeTC(TrackCandidates& tc,
+                       short type,
+                       unsigned int innerIdx,
+                       unsigned int outerIdx,
+                       const uint8_t* logicalLayers,
+                       const uint16_t* lowerModules,
+                       const unsigned int* hitIndices,
+                       int pixelSeedIndex,
+                       float centerX,
+                       float centerY,
+                       float radius,
+                       unsigned int idx,
+                       unsigned int directIdx) {
+    tc.trackCandidateType[idx] = type;
+    tc.directObjectIndices[idx] = directIdx;
+    tc.pixelSeedIndex[idx] = pixelSeedIndex;
+    tc.objectIndices[2 * idx] = innerIdx;
+    tc.objectIndices[2 * idx + 1] = outerIdx;
+    const int limits = type == 7 ? 7 : 5;
+    for (int i = 0; i < 7; i++) {
+      tc.logicalLayers[7 * idx + i] = i < limits ? logicalLayers[i] : 0;
+      tc.lowerModuleIndices[7 * idx + i] = i < limits ? lowerModules[i] : 0;
+    }
+    for (int i = 0; i < 14; i++)
+      tc.hitIndices[14 * idx + i] = i < 2 * limits ? hitIndices[i] : 0;
+    tc.centerX[idx] = centerX;
+    tc.centerY[idx] = centerY;
+    tc.radius[idx] = radius;
+  }
+
+  // pT5 -> TC (SDL/TrackCandidate.h:531-581); one block per event.
+  __global__ void kAddPT5TC(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.pt5.nPixelQuintuplets;
+    const unsigned int pLS_offset = es.lsOffset[es.nLowerModules];
+    const unsigned int start = *ev.tc.nTrackCandidates;
+    TrackCandidates tc = ev.tc;
+    PixelQuintuplets p = ev.pt5;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      bool f = i < n && !p.isDup[i];
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(f ? 1u : 0u, tot);
+      unsigned int idx = start + carry + ex;
+      if (f && idx < kMaxPixelTrackCandidates) {
+        float radius = 0.5f * (p.pixelRadius[i] + p.quintupletRadius[i]);
+        unsigned int pix = p.pixelIndices[i];
+        storeTC(tc, 7, pix, p.T5Indices[i], &p.logicalLayers[7 * i], &p.lowerModuleIndices[7 * i], &p.hitIndices[14 * i],
+                static_cast<int>(ev.ls.seedIdx[pix - pLS_offset]), p.centerX[i], p.centerY[i], radius, idx, i);
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      unsigned int accepted = (start + carry <= kMaxPixelTrackCandidates) ? carry
+                              : (start < kMaxPixelTrackCandidates ? kMaxPixelTrackCandidates - start : 0u);
+      if (accepted < carry)
+        atomicOr(&ev.sc->status, kStatusTCTruncated);
+      *tc.nTrackCandidates = start + accepted;
+      *tc.nTrackCandidatespT5 += accepted;
+    }
+  }
+
+  // ============================================================== pT3
+  // Candidate modules of a pLS for pT3 (SDL/PixelTriplet.h:1046-1081).
+  __device__ __forceinline__ unsigned int pt3ModuleCount(DeviceES const& es, const EventView& ev, uint16_t mod) {
+    if (mod >= es.nLowerModules)
+      return 0;
+    if (es.m.moduleType[mod] == TwoS)
+      return 0;
+    int layer = es.m.layers[mod];
+    if (layer != 1 && layer != 2)
+      return 0;
+    return ev.t3.nTriplets[mod];
+  }
+
+  template <bool kEmit>
+  __device__ __forceinline__ void pt3Walk(DeviceES const& es, const EventView& ev, unsigned int iPLS, unsigned int* pre,
+                                          uint16_t* mods) {
+    if (ev.ls.isDup[iPLS] || ev.ls.partOfPT5[iPLS])
+      return;
+    const unsigned int nConn = ev.plsConnSize[iPLS];
+    const unsigned int cidx = ev.plsConnIndex[iPLS];
+    for (unsigned int k = laneId(); k < nConn; k += 32)
+      mods[k] = static_cast<uint16_t>(es.m.connectedPixels[cidx + k]);
+    __syncwarp();
+    const unsigned int total = warpPrefix(pre, int(nConn), [&](int k) { return pt3ModuleCount(es, ev, mods[k]); });
+    const unsigned int plsIndex = es.lsOffset[es.nLowerModules] + iPLS;
+    unsigned int count = 0;
+    unsigned int rankBase = kEmit ? ev.plsOffset[iPLS] : 0u;
+    Triplets t3 = ev.t3;
+    PixelTriplets pt3 = ev.pt3;
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      PT3Values v;
+      unsigned int t3i = 0;
+      short adj = 0;
+      if (f < total) {
+        int k = findSlot(pre, int(nConn), f);
+        uint16_t mod = mods[k];
+        adj = es.m.layers[mod] == 1 ? 1 : 0;
+        t3i = ev.rg.tripletModuleIndices[mod] + (f - pre[k]);
+        if (es.m.moduleType[t3.lowerModuleIndices[3 * t3i + 1]] != TwoS && !t3.partOfPT5[t3i])
+          ok = pt3Select(es.m, ev.rg, ev.md, ev.ls, t3, plsIndex, t3i, true, v);
+      }
+      unsigned int tot;
+      unsigned int r = rankBase + count + warpRank(ok, tot);
+      if (kEmit && ok && r < kMaxPixelTriplets) {
+        storePT3(es.m, ev.md, ev.ls, t3, pt3, plsIndex, iPLS, t3i, adj, v, r);
+        t3.partOfPT3[t3i] = 1;
+      }
+      count += tot;
+    }
+    if (!kEmit && laneId() == 0)
+      ev.plsCount[iPLS] = count;
+  }
+
+  __global__ void kPT3Count(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
+    __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
+      __syncwarp();
+      if (laneId() == 0)
+        ev.plsCount[i] = 0;
+      pt3Walk<false>(es, ev, i, sPre[wib], sMods[wib]);
+    }
+  }
+
+  __global__ void kPT3Emit(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
+    __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
+      __syncwarp();
+      if (ev.plsCount[i] == 0 || ev.plsOffset[i] >= kMaxPixelTriplets)
+        continue;
+      pt3Walk<true>(es, ev, i, sPre[wib], sMods[wib]);
+    }
+  }
+
+  // Shared pixel and outer hits of two pT3s (SDL/Kernels.h:138-200).
+  LST_DEV void sharedHitsPT3(const PixelTriplets& p, unsigned int ix, unsigned int jx, int& npMatched, int& nMatched) {
+    npMatched = 0;
+    for (int i = 0; i < 4; i++) {
+      int a = static_cast<int>(p.hitIndices[10 * ix + i]);
+      bool pm = false;
+      for (int j = 0; j < 4; j++)
+        if (a == static_cast<int>(p.hitIndices[10 * jx + j])) {
+          pm = true;
+          break;
+        }
+      if (pm)
+        npMatched++;
+    }
+    nMatched = 0;
+    for (int i = 0; i < 6; i++) {
+      int a = static_cast<int>(p.hitIndices[10 * ix + 4 + i]);
+      bool tm = false;
+      for (int j = 0; j < 6; j++)
+        if (a == static_cast<int>(p.hitIndices[10 * jx + 4 + j])) {
+          tm = true;
+          break;
+        }
+      if (tm)
+        nMatched++;
+    }
+  }
+
+  // SDL/Kernels.h:325-356
+  __global__ void kPT3Dedup(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.pt3.nPixelTriplets;
+    PixelTriplets p = ev.pt3;
+    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < n; ix += gridDim.x * blockDim.x) {
+      for (unsigned int jx = 0; jx < n; jx++) {
+        if (ix == jx)
+          continue;
+        int np, nm;
+        sharedHitsPT3(p, ix, jx, np, nm);
+        if ((np + nm) >= 5) {
+          uint8_t li = p.logicalLayers[5 * ix + 2], lj = p.logicalLayers[5 * jx + 2];
+          if (lj < li) {
+            p.isDup[ix] = 1;
+            break;
+          } else if (li == lj && p.score[ix] > p.score[jx]) {
+            p.isDup[ix] = 1;
+            break;
+          } else if (li == lj && (p.score[ix] == p.score[jx]) && (ix < jx)) {
+            p.isDup[ix] = 1;
+            break;
+          }
+        }
+      }
+    }
+  }
+
+  // ================================================== track candidates
+  // pT3 vs pT5 pixel eta/phi (SDL/TrackCandidate.h:204-243).
+  __global__ void kCrossCleanPT3(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nPT3 = *ev.pt3.nPixelTriplets;
+    const unsigned int nPT5 = *ev.pt5.nPixelQuintuplets;
+    const unsigned int prefix = es.lsOffset[es.nLowerModules];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPT3; i += gridDim.x * blockDim.x) {
+      if (ev.pt3.isDup[i])
+        continue;
+      float eta1 = ev.pt3.eta_pix[i], phi1 = ev.pt3.phi_pix[i];
+      for (unsigned int j = 0; j < nPT5; j++) {
+        unsigned int pLS_jx = ev.pt5.pixelIndices[j];
+        float eta2 = ev.ls.eta[pLS_jx - prefix];
+        float phi2 = ev.ls.phi[pLS_jx - prefix];
+        float dEta = fabs_(eta1 - eta2);
+        float dPhi = wrapDPhi(phi1, phi2);
+        float dR2 = dEta * dEta + dPhi * dPhi;
+        if (dR2 < 1e-5f)
+          ev.pt3.isDup[i] = 1;
+      }
+    }
+  }
+
+  // pT3 -> TC (SDL/TrackCandidate.h:383-433); one block per event.
+  __global__ void kAddPT3TC(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.pt3.nPixelTriplets;
+    const unsigned int pLS_offset = es.lsOffset[es.nLowerModules];
+    const unsigned int start = *ev.tc.nTrackCandidates;
+    TrackCandidates tc = ev.tc;
+    PixelTriplets p = ev.pt3;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      bool f = i < n && !p.isDup[i];
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(f ? 1u : 0u, tot);
+      unsigned int idx = start + carry + ex;
+      if (f && idx < kMaxPixelTrackCandidates) {
+        float radius = 0.5f * (p.pixelRadius[i] + p.tripletRadius[i]);
+        unsigned int pix = p.pixelSegmentIndices[i];
+        storeTC(tc, 5, i, i, &p.logicalLayers[5 * i], &p.lowerModuleIndices[5 * i], &p.hitIndices[10 * i],
+                static_cast<int>(ev.ls.seedIdx[pix - pLS_offset]), p.centerX[i], p.centerY[i], radius, idx, i);
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      unsigned int accepted = (start + carry <= kMaxPixelTrackCandidates) ? carry
+                              : (start < kMaxPixelTrackCandidates ? kMaxPixelTrackCandidates - start : 0u);
+      if (accepted < carry)
+        atomicOr(&ev.sc->status, kStatusTCTruncated);
+      *tc.nTrackCandidates = start + accepted;
+      *tc.nTrackCandidatespT3 += accepted;
+    }
+  }
+
+  // Cross-module T5 duplicate removal before TC building
+  // (SDL/Kernels.h:251-323); one warp per eligible module, marks t5Flag.
+  __global__ void kT5DedupBeforeTC(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    if (warp >= nE)
+      return;
+    const Quintuplets& q = ev.t5;
+    uint16_t lowmod1 = ev.rg.indicesOfEligibleT5Modules[warp];
+    unsigned int n1 = q.nQuintuplets[lowmod1];
+    if (n1 == 0)
+      return;
+    unsigned int base1 = ev.rg.quintupletModuleIndices[lowmod1];
+    for (unsigned int ix1 = laneId(); ix1 < n1; ix1 += 32) {
+      unsigned int ix = base1 + ix1;
+      if (q.partOfPT5[ix] || (q.isDup[ix] & 1))
+        continue;
+      float eta1 = q.eta[ix], phi1 = q.phi[ix], score1 = q.score_rphisum[ix];
+      for (int idx2 = warp; idx2 < nE; idx2++) {
+        uint16_t lowmod2 = ev.rg.indicesOfEligibleT5Modules[idx2];
+        unsigned int n2 = q.nQuintuplets[lowmod2];
+        unsigned int base2 = ev.rg.quintupletModuleIndices[lowmod2];
+        for (unsigned int jx1 = 0; jx1 < n2; jx1++) {
+          unsigned int jx = base2 + jx1;
+          if (ix == jx)
+            continue;
+          if (q.partOfPT5[jx] || (q.isDup[jx] & 1))
+            continue;
+          float eta2 = q.eta[jx], phi2 = q.phi[jx], score2 = q.score_rphisum[jx];
+          float dEta = fabs_(eta1 - eta2);
+          float dPhi = wrapDPhi(phi1, phi2);
+          if (dEta > 0.1f)
+            continue;
+          if (fabs_(dPhi) > 0.1f)
+            continue;
+          float dR2 = dEta * dEta + dPhi * dPhi;
+          int nMatched = sharedHitsT5(q, ix, jx);
+          if (dR2 < 0.001f || nMatched >= 5) {
+            if (score1 > score2)
+              ev.t5Flag[ix] = 1;
+            else if (score1 < score2)
+              ev.t5Flag[jx] = 1;
+            else
+              ev.t5Flag[ix < jx ? ix : jx] = 1;
+          }
+        }
+      }
+    }
+  }
+
+  __global__ void kMergeT5Flag(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= int(*ev.rg.nEligibleT5Modules))
+      return;
+    uint16_t lm = ev.rg.indicesOfEligibleT5Modules[warp];
+    unsigned int n = ev.t5.nQuintuplets[lm];
+    unsigned int base = ev.rg.quintupletModuleIndices[lm];
+    for (unsigned int j = laneId(); j < n; j += 32) {
+      if (ev.t5Flag[base + j]) {
+        ev.t5.isDup[base + j] |= 2;
+        ev.t5Flag[base + j] = 0;
+      }
+    }
+  }
+
+  // T5 vs pT5/pT3 eta/phi (SDL/TrackCandidate.h:245-300); one warp per eligible module.
+  __global__ void kCrossCleanT5(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= int(*ev.rg.nEligibleT5Modules))
+      return;
+    uint16_t lm = ev.rg.indicesOfEligibleT5Modules[warp];
+    unsigned int n = ev.t5.nQuintuplets[lm];
+    unsigned int base = ev.rg.quintupletModuleIndices[lm];
+    const unsigned int nPT5 = *ev.pt5.nPixelQuintuplets;
+    const unsigned int loop_bound = nPT5 + *ev.pt3.nPixelTriplets;
+    for (unsigned int j = laneId(); j < n; j += 32) {
+      unsigned int q = base + j;
+      if (ev.t5.isDup[q] or ev.t5.partOfPT5[q])
+        continue;
+      float eta1 = ev.t5.eta[q], phi1 = ev.t5.phi[q];
+      for (unsigned int jx = 0; jx < loop_bound; jx++) {
+        float eta2, phi2;
+        if (jx < nPT5) {
+          eta2 = ev.pt5.eta[jx];
+          phi2 = ev.pt5.phi[jx];
+        } else {
+          eta2 = ev.pt3.eta[jx - nPT5];
+          phi2 = ev.pt3.phi[jx - nPT5];
+        }
+        float dEta = fabs_(eta1 - eta2);
+        float dPhi = wrapDPhi(phi1, phi2);
+        float dR2 = dEta * dEta + dPhi * dPhi;
+        if (dR2 < 1e-3f)
+          ev.t5.isDup[q] = 1;
+      }
+    }
+  }
+
+  // T5 -> TC (SDL/TrackCandidate.h:435-487): count per eligible module, scan,
+  // then emit in (module, T5) order.
+  __global__ void kT5TCCount(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= int(*ev.rg.nEligibleT5Modules))
+      return;
+    uint16_t lm = ev.rg.indicesOfEligibleT5Modules[warp];
+    unsigned int n = ev.t5.nQuintuplets[lm];
+    unsigned int base = ev.rg.quintupletModuleIndices[lm];
+    unsigned int count = 0;
+    for (unsigned int start = 0; start < n; start += 32) {
+      unsigned int j = start + laneId();
+      bool f = false;
+      if (j < n) {
+        unsigned int q = base + j;
+        f = !(ev.t5.isDup[q] or ev.t5.partOfPT5[q]) && ev.t5.TightCutFlag[q];
+      }
+      count += __popc(__ballot_sync(kFullMask, f));
+    }
+    if (laneId() == 0)
+      ev.moduleCount[warp] = count;
+  }
+
+  __global__ void kT5TCScan(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.rg.nEligibleT5Modules;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int c = (i < n) ? ev.moduleCount[i] : 0u;
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(c, tot);
+      if (i < n)
+        ev.moduleOffset[i] = carry + ex;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      unsigned int accepted = carry < kMaxNonPixelTrackCandidates ? carry : kMaxNonPixelTrackCandidates;
+      if (accepted < carry)
+        atomicOr(&ev.sc->status, kStatusTCTruncated);
+      ev.moduleOffset[n] = accepted;
+    }
+  }
+
+  __global__ void kT5TCEmit(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    if (warp >= nE)
+      return;
+    const unsigned int start = *ev.tc.nTrackCandidates;
+    uint16_t lm = ev.rg.indicesOfEligibleT5Modules[warp];
+    unsigned int n = ev.t5.nQuintuplets[lm];
+    unsigned int base = ev.rg.quintupletModuleIndices[lm];
+    unsigned int rank = ev.moduleOffset[warp];
+    TrackCandidates tc = ev.tc;
+    const Quintuplets& q = ev.t5;
+    for (unsigned int s0 = 0; s0 < n; s0 += 32) {
+      unsigned int j = s0 + laneId();
+      bool f = false;
+      unsigned int qi = base + j;
+      if (j < n)
+        f = !(q.isDup[qi] or q.partOfPT5[qi]) && q.TightCutFlag[qi];
+      unsigned int tot;
+      unsigned int r = rank + warpRank(f, tot);
+      if (f && r < kMaxNonPixelTrackCandidates)
+        storeTC(tc, 4, qi, qi, &q.logicalLayers[5 * qi], &q.lowerModuleIndices[5 * qi], &q.hitIndices[10 * qi], -1,
+                q.regressionG[qi], q.regressionF[qi], q.regressionRadius[qi], start + r, qi);
+      rank += tot;
+    }
+  }
+
+  __global__ void kT5TCFinish(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+      unsigned int accepted = ev.moduleOffset[*ev.rg.nEligibleT5Modules];
+      *ev.tc.nTrackCandidates += accepted;
+      *ev.tc.nTrackCandidatesT5 += accepted;
+    }
+  }
+
+  // Shared pixel hits of two pLS, through their hit indices (SDL/TrackCandidate.h:165-202).
+  LST_DEV int sharedPixelHits(const Segments& s, const MiniDoublets& md, const Hits& h, unsigned int ix, unsigned int jx) {
+    int phits1[4] = {static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * ix]]]),
+                     static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * ix + 1]]]),
+                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * ix]]]),
+                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * ix + 1]]])};
+    int phits2[4] = {static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * jx]]]),
+                     static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * jx + 1]]]),
+                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * jx]]]),
+                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * jx + 1]]])};
+    int npMatched = 0;
+    for (int i = 0; i < 4; i++) {
+      bool pmatched = false;
+      if (phits1[i] == -1)
+        continue;
+      for (int j = 0; j < 4; j++) {
+        if (phits2[j] == -1)
+          continue;
+        if (phits1[i] == phits2[j]) {
+          pmatched = true;
+          break;
+        }
+      }
+      if (pmatched)
+        npMatched++;
+    }
+    return npMatched;
+  }
+
+  // pLS vs existing TCs (SDL/TrackCandidate.h:302-381).
+  __global__ void kCrossCleanPLS(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nPix = ev.ls.nSegments[es.pixelModule];
+    const unsigned int prefix = es.lsOffset[es.nLowerModules];
+    const unsigned int nTC = *ev.tc.nTrackCandidates;
+    Segments s = ev.ls;
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPix; i += gridDim.x * blockDim.x) {
+      if (!s.isQuad[i] || s.isDup[i])
+        continue;
+      float eta1 = s.eta[i], phi1 = s.phi[i];
+      bool dup = false;
+      for (unsigned int t = 0; t < nTC; t++) {
+        short type = ev.tc.trackCandidateType[t];
+        unsigned int innerIdx = ev.tc.objectIndices[2 * t];
+        if (type == 4) {
+          float dEta = fabs_(eta1 - ev.t5.eta[innerIdx]);
+          float dPhi = wrapDPhi(phi1, ev.t5.phi[innerIdx]);
+          if (dEta * dEta + dPhi * dPhi < 1e-3f)
+            dup = true;
+        }
+        if (type == 5) {
+          int pLSIndex = static_cast<int>(ev.pt3.pixelSegmentIndices[innerIdx]);
+          if (sharedPixelHits(s, ev.md, ev.hits, prefix + i, static_cast<unsigned int>(pLSIndex)) > 0)
+            dup = true;
+          float dEta = fabs_(eta1 - ev.pt3.eta_pix[innerIdx]);
+          float dPhi = wrapDPhi(phi1, ev.pt3.phi_pix[innerIdx]);
+          if (dEta * dEta + dPhi * dPhi < 0.000001f)
+            dup = true;
+        }
+        if (type == 7) {
+          unsigned int pLSIndex = innerIdx;
+          if (sharedPixelHits(s, ev.md, ev.hits, prefix + i, pLSIndex) > 0)
+            dup = true;
+          float dEta = fabs_(eta1 - s.eta[pLSIndex - prefix]);
+          float dPhi = wrapDPhi(phi1, s.phi[pLSIndex - prefix]);
+          if (dEta * dEta + dPhi * dPhi < 0.000001f)
+            dup = true;
+        }
+      }
+      if (dup)
+        s.isDup[i] = 1;
+    }
+  }
+
+  // pLS -> TC (SDL/TrackCandidate.h:489-529, quadruplets only); one block per event.
+  __global__ void kAddPLSTC(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = ev.ls.nSegments[es.pixelModule];
+    const unsigned int start = *ev.tc.nTrackCandidates;
+    const unsigned int nT5TC = *ev.tc.nTrackCandidatesT5;
+    TrackCandidates tc = ev.tc;
+    const Segments& s = ev.ls;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      bool f = i < n && s.isQuad[i] && !s.isDup[i];
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(f ? 1u : 0u, tot);
+      unsigned int idx = start + carry + ex;
+      if (f && idx - nT5TC < kMaxPixelTrackCandidates) {
+        tc.trackCandidateType[idx] = 8;
+        tc.directObjectIndices[idx] = i;
+        tc.pixelSeedIndex[idx] = static_cast<int>(s.seedIdx[i]);
+        tc.objectIndices[2 * idx] = i;
+        tc.objectIndices[2 * idx + 1] = i;
+        tc.hitIndices[14 * idx + 0] = s.pLSHitsIdxs[4 * i + 0];
+        tc.hitIndices[14 * idx + 1] = s.pLSHitsIdxs[4 * i + 2];
+        tc.hitIndices[14 * idx + 2] = s.pLSHitsIdxs[4 * i + 1];
+        tc.hitIndices[14 * idx + 3] = s.pLSHitsIdxs[4 * i + 3];
+        for (int k = 4; k < 14; ++k)
+          tc.hitIndices[14 * idx + k] = 0;
+        for (int k = 0; k < 7; ++k) {
+          tc.logicalLayers[7 * idx + k] = 0;
+          tc.lowerModuleIndices[7 * idx + k] = 0;
+        }
+        tc.centerX[idx] = 0;
+        tc.centerY[idx] = 0;
+        tc.radius[idx] = 0;
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      unsigned int room = (start - nT5TC < kMaxPixelTrackCandidates) ? kMaxPixelTrackCandidates - (start - nT5TC) : 0u;
+      unsigned int accepted = carry < room ? carry : room;
+      if (accepted < carry)
+        atomicOr(&ev.sc->status, kStatusTCTruncated);
+      *tc.nTrackCandidates = start + accepted;
+      *tc.nTrackCandidatespLS += accepted;
+    }
+  }
+
+
+  // ============================================================== counts
+  // Object counts of one event, as the reference's getNumberOf* members
+  // (SDL/Event.cc:1148-1487): per-layer sums over lower modules with the
+  // same inclusion rules as add*ToEventExplicit.  One block per event.
+  __global__ void kCounts(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sBins[4][11];
+    const EventView& ev = evs[blockIdx.y];
+    for (int i = threadIdx.x; i < 44; i += blockDim.x)
+      (&sBins[0][0])[i] = 0;
+    __syncthreads();
+    const Modules& m = es.m;
+    for (unsigned int i = threadIdx.x; i < es.nLowerModules; i += blockDim.x) {
+      int bin = (m.subdets[i] == Barrel) ? (m.layers[i] - 1) : (6 + m.layers[i] - 1);
+      if (bin < 0 || bin >= 11)
+        continue;
+      unsigned int nmd = ev.md.nMDs[i];
+      if (!(nmd == 0 or ev.hits.hitRanges[i * 2] == -1))
+        atomicAdd(&sBins[0][bin], nmd);
+      unsigned int nls = ev.ls.nSegments[i];
+      if (nls != 0)
+        atomicAdd(&sBins[1][bin], nls);
+      unsigned int nt3 = ev.t3.nTriplets[i];
+      if (nt3 != 0)
+        atomicAdd(&sBins[2][bin], nt3);
+      unsigned int nt5 = ev.t5.nQuintuplets[i];
+      if (!(nt5 == 0 or ev.rg.quintupletModuleIndices[i] == -1))
+        atomicAdd(&sBins[3][bin], nt5);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      lst_counts* c = ev.counts;
+      c->nHits = ev.sc->nHits;
+      c->nPixelSegments = ev.ls.nSegments[es.pixelModule];
+      c->status = ev.sc->status;
+      unsigned int tot[4] = {0, 0, 0, 0};
+      for (int k = 0; k < 4; ++k)
+        for (int b = 0; b < 11; ++b)
+          tot[k] += sBins[k][b];
+      for (int b = 0; b < 6; ++b) {
+        c->mdBarrel[b] = sBins[0][b];
+        c->lsBarrel[b] = sBins[1][b];
+        c->t3Barrel[b] = sBins[2][b];
+        c->t5Barrel[b] = sBins[3][b];
+      }
+      for (int b = 0; b < 5; ++b) {
+        c->mdEndcap[b] = sBins[0][6 + b];
+        c->lsEndcap[b] = sBins[1][6 + b];
+        c->t3Endcap[b] = sBins[2][6 + b];
+        c->t5Endcap[b] = sBins[3][6 + b];
+      }
+      c->nMiniDoublets = tot[0];
+      c->nSegments = tot[1];
+      c->nTriplets = tot[2];
+      c->nQuintuplets = tot[3];
+      c->nPixelTriplets = *ev.pt3.nPixelTriplets;
+      c->nPixelQuintuplets = *ev.pt5.nPixelQuintuplets;
+      c->nTrackCandidates = *ev.tc.nTrackCandidates;
+      c->nTrackCandidatesPT5 = *ev.tc.nTrackCandidatespT5;
+      c->nTrackCandidatesPT3 = *ev.tc.nTrackCandidatespT3;
+      c->nTrackCandidatesPLS = *ev.tc.nTrackCandidatespLS;
+      c->nTrackCandidatesT5 = *ev.tc.nTrackCandidatesT5;
+      c->nPixelTripletsFound = ev.sc->nPT3Total;
+      c->nPixelQuintupletsFound = ev.sc->nPT5Total;
+      for (int k = 0; k < 4; ++k)
+        c->reserved[k] = 0;
+    }
+  }
+
+  // ============================================================ inputs
+  // Sets the hit and pLS counts of one event (per-event input path).
+  __global__ void kSetInputCounts(const EventView* evs, int slot, int setHits, unsigned int nHits, int setPLS,
+                                  unsigned int nPLS, unsigned int statusBits) {
+    const EventView& ev = evs[slot];
+    if (setHits)
+      ev.sc->nHits = nHits;
+    if (setPLS)
+      ev.sc->nPLS = nPLS;
+    ev.sc->status |= statusBits;
+  }
+
+  // Byte layout of one packed input event (see lst_packed_size).
+  struct PackedLayout {
+    size_t x, y, z, detId, idx, h0, h1, h2, h3, dPhiChange, ptIn, ptErr, px, py, pz, eta, etaErr, phi, charge,
+        seedIdx, superbin, pixelType, isQuad, end;
+  };
+  LST_HD PackedLayout packedLayout(unsigned int nHits, unsigned int nPLS) {
+    PackedLayout L;
+    size_t o = 16;
+    size_t h4 = 4 * size_t(nHits), p4 = 4 * size_t(nPLS);
+    L.x = o; o += h4;
+    L.y = o; o += h4;
+    L.z = o; o += h4;
+    L.detId = o; o += h4;
+    L.idx = o; o += h4;
+    L.h0 = o; o += p4;
+    L.h1 = o; o += p4;
+    L.h2 = o; o += p4;
+    L.h3 = o; o += p4;
+    L.dPhiChange = o; o += p4;
+    L.ptIn = o; o += p4;
+    L.ptErr = o; o += p4;
+    L.px = o; o += p4;
+    L.py = o; o += p4;
+    L.pz = o; o += p4;
+    L.eta = o; o += p4;
+    L.etaErr = o; o += p4;
+    L.phi = o; o += p4;
+    L.charge = o; o += p4;
+    L.seedIdx = o; o += p4;
+    L.superbin = o; o += p4;
+    L.pixelType = o; o += nPLS;
+    L.isQuad = o; o += nPLS;
+    L.end = (o + 15) & ~size_t(15);
+    return L;
+  }
+
+  // Unpacks the packed inputs of a batch into the event stores: the hits
+  // (addHitToEvent's copies) and the pixel-segment fields
+  // (addPixelSegmentToEvent's copies).  blockIdx.y = event within the batch.
+  __global__ void kUnpack(const EventView* evs, const unsigned char* blobs, const unsigned long long* offsets) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned char* b = blobs + offsets[blockIdx.y];
+    const unsigned int* hdr = reinterpret_cast<const unsigned int*>(b);
+    unsigned int nHits = hdr[0], nPLSIn = hdr[1];
+    unsigned int status = 0;
+    bool reject = nHits > ev.maxHits;
+    unsigned int nPLS = nPLSIn;
+    if (reject) {
+      status |= kStatusHitCapacity;
+      nHits = 0;
+      nPLS = 0;
+    }
+    if (nPLS > kMaxPixelSegments) {
+      status |= kStatusPLSTruncated;
+      nPLS = kMaxPixelSegments;
+    }
+    if (nHits == 0 && nPLS > 0) {
+      status |= kStatusInvalidInput;
+      nPLS = 0;
+    }
+    const PackedLayout L = packedLayout(reject ? 0u : hdr[0], reject ? 0u : nPLSIn);
+    const unsigned int stride = gridDim.x * blockDim.x;
+    const unsigned int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    for (unsigned int i = t0; i < nHits; i += stride) {
+      ev.hits.xs[i] = reinterpret_cast<const float*>(b + L.x)[i];
+      ev.hits.ys[i] = reinterpret_cast<const float*>(b + L.y)[i];
+      ev.hits.zs[i] = reinterpret_cast<const float*>(b + L.z)[i];
+      ev.hits.detid[i] = reinterpret_cast<const unsigned int*>(b + L.detId)[i];
+      ev.hits.idxs[i] = reinterpret_cast<const unsigned int*>(b + L.idx)[i];
+    }
+    for (unsigned int i = t0; i < nPLS; i += stride) {
+      ev.plsHit0[i] = reinterpret_cast<const unsigned int*>(b + L.h0)[i];
+      ev.plsHit1[i] = reinterpret_cast<const unsigned int*>(b + L.h1)[i];
+      ev.plsHit2[i] = reinterpret_cast<const unsigned int*>(b + L.h2)[i];
+      ev.plsHit3[i] = reinterpret_cast<const unsigned int*>(b + L.h3)[i];
+      ev.plsDPhiChange[i] = reinterpret_cast<const float*>(b + L.dPhiChange)[i];
+      ev.ls.ptIn[i] = reinterpret_cast<const float*>(b + L.ptIn)[i];
+      ev.ls.ptErr[i] = reinterpret_cast<const float*>(b + L.ptErr)[i];
+      ev.ls.px[i] = reinterpret_cast<const float*>(b + L.px)[i];
+      ev.ls.py[i] = reinterpret_cast<const float*>(b + L.py)[i];
+      ev.ls.pz[i] = reinterpret_cast<const float*>(b + L.pz)[i];
+      ev.ls.eta[i] = reinterpret_cast<const float*>(b + L.eta)[i];
+      ev.ls.etaErr[i] = reinterpret_cast<const float*>(b + L.etaErr)[i];
+      ev.ls.phi[i] = reinterpret_cast<const float*>(b + L.phi)[i];
+      ev.ls.charge[i] = reinterpret_cast<const int*>(b + L.charge)[i];
+      ev.ls.seedIdx[i] = reinterpret_cast<const unsigned int*>(b + L.seedIdx)[i];
+      ev.ls.superbin[i] = reinterpret_cast<const int*>(b + L.superbin)[i];
+      ev.ls.pixelType[i] = reinterpret_cast<const int8_t*>(b + L.pixelType)[i];
+      ev.ls.isQuad[i] = reinterpret_cast<const int8_t*>(b + L.isQuad)[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ev.sc->nHits = nHits;
+      ev.sc->nPLS = nPLS;
+      ev.sc->status |= status;
+    }
+  }
+
+}  // namespace lst
