@@ -1,0 +1,486 @@
+#!/usr/bin/env python
+"""PU200-shaped events/s of the LST object-building chain on B200.
+
+A step is one batch of seeded PU200-shaped events (generator configuration 2:
+~20 hard tracks + Poisson(200) vertices x Poisson(60) particles, 1% noise
+hits) taken through every stage: hit preparation, mini-doublets, segments,
+triplets, quintuplets (reference-weight DNN), pLS cleaning, pT5, pT3 and
+track candidates.
+
+Reported:
+  value        batched throughput: the whole batch in one launch per kernel,
+               inputs already resident on the device (lst_batch_ingest +
+               lst_batch_run), events/s over all ranks
+  drop_in      the same events one at a time (per-event launches), events/s
+  e2e          batched through the C ABI from pinned host buffers: packed
+               input upload, all stages, LST::getOutput-style track-candidate
+               hit lists copied back (lst_batch_upload + lst_batch_run +
+               lst_batch_get_output), events/s; e2e_drop_in is the per-event
+               C ABI (add_hits + add_pixel_segments from host arrays, stages,
+               get_output) event by event
+  roofline     the kernel with the largest share of device time, its
+               algorithmic bytes per launch over its CUDA-event duration
+  cpu_baseline the reference CPU backend (oracle/_ref, reference compiler
+               flags) on the host cores, one event per thread
+
+--impl reference times only the reference CPU backend on this workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "PU200 events/s on 1 B200 (batched 64/launch; per-event drop-in reported beside it)"
+HBM_FALLBACK_GBS = 6650.0
+
+# Algorithmic bytes per object of the dominant kernels: each input read once,
+# each output record written once, in the reference's field widths.
+#   MD: 40 B per hit in (x, y, z, rt, phi, eta, 4 edges) + 134 B per MD out
+#   LS: 44 B per MD in + 80 B per module (module map) + 44 B per LS out
+#   T3: 24 B per LS + 20 B per MD in + 60 B per T3 out
+#   T5: 60 B per T3 + 56 B per MD in + 110 B per T5 out
+#   pT3/pT5: 76 B per pLS + 4 B per connected-module entry + 60 B per T3 (or
+#            110 B per T5) in + 100 B per pT3/pT5 out
+ALGO_BYTES = {
+    "kCreateMD": lambda c: 40 * c["nHits"] + 134 * c["nMD"],
+    "kCreateLS": lambda c: 44 * c["nMD"] + 80 * c["nLower"] + 44 * c["nLS"],
+    "kCreateT3": lambda c: 24 * c["nLS"] + 20 * c["nMD"] + 60 * c["nT3"],
+    "kCreateT5": lambda c: 60 * c["nT3"] + 56 * c["nMD"] + 110 * c["nT5"],
+    "kPT3Count": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 60 * c["nT3"],
+    "kPT3Emit": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 60 * c["nT3"] + 100 * c["nPT3"],
+    "kPT5Count": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 110 * c["nT5"],
+    "kPT5Emit": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 110 * c["nT5"] + 100 * c["nPT5"],
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def generate(config: int, first: int, n: int, workers: int):
+    from tracklooper_b200 import gen
+
+    with ThreadPoolExecutor(max_workers=max(1, workers)) as pool:
+        return list(pool.map(lambda i: gen.generate_event(config, first + i), range(n)))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled
+    to the bench workload there; None if no capture is committed."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------- ours
+def run_ours(args, rank, world, local, events):
+    import torch
+    import torch.distributed as tdist
+
+    from tracklooper_b200 import lst
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = len(events)
+    es = lst.ES(device=local)
+    max_hits = max(e.n_hits for e in events)
+    max_hits = ((max_hits + 4095) // 4096) * 4096
+    eset = lst.EventSet(es, n_slots=B, max_hits=max_hits)
+    stream = torch.cuda.ExternalStream(eset.stream(), device=dev)
+
+    blob_np, offsets = lst.pack_events(events)
+    pinned = torch.empty(blob_np.nbytes, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = blob_np
+    blob = pinned.numpy()
+    in_bytes = int(blob.nbytes)
+
+    # output buffers (pinned)
+    tc_cap = 31000 * B
+    out_hits = torch.empty(tc_cap * 14, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    out_len = torch.empty(tc_cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    out_seed = torch.empty(tc_cap, dtype=torch.int32, pin_memory=True).numpy()
+    out_type = torch.empty(tc_cap, dtype=torch.int16, pin_memory=True).numpy()
+    tco = np.zeros(B + 1, np.uint64)
+    hco = np.zeros(B + 1, np.uint64)
+    outs = lst.Output(out_hits.ctypes.data, out_hits.size, out_len.ctypes.data, out_seed.ctypes.data,
+                      out_type.ctypes.data, out_len.size, tco.ctypes.data, hco.ctypes.data)
+    lib = lst.library()
+    import ctypes
+
+    def get_output():
+        lst._check(lib.lst_batch_get_output(eset.handle, 0, B, ctypes.byref(outs)), "lst_batch_get_output")
+        n_tc, n_h = int(tco[-1]), int(hco[-1])
+        return n_tc * (4 + 4 + 2) + n_h * 4 + 2 * (B + 1) * 8
+
+    # first pass: upload + all stages + output (also a correctness gate on status bits)
+    eset.upload_packed(0, blob, offsets)
+    eset.run(0, B)
+    counts = eset.batch_counts(0, B)
+    bad = [i for i, c in enumerate(counts) if c["status"] & ~0x30]
+    if bad:
+        raise RuntimeError(f"events with input errors: {bad[:5]}")
+    d2h_bytes = get_output()
+
+    def batched_step():
+        eset.ingest(0, B)
+        eset.run(0, B)
+
+    def dropin_step():
+        for i in range(B):
+            eset.ingest(i, 1)
+            eset.run(i, 1)
+
+    def timed(step, k, sampler=None):
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        l0 = eset.launches()
+        start.record(stream)
+        for _ in range(k):
+            step()
+        stop.record(stream)
+        stop.synchronize()
+        l1 = eset.launches()
+        clocks = sampler.stop() if sampler else None
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, l1 - l0, clocks
+
+    # warm-up
+    for _ in range(args.warmup):
+        batched_step()
+    for _ in range(max(1, args.warmup // 2)):
+        dropin_step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    ms_b, launches_b, clocks = timed(batched_step, args.steps, sampler)
+    ms_d, _, _ = timed(dropin_step, max(1, args.steps // 2))
+    steps_d = max(1, args.steps // 2)
+
+    # e2e batched: host packed inputs -> device -> stages -> track-candidate output on host
+    def e2e_step():
+        eset.upload_packed(0, blob, offsets)
+        eset.run(0, B)
+        get_output()
+
+    for _ in range(2):
+        e2e_step()
+    ms_e, _, _ = timed(e2e_step, args.steps)
+
+    # e2e drop-in: per-event C ABI calls with host arrays, event by event
+    ev1 = lst.Event(es, event_set=eset, slot=0)
+
+    def e2e_dropin_step():
+        for i, inp in enumerate(events):
+            e = lst.Event(es, event_set=eset, slot=i)
+            e.run(inp)
+            eset.output(i, 1)
+
+    e2e_dropin_step()
+    n_dropin_e2e = max(1, args.steps // 4)
+    ms_de, _, _ = timed(e2e_dropin_step, n_dropin_e2e)
+    del ev1
+
+    # per-kernel device time (instrumented pass over the same batched steps)
+    eset.set_profiling(True)
+    for _ in range(args.steps):
+        batched_step()
+    prof = eset.profile()
+    eset.set_profiling(False)
+
+    tot = sum(v[1] for v in prof.values())
+    top = sorted(prof.items(), key=lambda kv: -kv[1][1])
+    agg = {
+        "nHits": sum(c["nHits"] for c in counts),
+        "nMD": sum(c["nMiniDoublets"] for c in counts) + sum(2 * c["nPixelSegments"] for c in counts),
+        "nLS": sum(c["nSegments"] for c in counts),
+        "nT3": sum(c["nTriplets"] for c in counts),
+        "nT5": sum(c["nQuintuplets"] for c in counts),
+        "nPLS": sum(c["nPixelSegments"] for c in counts),
+        "nPT3": sum(c["nPixelTriplets"] for c in counts),
+        "nPT5": sum(c["nPixelQuintuplets"] for c in counts),
+        "nTC": sum(c["nTrackCandidates"] for c in counts),
+        "nLower": es.info["nLowerModules"] * B,
+    }
+    peak, peak_kind = hbm_peak()
+    dominant = next((k for k, _ in top if k in ALGO_BYTES), top[0][0])
+    dlaunches, dms = prof[dominant]
+    algo = ALGO_BYTES[dominant](agg) if dominant in ALGO_BYTES else None
+    achieved = (algo / (dms / dlaunches * 1e-3) / 1e9) if algo else None
+    roofline = {
+        "bound": "hbm",
+        "kernel": dominant,
+        "achieved": round(achieved, 2) if achieved else None,
+        "peak": peak,
+        "peak_kind": f"{peak_kind} (copy bandwidth)",
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 5) if achieved else None,
+        "traffic": committed_traffic(dominant),
+        "algorithmic_bytes_per_launch": algo,
+        "launch_ms": round(dms / dlaunches, 4),
+        "share_of_device_time": round(dms / tot, 4) if tot else None,
+    }
+    kernel_table = {k: {"launches": v[0], "ms_per_step": round(v[1] / args.steps, 4),
+                        "share": round(v[1] / tot, 4) if tot else None} for k, v in top[:12]}
+
+    events_all = B * world
+    value = events_all * args.steps / (ms_b * 1e-3)
+    res = {
+        "value": value,
+        "ms_per_step": ms_b / args.steps,
+        "drop_in": {"value": events_all * steps_d / (ms_d * 1e-3), "unit": "events/s",
+                    "ms_per_event": ms_d / steps_d / B},
+        "batched_over_drop_in": (ms_d / steps_d) / (ms_b / args.steps),
+        "e2e": {"value": events_all * args.steps / (ms_e * 1e-3), "unit": "events/s",
+                "h2d_bytes_per_step": in_bytes + 8 * B, "d2h_bytes_per_step": d2h_bytes,
+                "mode": "batched C ABI from pinned host buffers (lst_batch_upload, lst_batch_run, lst_batch_get_output)"},
+        "e2e_drop_in": {"value": events_all * n_dropin_e2e / (ms_de * 1e-3), "unit": "events/s",
+                        "mode": "per-event C ABI from host arrays (add_hits, add_pixel_segments, stages, output)"},
+        "gpu_launches": launches_b,
+        "clocks": clocks,
+        "roofline": roofline,
+        "kernels": kernel_table,
+        "objects_per_event": {k: round(v / B, 1) for k, v in agg.items() if k != "nLower"},
+        "device_memory_gb": round(eset.memory_bytes() / 1e9, 2),
+        "l2": f"inputs larger than L2: {in_bytes / 1e6:.0f} MB of packed inputs per step plus the object arenas",
+    }
+    eset.close()
+    es.close()
+    return res
+
+
+# ----------------------------------------------------------- reference CPU
+def run_reference_cpu(events, threads: int, min_events: int, budget_s: float = 20.0):
+    """Reference CPU backend, one event per thread at a time; returns (events/s, events, threads, seconds)."""
+    from oracle import reflib
+
+    variant = "fast"
+    if not reflib.available(variant):
+        raise FileNotFoundError(reflib.library_path(variant))
+    base = reflib.RefLST(variant)
+    workers = [base] + [base.fork() for _ in range(threads - 1)]
+    # warm one event per worker (page-in, allocator)
+    n = max(min_events, threads)
+    lock = threading.Lock()
+    next_i = [0]
+    done = [0]
+    t_end = [None]
+
+    def work(w):
+        while True:
+            with lock:
+                i = next_i[0]
+                if i >= n:
+                    return
+                next_i[0] += 1
+            w.run_event(events[i % len(events)])
+            with lock:
+                done[0] += 1
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=work, args=(w,)) for w in workers]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    for w in workers[1:]:
+        w.close()
+    base.close()
+    return done[0] / dt, done[0], threads, dt
+
+
+def cpu_threads(ncpu: int) -> int:
+    """Host threads for the reference CPU backend: all cores, bounded by memory
+    (each in-flight reference event holds ~0.6 GB of object arenas)."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail_gb = int(line.split()[1]) / 1e6
+                    return max(1, min(ncpu, int(avail_gb / 0.6)))
+    except OSError:
+        pass
+    return ncpu
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--cpu-events", type=int, default=0, help="reference CPU sample size (0: 2 per thread)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_env()
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+    config = {"workload": f"PU200-shaped events (generator configuration {args.config}), batch of {args.batch} per GPU",
+              "events_per_step_per_gpu": args.batch, "geometry": "OT800_IT615_pt0.8",
+              "t5_selection": "reference-weight DNN", "parallelism": f"replicas x{world}"}
+    base = {"metric": METRIC, "unit": "events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator, PU200-shaped)", "config": config}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        events = generate(args.config, 0, args.batch, ncpu)
+        threads = cpu_threads(ncpu)
+        n = args.cpu_events or 2 * threads
+        for _ in range(min(1, args.warmup)):
+            run_reference_cpu(events, threads, threads)
+        rates = []
+        t_all = 0.0
+        for _ in range(args.steps):
+            r, ne, th, dt = run_reference_cpu(events, threads, n)
+            rates.append(r)
+            t_all += dt
+        value = statistics.mean(rates)
+        line = dict(base)
+        line.update({"impl": "reference", "value": value, "ms_per_step": 1e3 * t_all / args.steps,
+                     "cpu_baseline": {"value": value, "unit": "events/s", "cores": threads, "kind": "reference",
+                                      "sample": f"{n} events per step, one event per thread, liblstref_fast.so"},
+                     "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch.distributed as tdist
+        import datetime
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    events = generate(args.config, rank * args.batch, args.batch, ncpu)
+    res = run_ours(args, rank, world, local, events)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        try:
+            threads = cpu_threads(ncpu)
+            r, ne, th, dt = run_reference_cpu(events, threads, args.cpu_events or 2 * threads)
+            cpu = {"value": r, "unit": "events/s", "cores": th, "kind": "reference",
+                   "sample": f"{ne} events of this batch, one event per thread, {dt:.1f} s wall, liblstref_fast.so"}
+        except Exception as e:  # the CPU baseline is reported, not required
+            cpu = {"value": None, "unit": "events/s", "cores": ncpu, "kind": "reference", "sample": f"failed: {e}"}
+
+    if world > 1:
+        import torch.distributed as tdist
+
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        line = dict(base)
+        line.update(res)
+        line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

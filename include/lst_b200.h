@@ -100,6 +100,12 @@ typedef struct lst_es_info {
 /* Last error message of the calling thread (empty if none). */
 const char* lst_last_error(void);
 
+/* Launch resources of the library's kernels (registers per thread, the
+ * largest block they can be launched with, local and static shared memory). */
+int lst_kernel_count(void);
+int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_threads_per_block, size_t* local_bytes,
+                          size_t* static_smem_bytes);
+
 /* ------------------------------------------------------------------ ES */
 /* Loads the geometry directory (the OT800_IT615_pt0.8 layout: sensor
  * centroids, module connection map, pixel maps, endcap and tilted-barrel
@@ -205,10 +211,48 @@ int lst_field_info(int i, const char** name, size_t* elem_size, char* kind);
 size_t lst_packed_size(uint32_t n_hits, uint32_t n_pls);
 int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
                      const uint64_t* blob_offsets);
+/* Repeats the unpacking of the last uploaded inputs of slots [first,
+ * first + count) (as lst_batch_upload without the host-to-device copy), for
+ * re-running events whose inputs are already resident on the device. */
+int lst_batch_ingest(lst_event* ev, int first, int count);
 /* Runs stages [first_stage, last_stage] for slots [first, first + count). */
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage);
 /* Copies the counts of slots [first, first + count) into out[count]. */
 int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out);
+
+/* Track-candidate output of LST::getOutput (SDL/LST.cc:367-427) for slots
+ * [first, first + count), flattened over the events: candidate k of the batch
+ * has type[k], seedIdx[k] (pixelSeedIndex) and len[k] input-ntuple hit
+ * indices, stored back to back in hits[].  Event i owns candidates
+ * [event_tc_offsets[i], event_tc_offsets[i + 1]) and hits
+ * [event_hit_offsets[i], event_hit_offsets[i + 1]); both offset arrays hold
+ * count + 1 entries and are always filled.  If tc_capacity or hits_capacity
+ * is too small, nothing else is written and the call returns -1. */
+typedef struct lst_output {
+  uint32_t* hits;
+  size_t hits_capacity;
+  uint32_t* len;
+  int32_t* seedIdx;
+  int16_t* type;
+  size_t tc_capacity;
+  uint64_t* event_tc_offsets;
+  uint64_t* event_hit_offsets;
+} lst_output;
+int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out);
+
+/* ---------------------------------------------------------- accounting */
+/* Number of kernels the set has launched since it was created. */
+int lst_event_launches(const lst_event* ev, uint64_t* n);
+/* With profiling on, every launch of the set is bracketed by CUDA events on
+ * its stream; lst_event_get_profile synchronises, sums the elapsed times per
+ * kernel since profiling was switched on (or last read) and clears them. */
+typedef struct lst_kernel_time {
+  const char* name;
+  uint64_t launches;
+  double total_ms;
+} lst_kernel_time;
+int lst_event_set_profiling(lst_event* ev, int on);
+int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int* n_kernels);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,8 @@ class StoreIndex:
 def _object_index(store: str, name: str, arr_len: int, si: StoreIndex, sizes: dict):
     """(indices, multiplicity) of the live entries of field `name`, or None to compare all."""
     fld = name.split(".", 1)[1]
+    if name == "ranges.indicesOfEligibleT5Modules":
+        return np.arange(int(si.get("ranges.nEligibleT5Modules")[0])), 1
     if store == "hits":
         if arr_len % sizes["H"] == 0 and arr_len // sizes["H"] <= 1 and not fld.startswith("hitRanges"):
             return si.hits, 1
@@ -139,9 +141,11 @@ def compare_stores(get_a, get_b, names, n_lower: int, n_hits: int, sizes: dict, 
             continue
         a = get_a(name)
         b = get_b(name)
-        if a is None or b is None:
-            problems.append(f"{name}: missing on one side")
+        if a is None:
+            problems.append(f"{name}: missing")
             continue
+        if b is None:  # a store the other side allocated with zero length
+            b = np.zeros(0, a.dtype)
         store = name.split(".", 1)[0]
         sel = _object_index(store, name, a.size, sa, sizes)
         if sel is None:
@@ -151,7 +155,9 @@ def compare_stores(get_a, get_b, names, n_lower: int, n_hits: int, sizes: dict, 
         else:
             idx, mult = sel
             full = _expand(idx, mult)
-            full = full[full < min(a.size, b.size)]
+            if full.size and int(full.max()) >= min(a.size, b.size):
+                problems.append(f"{name}: live entries up to {int(full.max())} but lengths {a.size}, {b.size}")
+                continue
             av, bv, where = a[full], b[full], full
         if av.dtype.kind == "f":
             av = av.view(np.uint32 if av.dtype.itemsize == 4 else np.uint64)

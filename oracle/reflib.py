@@ -75,13 +75,23 @@ class RefLST:
         self.n_modules, self.n_lower = nm.value, nl.value
         self.ev = lib.lstref_event_create(self.es)
 
+    def fork(self) -> "RefLST":
+        """Another event on the same event setup (for one event per thread)."""
+        other = RefLST.__new__(RefLST)
+        other.lib = self.lib
+        other.es = self.es
+        other._owns_es = False
+        other.n_pixels, other.n_modules, other.n_lower = self.n_pixels, self.n_modules, self.n_lower
+        other.ev = self.lib.lstref_event_create(self.es)
+        return other
+
     def close(self):
         if self.ev:
             self.lib.lstref_event_destroy(self.ev)
             self.ev = None
-        if self.es:
+        if self.es and getattr(self, "_owns_es", True):
             self.lib.lstref_es_free(self.es)
-            self.es = None
+        self.es = None
 
     def __del__(self):
         try:

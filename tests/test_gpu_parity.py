@@ -64,7 +64,6 @@ def _compare_event(ref, es, event, inp, stages=STAGES):
         p = compare.compare_stores(get_gpu, get_ref, fields, es.info["nLowerModules"], inp.n_hits, _sizes(es, event))
         if p:
             problems.append((st, p))
-            break
     return problems
 
 
@@ -86,3 +85,67 @@ def test_pu200_events(ref, es, event, index):
     assert not problems, _fmt(problems)
     c = event.counts()
     assert c["nTrackCandidates"] > 1000
+
+
+def _ref_output(ref, dtypes):
+    """LST::getOutput restated on the reference's stores (SDL/LST.cc:367-427)."""
+    n = int(ref.field("tc.nTrackCandidates", dtype=np.uint32)[0])
+    types = ref.field("tc.trackCandidateType", dtype=np.int16)[:n]
+    seeds = ref.field("tc.pixelSeedIndex", dtype=np.int32)[:n]
+    th = ref.field("tc.hitIndices", dtype=np.uint32)
+    idxs = ref.field("hits.idxs", dtype=np.uint32)
+    hits = []
+    for i in range(n):
+        t = int(types[i])
+        maxn = {7: 14, 5: 10, 4: 10, 8: 4}.get(t, 0)
+        out = []
+        for k in range(maxn):
+            g = int(th[14 * i + k])
+            h = g if t == 8 else int(idxs[g])
+            if t != 4 and len(out) == 3 and out[-1] == h:
+                continue
+            out.append(h)
+        hits.append(out)
+    return hits, types, seeds
+
+
+@pytest.mark.parametrize("index", [0])
+def test_get_output_matches_reference(ref, es, event, index):
+    inp = gen.generate_event(2, 10 + index)
+    ref.run_event(inp)
+    event.run(inp)
+    hits, ln, seed, typ = event.getOutput()
+    rhits, rtypes, rseeds = _ref_output(ref, lst.field_dtypes())
+    assert len(hits) == len(rhits) > 0
+    assert np.array_equal(typ, rtypes)
+    assert np.array_equal(seed, rseeds)
+    assert np.array_equal(ln, np.array([len(h) for h in rhits], np.uint32))
+    assert hits == rhits
+
+
+def test_batched_uneven_events_match_reference(ref, es):
+    """Four uneven events (pileup 140-250) in one batched launch per kernel."""
+    inputs = [gen.generate_event(3, i) for i in range(4)]
+    eset = lst.EventSet(es, n_slots=4, max_hits=max(i.n_hits for i in inputs) + 1024)
+    blob, offsets = lst.pack_events(inputs)
+    eset.upload_packed(0, blob, offsets)
+    eset.run(0, 4)
+    dtypes = lst.field_dtypes()
+    names = list(dtypes)
+    sizes = {"H": eset.max_hits, "MD": es.info["nTotalMDs"], "LS": es.info["nTotalSegments"],
+             "T3": es.info["maxTriplets"], "T5": es.info["maxQuintuplets"]}
+    counts = eset.batch_counts(0, 4)
+    for slot, inp in enumerate(inputs):
+        ref.run_event(inp)
+        p = compare.compare_stores(lambda n: eset.field(slot, n), lambda n: ref.field(n, dtype=dtypes[n]), names,
+                                   es.info["nLowerModules"], inp.n_hits, sizes)
+        assert not p, f"slot {slot}: " + "; ".join(p[:8])
+        assert counts[slot]["nTrackCandidates"] == int(ref.field("tc.nTrackCandidates", dtype=np.uint32)[0])
+    # the batch output equals the per-slot outputs
+    hits, ln, seed, typ, tco, hco = eset.output(0, 4, tc_capacity=4 * 31000, hits_capacity=4 * 31000 * 14)
+    for slot in range(4):
+        h1, l1, s1, t1, _, _ = eset.output(slot, 1)
+        a, b = int(tco[slot]), int(tco[slot + 1])
+        assert np.array_equal(ln[a:b], l1) and np.array_equal(seed[a:b], s1) and np.array_equal(typ[a:b], t1)
+        assert np.array_equal(hits[int(hco[slot]):int(hco[slot + 1])], h1)
+    eset.close()

@@ -50,7 +50,8 @@ namespace lst {
     unsigned int status;
     unsigned int nPT5Total;
     unsigned int nPT3Total;
-    unsigned int pad[3];
+    unsigned int nOutHits;  // output hit-list length of the event's track candidates
+    unsigned int pad[2];
   };
 
   // All device pointers of one event.
@@ -81,6 +82,8 @@ namespace lst {
     unsigned int* moduleOffset;
     uint8_t* t5Flag;   // removal marks of the cross-module T5 cleaning
     uint8_t* plsFlag;  // removal marks of the second pLS cleaning pass
+    unsigned int* tcOutLen;     // output hits per track candidate
+    unsigned int* tcOutOffset;  // offset of a candidate's hits in the event's output
     unsigned int maxHits;
   };
 

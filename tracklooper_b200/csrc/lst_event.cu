@@ -42,6 +42,27 @@ namespace {
       return cudaFail(e_, #call);      \
   } while (0)
 
+  // Launches a kernel on stream `s` and returns an error naming it if the
+  // launch is rejected.
+  // With profiling on, each launch is bracketed by two CUDA events on the
+  // same stream (see lst_event_set_profiling).
+#define LST_LAUNCH(kernel, grid, block, ...)                   \
+  do {                                                         \
+    cudaEvent_t p0_ = nullptr;                                 \
+    if (ev->profiling && (p0_ = profEvent(ev)))                \
+      cudaEventRecord(p0_, s);                                 \
+    kernel<<<(grid), (block), 0, s>>>(__VA_ARGS__);            \
+    cudaError_t e_ = cudaGetLastError();                       \
+    if (e_ != cudaSuccess)                                     \
+      return cudaFail(e_, #kernel);                            \
+    ++ev->launches;                                            \
+    cudaEvent_t p1_ = nullptr;                                 \
+    if (p0_ && (p1_ = profEvent(ev))) {                        \
+      cudaEventRecord(p1_, s);                                 \
+      ev->profile.push_back(ProfRecord{#kernel, p0_, p1_});    \
+    }                                                          \
+  } while (0)
+
   // Carves 256-byte-aligned sub-arrays out of one allocation.  With a null
   // base it only measures.
   struct Carver {
@@ -232,6 +253,13 @@ namespace {
 }  // namespace
 
 // ---------------------------------------------------------------- events
+namespace {
+  struct ProfRecord {
+    const char* kernel;
+    cudaEvent_t start, stop;
+  };
+}  // namespace
+
 struct lst_event {
   lst_es* es = nullptr;
   int nSlots = 0;
@@ -249,10 +277,38 @@ struct lst_event {
   unsigned char* inbox = nullptr;
   size_t inboxBytes = 0;
   unsigned long long* dOffsets = nullptr;
+  bool inboxValid = false;
   // per-slot counts, contiguous on the device and in pinned host memory
   lst_counts* dCounts = nullptr;
   lst_counts* hCounts = nullptr;
+  // track-candidate output staging (grown on demand)
+  unsigned long long* dOutOffsets = nullptr;  // 2 * (nSlots + 1)
+  unsigned long long* hOutOffsets = nullptr;  // pinned copy
+  unsigned char* dOut = nullptr;
+  size_t dOutBytes = 0;
+  // launch accounting and optional per-launch timing
+  unsigned long long launches = 0;
+  bool profiling = false;
+  std::vector<cudaEvent_t> eventPool;
+  size_t poolUsed = 0;
+  std::vector<ProfRecord> profile;
 };
+
+namespace {
+  // Next timing event of the set's pool (grown on demand); null if the
+  // runtime cannot create one, in which case that launch is not timed.
+  cudaEvent_t profEvent(lst_event* ev) {
+    if (ev->poolUsed == ev->eventPool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+      ev->eventPool.push_back(e);
+    }
+    return ev->eventPool[ev->poolUsed++];
+  }
+}  // namespace
 
 namespace {
 
@@ -274,37 +330,33 @@ namespace {
     return 0;
   }
 
-  int launchStatus(const char* what) {
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess)
-      return cudaFail(e, what);
-    return 0;
-  }
 
   int runReset(lst_event* ev, int first, int count) {
     const lst_es* es = ev->es;
     dim3 g(blocksFor(2 * size_t(es->view.nModules), count), count);
-    lst::kResetEvent<<<g, kThreads, 0, ev->stream>>>(es->view, ev->dv + first);
-    return launchStatus("kResetEvent");
+    cudaStream_t s = ev->stream;
+    LST_LAUNCH(lst::kResetEvent, g, kThreads, es->view, ev->dv + first);
+    return 0;
   }
 
   int runHitKernels(lst_event* ev, int first, int count) {
     const lst::DeviceES& d = ev->es->view;
-    lst::kHitPrep<<<dim3(blocksFor(ev->maxHits, count), count), kThreads, 0, ev->stream>>>(d, ev->dv + first);
-    lst::kModuleRanges<<<dim3(blocksFor(d.nLowerModules, count), count), kThreads, 0, ev->stream>>>(d, ev->dv + first);
-    return launchStatus("hit kernels");
+    cudaStream_t s = ev->stream;
+    LST_LAUNCH(lst::kHitPrep, dim3(blocksFor(ev->maxHits, count), count), kThreads, d, ev->dv + first);
+    LST_LAUNCH(lst::kModuleRanges, dim3(blocksFor(d.nLowerModules, count), count), kThreads, d, ev->dv + first);
+    return 0;
   }
 
   int runPixelIngest(lst_event* ev, int first, int count) {
     const lst::DeviceES& d = ev->es->view;
-    lst::kPixelIngest<<<dim3(blocksFor(lst::kMaxPixelSegments, count), count), kThreads, 0, ev->stream>>>(
-        d, ev->dv + first);
-    return launchStatus("kPixelIngest");
+    cudaStream_t s = ev->stream;
+    LST_LAUNCH(lst::kPixelIngest, dim3(blocksFor(lst::kMaxPixelSegments, count), count), kThreads, d, ev->dv + first);
+    return 0;
   }
 
   // Warp-per-object kernels: blocks of `warps` warps.
   dim3 warpGrid(size_t nObjects, int warps, int count) {
-    return dim3(blocksFor(nObjects, count, 32u * warps) , count);
+    return dim3(blocksFor(nObjects * 32, count, 32u * warps), count);
   }
 
   int runStage(lst_event* ev, int first, int count, int stage) {
@@ -316,74 +368,89 @@ namespace {
     const dim3 one(1, count);
     switch (stage) {
       case LST_STAGE_MINI_DOUBLETS:
-        lst::kCreateMD<<<warpGrid(nLower, 8, count), 256, 0, s>>>(d, v);
-        lst::kMDRanges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kCreateMD, warpGrid(nLower, 8, count), 256, d, v);
+        LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;
       case LST_STAGE_SEGMENTS:
-        lst::kCreateLS<<<warpGrid(nLower, lst::kLSWarps, count), 32 * lst::kLSWarps, 0, s>>>(d, v);
-        lst::kLSRanges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kCreateLS, warpGrid(nLower, lst::kLSWarps, count), 32 * lst::kLSWarps, d, v);
+        LST_LAUNCH(lst::kLSRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;
       case LST_STAGE_TRIPLETS:
-        lst::kT3Offsets<<<one, 1024, 0, s>>>(d, v);
-        lst::kCreateT3<<<warpGrid(nLower, lst::kT3Warps, count), 32 * lst::kT3Warps, 0, s>>>(d, v);
-        lst::kT3Ranges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kT3Offsets, one, 1024, d, v);
+        LST_LAUNCH(lst::kCreateT3, warpGrid(nLower, lst::kT3Warps, count), 32 * lst::kT3Warps, d, v);
+        LST_LAUNCH(lst::kT3Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;
       case LST_STAGE_QUINTUPLETS: {
         if (ev->t5Method == LST_T5_DNN && !ev->es->haveDnn)
           return setError("the DNN T5 method needs weights (lst_es_load or lst_es_set_t5dnn_weights)");
         bool useDnn = ev->t5Method == LST_T5_DNN;
-        lst::kT5Eligible<<<one, 1024, 0, s>>>(d, v);
-        lst::kCreateT5<<<warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, 0, s>>>(
-            d, v, useDnn);
-        lst::kT5DedupAfterBuild<<<dim3(ceilDiv(nLower * 32, 256), count), 256, 0, s>>>(d, v);
-        lst::kT5Ranges<<<dim3(blocksFor(nLower, count), count), kThreads, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kT5Eligible, one, 1024, d, v);
+        LST_LAUNCH(lst::kCreateT5, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v, useDnn);
+        LST_LAUNCH(lst::kT5DedupAfterBuild, dim3(ceilDiv(nLower * 32, 256), count), 256, d, v);
+        LST_LAUNCH(lst::kT5Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;
       }
       case LST_STAGE_PLS_CLEANING:
-        lst::kPLSClean<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v, false);
+        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, false);
         break;
       case LST_STAGE_PIXEL_QUINTUPLETS:
-        lst::kPixelConnect<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
-        lst::kPT5Count<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
-        lst::kPLSScan<<<one, 1024, 0, s>>>(d, v, 0);
-        lst::kPT5Emit<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
-        lst::kPT5Dedup<<<dim3(blocksFor(lst::kMaxPixelQuintuplets, count), count), kThreads, 0, s>>>(d, v);
-        lst::kAddPT5TC<<<one, 1024, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
+        LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 0);
+        LST_LAUNCH(lst::kPT5Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
+        LST_LAUNCH(lst::kPT5Dedup, dim3(blocksFor(lst::kMaxPixelQuintuplets, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kAddPT5TC, one, 1024, d, v);
         break;
       case LST_STAGE_PIXEL_TRIPLETS:
-        lst::kPixelConnect<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
-        lst::kPT3Count<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
-        lst::kPLSScan<<<one, 1024, 0, s>>>(d, v, 1);
-        lst::kPT3Emit<<<warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, 0, s>>>(d, v);
-        lst::kPT3Dedup<<<dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPT3Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
+        LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 1);
+        LST_LAUNCH(lst::kPT3Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
+        LST_LAUNCH(lst::kPT3Dedup, dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, d, v);
         break;
       case LST_STAGE_TRACK_CANDIDATES: {
         const size_t nE = ev->es->nEligibleMax;
         const dim3 eligGrid(ceilDiv(std::max<size_t>(nE, 1) * 32, 256), count);
-        lst::kCrossCleanPT3<<<dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, 0, s>>>(d, v);
-        lst::kAddPT3TC<<<one, 1024, 0, s>>>(d, v);
-        lst::kT5DedupBeforeTC<<<eligGrid, 256, 0, s>>>(d, v);
-        lst::kMergeT5Flag<<<eligGrid, 256, 0, s>>>(d, v);
-        lst::kCrossCleanT5<<<eligGrid, 256, 0, s>>>(d, v);
-        lst::kT5TCCount<<<eligGrid, 256, 0, s>>>(d, v);
-        lst::kT5TCScan<<<one, 1024, 0, s>>>(d, v);
-        lst::kT5TCEmit<<<eligGrid, 256, 0, s>>>(d, v);
-        lst::kT5TCFinish<<<one, 32, 0, s>>>(d, v);
-        lst::kPLSClean<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v, true);
-        lst::kMergePLSFlag<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
-        lst::kCrossCleanPLS<<<dim3(blocksFor(P, count), count), kThreads, 0, s>>>(d, v);
-        lst::kAddPLSTC<<<one, 1024, 0, s>>>(d, v);
+        LST_LAUNCH(lst::kCrossCleanPT3, dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kAddPT3TC, one, 1024, d, v);
+        LST_LAUNCH(lst::kT5DedupBeforeTC, eligGrid, 256, d, v);
+        LST_LAUNCH(lst::kMergeT5Flag, eligGrid, 256, d, v);
+        LST_LAUNCH(lst::kCrossCleanT5, eligGrid, 256, d, v);
+        LST_LAUNCH(lst::kT5TCCount, eligGrid, 256, d, v);
+        LST_LAUNCH(lst::kT5TCScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kT5TCEmit, eligGrid, 256, d, v);
+        LST_LAUNCH(lst::kT5TCFinish, one, 32, d, v);
+        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, true);
+        LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kCrossCleanPLS, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kAddPLSTC, one, 1024, d, v);
         break;
       }
       default:
         return setError("unknown stage " + std::to_string(stage));
     }
-    return launchStatus("stage kernels");
+    return 0;
   }
 
   int runCounts(lst_event* ev, int first, int count) {
-    lst::kCounts<<<dim3(1, count), 256, 0, ev->stream>>>(ev->es->view, ev->dv + first);
-    return launchStatus("kCounts");
+    cudaStream_t s = ev->stream;
+    LST_LAUNCH(lst::kCounts, dim3(1, count), 256, ev->es->view, ev->dv + first);
+    return 0;
+  }
+
+  // Resets slots [first, first + count) and unpacks their packed inputs from
+  // the device inbox: the work of addHitToEvent + addPixelSegmentToEvent.
+  int ingestInbox(lst_event* ev, int first, int count) {
+    int rc = runReset(ev, first, count);
+    if (rc)
+      return rc;
+    cudaStream_t s = ev->stream;
+    LST_LAUNCH(lst::kUnpack, dim3(blocksFor(ev->maxHits, count), count), kThreads, ev->dv + first, ev->inbox,
+               ev->dOffsets + first);
+    rc = runHitKernels(ev, first, count);
+    if (rc)
+      return rc;
+    return runPixelIngest(ev, first, count);
   }
 
   int readCounts(lst_event* ev, int first, int count, lst_counts* out) {
@@ -400,9 +467,90 @@ namespace {
 }  // namespace
 
 // ================================================================== C ABI
+namespace {
+
+  struct KernelEntry {
+    const char* name;
+    const void* fn;
+  };
+
+  // Every kernel of the library (for launch-resource queries).
+  const std::vector<KernelEntry>& kernelTable() {
+    static const std::vector<KernelEntry> t = {
+        {"kResetEvent", (const void*)lst::kResetEvent},
+        {"kHitPrep", (const void*)lst::kHitPrep},
+        {"kModuleRanges", (const void*)lst::kModuleRanges},
+        {"kPixelIngest", (const void*)lst::kPixelIngest},
+        {"kCreateMD", (const void*)lst::kCreateMD},
+        {"kMDRanges", (const void*)lst::kMDRanges},
+        {"kCreateLS", (const void*)lst::kCreateLS},
+        {"kLSRanges", (const void*)lst::kLSRanges},
+        {"kT3Offsets", (const void*)lst::kT3Offsets},
+        {"kCreateT3", (const void*)lst::kCreateT3},
+        {"kT3Ranges", (const void*)lst::kT3Ranges},
+        {"kT5Eligible", (const void*)lst::kT5Eligible},
+        {"kCreateT5", (const void*)lst::kCreateT5},
+        {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
+        {"kT5Ranges", (const void*)lst::kT5Ranges},
+        {"kPLSClean", (const void*)lst::kPLSClean},
+        {"kMergePLSFlag", (const void*)lst::kMergePLSFlag},
+        {"kPixelConnect", (const void*)lst::kPixelConnect},
+        {"kPT5Count", (const void*)lst::kPT5Count},
+        {"kPT5Emit", (const void*)lst::kPT5Emit},
+        {"kPLSScan", (const void*)lst::kPLSScan},
+        {"kPT5Dedup", (const void*)lst::kPT5Dedup},
+        {"kAddPT5TC", (const void*)lst::kAddPT5TC},
+        {"kPT3Count", (const void*)lst::kPT3Count},
+        {"kPT3Emit", (const void*)lst::kPT3Emit},
+        {"kPT3Dedup", (const void*)lst::kPT3Dedup},
+        {"kCrossCleanPT3", (const void*)lst::kCrossCleanPT3},
+        {"kAddPT3TC", (const void*)lst::kAddPT3TC},
+        {"kT5DedupBeforeTC", (const void*)lst::kT5DedupBeforeTC},
+        {"kMergeT5Flag", (const void*)lst::kMergeT5Flag},
+        {"kCrossCleanT5", (const void*)lst::kCrossCleanT5},
+        {"kT5TCCount", (const void*)lst::kT5TCCount},
+        {"kT5TCScan", (const void*)lst::kT5TCScan},
+        {"kT5TCEmit", (const void*)lst::kT5TCEmit},
+        {"kT5TCFinish", (const void*)lst::kT5TCFinish},
+        {"kCrossCleanPLS", (const void*)lst::kCrossCleanPLS},
+        {"kAddPLSTC", (const void*)lst::kAddPLSTC},
+        {"kCounts", (const void*)lst::kCounts},
+        {"kSetInputCounts", (const void*)lst::kSetInputCounts},
+        {"kUnpack", (const void*)lst::kUnpack},
+        {"kOutputSizes", (const void*)lst::kOutputSizes},
+        {"kOutputEventOffsets", (const void*)lst::kOutputEventOffsets},
+        {"kOutputGather", (const void*)lst::kOutputGather},
+    };
+    return t;
+  }
+
+}  // namespace
+
 extern "C" {
 
 const char* lst_last_error(void) { return g_lastError.c_str(); }
+
+int lst_kernel_count(void) { return static_cast<int>(kernelTable().size()); }
+
+int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_threads_per_block, size_t* local_bytes,
+                          size_t* static_smem_bytes) {
+  const auto& t = kernelTable();
+  if (i < 0 || i >= static_cast<int>(t.size()))
+    return setError("kernel index out of range");
+  cudaFuncAttributes a;
+  LST_CUDA(cudaFuncGetAttributes(&a, t[i].fn));
+  if (name)
+    *name = t[i].name;
+  if (num_regs)
+    *num_regs = a.numRegs;
+  if (max_threads_per_block)
+    *max_threads_per_block = a.maxThreadsPerBlock;
+  if (local_bytes)
+    *local_bytes = a.localSizeBytes;
+  if (static_smem_bytes)
+    *static_smem_bytes = a.sharedSizeBytes;
+  return 0;
+}
 
 int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out) {
   if (!geometry_dir || !out)
@@ -533,6 +681,8 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
   LST_CUDA(cudaMemcpy(ev->dv, ev->hv.data(), sizeof(lst::EventView) * n_slots, cudaMemcpyHostToDevice));
   LST_CUDA(cudaMalloc(&ev->dOffsets, sizeof(unsigned long long) * n_slots));
   LST_CUDA(cudaMallocHost(&ev->hCounts, sizeof(lst_counts) * n_slots));
+  LST_CUDA(cudaMalloc(&ev->dOutOffsets, sizeof(unsigned long long) * 2 * (n_slots + 1)));
+  LST_CUDA(cudaMallocHost(&ev->hOutOffsets, sizeof(unsigned long long) * 2 * (n_slots + 1)));
   // Start every slot empty.
   int rc = runReset(ev.get(), 0, n_slots);
   if (rc)
@@ -554,6 +704,12 @@ void lst_event_destroy(lst_event* ev) {
   if (ev->inbox)
     cudaFree(ev->inbox);
   cudaFreeHost(ev->hCounts);
+  cudaFree(ev->dOutOffsets);
+  cudaFreeHost(ev->hOutOffsets);
+  for (cudaEvent_t e : ev->eventPool)
+    cudaEventDestroy(e);
+  if (ev->dOut)
+    cudaFree(ev->dOut);
   if (ev->ownStream)
     cudaStreamDestroy(ev->stream);
   delete ev;
@@ -614,10 +770,7 @@ int lst_event_add_hits(lst_event* ev, int slot, uint32_t n, const float* x, cons
     LST_CUDA(cudaMemcpyAsync(v.hits.detid, detId, n * sizeof(uint32_t), cudaMemcpyDefault, s));
     LST_CUDA(cudaMemcpyAsync(v.hits.idxs, idxInNtuple, n * sizeof(uint32_t), cudaMemcpyDefault, s));
   }
-  lst::kSetInputCounts<<<1, 1, 0, s>>>(ev->dv, slot, 1, n, 1, 0u, 0u);
-  rc = launchStatus("kSetInputCounts");
-  if (rc)
-    return rc;
+  LST_LAUNCH(lst::kSetInputCounts, 1, 1, ev->dv, slot, 1, n, 1, 0u, 0u);
   return runHitKernels(ev, slot, 1);
 }
 
@@ -663,10 +816,7 @@ int lst_event_add_pixel_segments(lst_event* ev, int slot, uint32_t n, const uint
     LST_CUDA(cudaMemcpyAsync(v.ls.superbin, superbin, size * 4, cudaMemcpyDefault, s));
     LST_CUDA(cudaMemcpyAsync(v.ls.pixelType, pixelType, size, cudaMemcpyDefault, s));
   }
-  lst::kSetInputCounts<<<1, 1, 0, s>>>(ev->dv, slot, 0, 0u, 1, size, status);
-  rc = launchStatus("kSetInputCounts");
-  if (rc)
-    return rc;
+  LST_LAUNCH(lst::kSetInputCounts, 1, 1, ev->dv, slot, 0, 0u, 1, size, status);
   return runPixelIngest(ev, slot, 1);
 }
 
@@ -800,18 +950,17 @@ int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, siz
   cudaStream_t s = ev->stream;
   LST_CUDA(cudaMemcpyAsync(ev->inbox, blobs, total_bytes, cudaMemcpyDefault, s));
   LST_CUDA(cudaMemcpyAsync(ev->dOffsets + first, blob_offsets, sizeof(uint64_t) * count, cudaMemcpyDefault, s));
-  rc = runReset(ev, first, count);
+  ev->inboxValid = true;
+  return ingestInbox(ev, first, count);
+}
+
+int lst_batch_ingest(lst_event* ev, int first, int count) {
+  int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
-  lst::kUnpack<<<dim3(blocksFor(ev->maxHits, count), count), kThreads, 0, s>>>(ev->dv + first, ev->inbox,
-                                                                             ev->dOffsets + first);
-  rc = launchStatus("kUnpack");
-  if (rc)
-    return rc;
-  rc = runHitKernels(ev, first, count);
-  if (rc)
-    return rc;
-  return runPixelIngest(ev, first, count);
+  if (!ev->inboxValid)
+    return setError("lst_batch_ingest: no packed inputs uploaded");
+  return count == 0 ? 0 : ingestInbox(ev, first, count);
 }
 
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage) {
@@ -851,6 +1000,116 @@ int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out) {
   if (count == 0)
     return 0;
   return readCounts(ev, first, count, out);
+}
+
+int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (!out || !out->event_tc_offsets || !out->event_hit_offsets)
+    return setError("lst_batch_get_output: null output");
+  if (count == 0) {
+    out->event_tc_offsets[0] = 0;
+    out->event_hit_offsets[0] = 0;
+    return 0;
+  }
+  cudaStream_t s = ev->stream;
+  const lst::EventView* v = ev->dv + first;
+  LST_LAUNCH(lst::kOutputSizes, dim3(1, count), 1024, v);
+  LST_LAUNCH(lst::kOutputEventOffsets, 1, 1024, v, count, ev->dOutOffsets);
+  const size_t nOff = 2 * (size_t(count) + 1);
+  LST_CUDA(cudaMemcpyAsync(ev->hOutOffsets, ev->dOutOffsets, sizeof(unsigned long long) * nOff,
+                           cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaStreamSynchronize(s));
+  const unsigned long long* tcOff = ev->hOutOffsets;
+  const unsigned long long* hitOff = ev->hOutOffsets + count + 1;
+  for (int i = 0; i <= count; ++i) {
+    out->event_tc_offsets[i] = tcOff[i];
+    out->event_hit_offsets[i] = hitOff[i];
+  }
+  const size_t nTC = tcOff[count], nHits = hitOff[count];
+  if (nTC > out->tc_capacity || nHits > out->hits_capacity)
+    return setError("lst_batch_get_output: output capacity too small (" + std::to_string(nTC) + " candidates, " +
+                    std::to_string(nHits) + " hits needed)");
+  if (nTC == 0)
+    return 0;
+  if (!out->hits || !out->len || !out->seedIdx || !out->type)
+    return setError("lst_batch_get_output: null output array");
+  // Device staging: hits | len | seedIdx | type, each 256-byte aligned.
+  Carver c;
+  c.take<unsigned int>(nHits);
+  c.take<unsigned int>(nTC);
+  c.take<int>(nTC);
+  c.take<short>(nTC);
+  if (c.off > ev->dOutBytes) {
+    if (ev->dOut)
+      LST_CUDA(cudaFree(ev->dOut));
+    ev->dOut = nullptr;
+    ev->dOutBytes = 0;
+    size_t want = (c.off + (4u << 20) - 1) & ~size_t((4u << 20) - 1);
+    LST_CUDA(cudaMalloc(&ev->dOut, want));
+    ev->dOutBytes = want;
+  }
+  Carver d;
+  d.base = reinterpret_cast<char*>(ev->dOut);
+  unsigned int* dHits = d.take<unsigned int>(nHits);
+  unsigned int* dLen = d.take<unsigned int>(nTC);
+  int* dSeed = d.take<int>(nTC);
+  short* dType = d.take<short>(nTC);
+  LST_LAUNCH(lst::kOutputGather, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, v, count,
+             ev->dOutOffsets, dHits, dLen, dSeed, dType);
+  LST_CUDA(cudaMemcpyAsync(out->hits, dHits, nHits * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaMemcpyAsync(out->len, dLen, nTC * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaMemcpyAsync(out->seedIdx, dSeed, nTC * sizeof(int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaMemcpyAsync(out->type, dType, nTC * sizeof(short), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int lst_event_launches(const lst_event* ev, uint64_t* n) {
+  if (!ev || !n)
+    return setError("lst_event_launches: null argument");
+  *n = ev->launches;
+  return 0;
+}
+
+int lst_event_set_profiling(lst_event* ev, int on) {
+  if (!ev)
+    return setError("null event set");
+  LST_CUDA(cudaStreamSynchronize(ev->stream));
+  ev->profiling = on != 0;
+  ev->profile.clear();
+  ev->poolUsed = 0;
+  return 0;
+}
+
+int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int* n_kernels) {
+  if (!ev || !n_kernels)
+    return setError("lst_event_get_profile: null argument");
+  LST_CUDA(cudaStreamSynchronize(ev->stream));
+  std::vector<lst_kernel_time> acc;
+  for (const ProfRecord& r : ev->profile) {
+    float ms = 0.f;
+    LST_CUDA(cudaEventElapsedTime(&ms, r.start, r.stop));
+    const char* name = r.kernel;
+    if (std::strncmp(name, "lst::", 5) == 0)
+      name += 5;
+    auto it = std::find_if(acc.begin(), acc.end(), [&](const lst_kernel_time& k) { return std::strcmp(k.name, name) == 0; });
+    if (it == acc.end()) {
+      lst_kernel_time k{};
+      k.name = name;
+      acc.push_back(k);
+      it = acc.end() - 1;
+    }
+    it->launches += 1;
+    it->total_ms += ms;
+  }
+  *n_kernels = static_cast<int>(acc.size());
+  for (int i = 0; i < static_cast<int>(acc.size()) && i < capacity && out; ++i)
+    out[i] = acc[i];
+  ev->profile.clear();
+  ev->poolUsed = 0;
+  return 0;
 }
 
 }  // extern "C"

@@ -222,4 +222,6 @@
   X(moduleCount, unsigned int, L + 1)                 \
   X(moduleOffset, unsigned int, L + 1)                \
   X(t5Flag, uint8_t, T5)                              \
-  X(plsFlag, uint8_t, P)
+  X(plsFlag, uint8_t, P)                              \
+  X(tcOutLen, unsigned int, TC)                       \
+  X(tcOutOffset, unsigned int, TC)

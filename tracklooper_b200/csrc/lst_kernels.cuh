@@ -422,7 +422,7 @@ namespace lst {
 
   // ============================================================ triplets
   // Per-module triplet offsets (SDL/Triplet.h:1007-1102); one block per event.
-  __global__ void kT3Offsets(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kT3Offsets(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     unsigned int carry = 0;
     for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
@@ -518,7 +518,7 @@ namespace lst {
 
   // ========================================================= quintuplets
   // Eligible T5 seed modules and their offsets (SDL/Quintuplet.h:3117-3213).
-  __global__ void kT5Eligible(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kT5Eligible(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     unsigned int carryN = 0, carryQ = 0;
     for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
@@ -864,7 +864,7 @@ namespace lst {
 
   // Exclusive scan of the per-pLS pass counts; one block per event.
   // which = 0: pT5 (cap 15000), 1: pT3 (cap 5000).
-  __global__ void kPLSScan(DeviceES es, const EventView* evs, int which) {
+  __global__ void __launch_bounds__(1024) kPLSScan(DeviceES es, const EventView* evs, int which) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = ev.ls.nSegments[es.pixelModule];
     unsigned int carry = 0;
@@ -964,7 +964,7 @@ namespace lst {
   }
 
   // pT5 -> TC (SDL/TrackCandidate.h:531-581); one block per event.
-  __global__ void kAddPT5TC(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kAddPT5TC(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt5.nPixelQuintuplets;
     const unsigned int pLS_offset = es.lsOffset[es.nLowerModules];
@@ -1160,7 +1160,7 @@ namespace lst {
   }
 
   // pT3 -> TC (SDL/TrackCandidate.h:383-433); one block per event.
-  __global__ void kAddPT3TC(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kAddPT3TC(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt3.nPixelTriplets;
     const unsigned int pLS_offset = es.lsOffset[es.nLowerModules];
@@ -1317,7 +1317,7 @@ namespace lst {
       ev.moduleCount[warp] = count;
   }
 
-  __global__ void kT5TCScan(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kT5TCScan(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.rg.nEligibleT5Modules;
     unsigned int carry = 0;
@@ -1450,7 +1450,7 @@ namespace lst {
   }
 
   // pLS -> TC (SDL/TrackCandidate.h:489-529, quadruplets only); one block per event.
-  __global__ void kAddPLSTC(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kAddPLSTC(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = ev.ls.nSegments[es.pixelModule];
     const unsigned int start = *ev.tc.nTrackCandidates;
@@ -1671,6 +1671,91 @@ namespace lst {
       ev.sc->nHits = nHits;
       ev.sc->nPLS = nPLS;
       ev.sc->status |= status;
+    }
+  }
+
+
+  // ============================================================ output
+  // Track-candidate output in the form of LST::getOutput
+  // (SDL/LST.cc:367-427): per candidate its type, pixel seed index and the
+  // list of input-ntuple hit indices (14 / 10 / 10 / 4 slots for pT5 / pT3 /
+  // T5 / pLS, a repeated 4th hit of pixel objects dropped).
+  __device__ __forceinline__ int tcOutputHits(const EventView& ev, unsigned int idx, unsigned int* out) {
+    const short type = ev.tc.trackCandidateType[idx];
+    const int maxN = type == 7 ? 14 : (type == 5 ? 10 : (type == 4 ? 10 : (type == 8 ? 4 : 0)));
+    int n = 0;
+    unsigned int last = 0;
+    for (int i = 0; i < maxN; ++i) {
+      unsigned int g = ev.tc.hitIndices[14 * idx + i];
+      unsigned int h = (type == 8) ? g : ev.hits.idxs[g];
+      if (type != 4 && n == 3 && last == h)
+        continue;
+      if (out)
+        out[n] = h;
+      ++n;
+      last = h;
+    }
+    return n;
+  }
+
+  // Per event: output length of every candidate and their offsets; one block
+  // per event.
+  __global__ void __launch_bounds__(1024) kOutputSizes(const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.tc.nTrackCandidates;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int len = (i < n) ? static_cast<unsigned int>(tcOutputHits(ev, i, nullptr)) : 0u;
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(len, tot);
+      if (i < n) {
+        ev.tcOutLen[i] = len;
+        ev.tcOutOffset[i] = carry + ex;
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0)
+      ev.sc->nOutHits = carry;
+  }
+
+  // Offsets of each event's candidates and hits inside the batch output
+  // (exclusive scans over the events); one block.
+  __global__ void __launch_bounds__(1024) kOutputEventOffsets(const EventView* evs, int count,
+                                                              unsigned long long* offsets) {
+    unsigned long long carryTC = 0, carryHits = 0;
+    for (int base = 0; base < count; base += blockDim.x) {
+      int i = base + threadIdx.x;
+      unsigned int ntc = (i < count) ? *evs[i].tc.nTrackCandidates : 0u;
+      unsigned int nh = (i < count) ? evs[i].sc->nOutHits : 0u;
+      unsigned int totTC, totH;
+      unsigned int exTC = blockExclusiveScan(ntc, totTC);
+      unsigned int exH = blockExclusiveScan(nh, totH);
+      if (i < count) {
+        offsets[i] = carryTC + exTC;
+        offsets[count + 1 + i] = carryHits + exH;
+      }
+      carryTC += totTC;
+      carryHits += totH;
+    }
+    if (threadIdx.x == 0) {
+      offsets[count] = carryTC;
+      offsets[2 * count + 1] = carryHits;
+    }
+  }
+
+  // Writes the batch output: hits, len, seedIdx and type, contiguous.
+  __global__ void kOutputGather(const EventView* evs, int count, const unsigned long long* offsets,
+                                unsigned int* outHits, unsigned int* outLen, int* outSeed, short* outType) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.tc.nTrackCandidates;
+    const unsigned long long tc0 = offsets[blockIdx.y];
+    const unsigned long long h0 = offsets[count + 1 + blockIdx.y];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      tcOutputHits(ev, i, outHits + h0 + ev.tcOutOffset[i]);
+      outLen[tc0 + i] = ev.tcOutLen[i];
+      outSeed[tc0 + i] = ev.tc.pixelSeedIndex[i];
+      outType[tc0 + i] = ev.tc.trackCandidateType[i];
     }
   }
 

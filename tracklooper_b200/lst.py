@@ -62,6 +62,8 @@ STATUS_BITS = {
 # Exported symbols of include/lst_b200.h.
 EXPORTS = (
     "lst_last_error",
+    "lst_kernel_count",
+    "lst_kernel_attributes",
     "lst_es_load",
     "lst_es_free",
     "lst_es_get_info",
@@ -92,8 +94,13 @@ EXPORTS = (
     "lst_field_info",
     "lst_packed_size",
     "lst_batch_upload",
+    "lst_batch_ingest",
     "lst_batch_run",
     "lst_batch_get_counts",
+    "lst_batch_get_output",
+    "lst_event_launches",
+    "lst_event_set_profiling",
+    "lst_event_get_profile",
 )
 
 
@@ -140,6 +147,25 @@ class Counts(ctypes.Structure):
         return out
 
 
+class Output(ctypes.Structure):
+    """lst_output (include/lst_b200.h)."""
+
+    _fields_ = [
+        ("hits", ctypes.c_void_p),
+        ("hits_capacity", ctypes.c_size_t),
+        ("len", ctypes.c_void_p),
+        ("seedIdx", ctypes.c_void_p),
+        ("type", ctypes.c_void_p),
+        ("tc_capacity", ctypes.c_size_t),
+        ("event_tc_offsets", ctypes.c_void_p),
+        ("event_hit_offsets", ctypes.c_void_p),
+    ]
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
+
+
 class EsInfo(ctypes.Structure):
     _fields_ = [
         ("nModules", ctypes.c_uint32),
@@ -168,6 +194,9 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib = ctypes.CDLL(path)
         vp, u32, i32, sz = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_size_t
         lib.lst_last_error.restype = ctypes.c_char_p
+        lib.lst_kernel_count.argtypes = []
+        lib.lst_kernel_attributes.argtypes = [i32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(i32),
+                                              ctypes.POINTER(i32), ctypes.POINTER(sz), ctypes.POINTER(sz)]
         lib.lst_es_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, ctypes.POINTER(vp)]
         lib.lst_es_free.argtypes = [vp]
         lib.lst_es_free.restype = None
@@ -196,8 +225,13 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_packed_size.argtypes = [u32, u32]
         lib.lst_packed_size.restype = sz
         lib.lst_batch_upload.argtypes = [vp, i32, i32, vp, sz, vp]
+        lib.lst_batch_ingest.argtypes = [vp, i32, i32]
         lib.lst_batch_run.argtypes = [vp, i32, i32, i32, i32]
         lib.lst_batch_get_counts.argtypes = [vp, i32, i32, ctypes.POINTER(Counts)]
+        lib.lst_batch_get_output.argtypes = [vp, i32, i32, ctypes.POINTER(Output)]
+        lib.lst_event_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+        lib.lst_event_set_profiling.argtypes = [vp, i32]
+        lib.lst_event_get_profile.argtypes = [vp, ctypes.POINTER(KernelTime), i32, ctypes.POINTER(i32)]
         _lib = lib
         return lib
 
@@ -207,6 +241,20 @@ def _check(rc: int, what: str) -> int:
         msg = library().lst_last_error().decode(errors="replace")
         raise LSTError(f"{what}: {msg}")
     return rc
+
+
+def kernel_attributes() -> list[dict]:
+    """Registers, maximum block size and memory of every kernel (needs a GPU)."""
+    lib = library()
+    out = []
+    for i in range(lib.lst_kernel_count()):
+        name, regs, mt = ctypes.c_char_p(), ctypes.c_int(), ctypes.c_int()
+        local, smem = ctypes.c_size_t(), ctypes.c_size_t()
+        _check(lib.lst_kernel_attributes(i, ctypes.byref(name), ctypes.byref(regs), ctypes.byref(mt),
+                                         ctypes.byref(local), ctypes.byref(smem)), "lst_kernel_attributes")
+        out.append({"name": name.value.decode(), "regs": regs.value, "max_threads": mt.value,
+                    "local_bytes": local.value, "smem_bytes": smem.value})
+    return out
 
 
 def field_names() -> list[str]:
@@ -362,9 +410,41 @@ class EventSet:
         _check(library().lst_batch_upload(self._h, first, offsets.size, blobs.ctypes.data, blobs.nbytes,
                                           offsets.ctypes.data), "lst_batch_upload")
 
+    def ingest(self, first: int, count: int):
+        _check(library().lst_batch_ingest(self._h, first, count), "lst_batch_ingest")
+
     def run(self, first: int, count: int, first_stage: int = STAGE_MINI_DOUBLETS,
             last_stage: int = STAGE_TRACK_CANDIDATES):
         _check(library().lst_batch_run(self._h, first, count, first_stage, last_stage), "lst_batch_run")
+
+    def output(self, first: int, count: int, tc_capacity: int = 31000, hits_capacity: int = 31000 * 14):
+        """LST::getOutput for slots [first, first + count): (hits, len, seedIdx, type, tc_offsets, hit_offsets)."""
+        hits = np.empty(hits_capacity, np.uint32)
+        ln = np.empty(tc_capacity, np.uint32)
+        seed = np.empty(tc_capacity, np.int32)
+        typ = np.empty(tc_capacity, np.int16)
+        tco = np.empty(count + 1, np.uint64)
+        hco = np.empty(count + 1, np.uint64)
+        o = Output(hits.ctypes.data, hits.size, ln.ctypes.data, seed.ctypes.data, typ.ctypes.data, ln.size,
+                   tco.ctypes.data, hco.ctypes.data)
+        _check(library().lst_batch_get_output(self._h, first, count, ctypes.byref(o)), "lst_batch_get_output")
+        ntc, nh = int(tco[-1]), int(hco[-1])
+        return hits[:nh], ln[:ntc], seed[:ntc], typ[:ntc], tco, hco
+
+    def launches(self) -> int:
+        n = ctypes.c_uint64()
+        _check(library().lst_event_launches(self._h, ctypes.byref(n)), "lst_event_launches")
+        return n.value
+
+    def set_profiling(self, on: bool):
+        _check(library().lst_event_set_profiling(self._h, int(bool(on))), "lst_event_set_profiling")
+
+    def profile(self) -> dict:
+        """{kernel: (launches, total ms)} since profiling was switched on or last read."""
+        arr = (KernelTime * 128)()
+        n = ctypes.c_int()
+        _check(library().lst_event_get_profile(self._h, arr, 128, ctypes.byref(n)), "lst_event_get_profile")
+        return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(min(n.value, 128))}
 
     def batch_counts(self, first: int, count: int) -> list[dict]:
         arr = (Counts * count)()
@@ -503,6 +583,12 @@ class Event:
 
     def getNumberOfT5TrackCandidates(self):
         return self.counts()["nTrackCandidatesT5"]
+
+    def getOutput(self):
+        """LST::getOutput: (hits per candidate, len, seedIdx, trackCandidateType)."""
+        hits, ln, seed, typ, _, _ = self._set.output(self._slot, 1)
+        bounds = np.concatenate(([0], np.cumsum(ln.astype(np.int64))))
+        return [hits[bounds[i]:bounds[i + 1]].tolist() for i in range(ln.size)], ln, seed, typ
 
     def run(self, inp, upto: str = "tc"):
         """addHitToEvent + addPixelSegmentToEvent + stages in LST::run order."""
