@@ -240,6 +240,22 @@ typedef struct lst_output {
 } lst_output;
 int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out);
 
+/* lst_batch_get_output without any device allocation (no reference
+ * counterpart: the reference allocates its host copies in getOutput).
+ * lst_batch_get_output grows its device staging buffer with cudaMalloc when a
+ * batch needs more room; callers that cannot allocate device memory at that
+ * point -- a framework whose caching allocator owns the device memory budget,
+ * or a producer that must not stall other streams with the device-wide
+ * synchronisation of cudaMalloc / cudaFree -- call this one.  It stages in a
+ * fixed 4 MiB device array compiled into the library (about 20 PU200-shaped
+ * events per call) and rejects a call whose output does not fit (or of more
+ * than 1023 events) with an error naming the size: split the slot range.  The
+ * first call on each device looks the array up (cudaGetSymbolAddress with
+ * that device current); make that first call before any stream capture.  All
+ * event sets of a device share the array, so calls that overlap in time (on
+ * different streams or host threads) race: serialise them. */
+int lst_batch_get_output_static(lst_event* ev, int first, int count, lst_output* out);
+
 /* ---------------------------------------------------------- accounting */
 /* Number of kernels the set has launched since it was created. */
 int lst_event_launches(const lst_event* ev, uint64_t* n);

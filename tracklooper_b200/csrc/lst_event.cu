@@ -12,6 +12,7 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <type_traits>
@@ -1058,6 +1059,131 @@ int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out) {
   short* dType = d.take<short>(nTC);
   LST_LAUNCH(lst::kOutputGather, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, v, count,
              ev->dOutOffsets, dHits, dLen, dSeed, dType);
+  LST_CUDA(cudaMemcpyAsync(out->hits, dHits, nHits * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaMemcpyAsync(out->len, dLen, nTC * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaMemcpyAsync(out->seedIdx, dSeed, nTC * sizeof(int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaMemcpyAsync(out->type, dType, nTC * sizeof(short), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------- output without device allocation
+// lst_batch_get_output stages the flattened track-candidate output in a device
+// buffer that it grows with cudaMalloc when a batch needs more room.  Some
+// callers cannot allocate at that point: a framework whose caching allocator
+// owns the device memory budget, or a producer that must not call cudaFree /
+// cudaMalloc between events because those calls synchronise the whole device
+// and stall the other streams.  lst_batch_get_output_static does the same work
+// with its staging in a fixed, file-scope device array instead.
+namespace {
+
+  // Bytes of the static staging array, and the part of it that holds the
+  // per-event offsets (2 x (events + 1) x 8 bytes).
+  constexpr size_t kStaticOutputBytes = size_t(4) << 20;
+  constexpr size_t kStaticOffsetBytes = size_t(16) << 10;
+  constexpr int kStaticOutputMaxEvents = static_cast<int>(kStaticOffsetBytes / (2 * sizeof(unsigned long long))) - 1;
+
+  static __device__ __align__(256) unsigned char g_staticOutput[kStaticOutputBytes];
+
+  // Device address of g_staticOutput per device, looked up once per device
+  // with that device current.
+  constexpr int kMaxDevices = 64;
+  std::mutex g_staticOutputMutex;
+  unsigned char* g_staticOutputPtr[kMaxDevices] = {};
+
+  int staticOutputScratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kMaxDevices)
+      return setError("device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_staticOutputMutex);
+    if (!g_staticOutputPtr[device]) {
+      int current = 0;
+      LST_CUDA(cudaGetDevice(&current));
+      if (current != device)
+        LST_CUDA(cudaSetDevice(device));
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_staticOutput);
+      if (current != device)
+        cudaSetDevice(current);
+      if (e != cudaSuccess)
+        return cudaFail(e, "cudaGetSymbolAddress(static output staging)");
+      g_staticOutputPtr[device] = static_cast<unsigned char*>(p);
+    }
+    *out = g_staticOutputPtr[device];
+    return 0;
+  }
+
+  // Launch without the profiling hook (which creates CUDA events on demand).
+#define LST_LAUNCH_PLAIN(kernel, grid, block, ...)             \
+  do {                                                         \
+    kernel<<<(grid), (block), 0, s>>>(__VA_ARGS__);            \
+    cudaError_t e_ = cudaGetLastError();                       \
+    if (e_ != cudaSuccess)                                     \
+      return cudaFail(e_, #kernel);                            \
+    ++ev->launches;                                            \
+  } while (0)
+
+}  // namespace
+
+extern "C" {
+
+int lst_batch_get_output_static(lst_event* ev, int first, int count, lst_output* out) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (!out || !out->event_tc_offsets || !out->event_hit_offsets)
+    return setError("lst_batch_get_output_static: null output");
+  if (count == 0) {
+    out->event_tc_offsets[0] = 0;
+    out->event_hit_offsets[0] = 0;
+    return 0;
+  }
+  if (count > kStaticOutputMaxEvents)
+    return setError("lst_batch_get_output_static: at most " + std::to_string(kStaticOutputMaxEvents) +
+                    " events per call (split the slot range)");
+  unsigned char* scratch = nullptr;
+  rc = staticOutputScratch(ev->es->device, &scratch);
+  if (rc)
+    return rc;
+  // Every byte of the staging that is read in this call is first written in
+  // this call (scans write all offsets, the gather all output entries), so
+  // nothing needs clearing.
+  unsigned long long* dOffsets = reinterpret_cast<unsigned long long*>(scratch);
+  cudaStream_t s = ev->stream;
+  const lst::EventView* v = ev->dv + first;
+  LST_LAUNCH_PLAIN(lst::kOutputSizes, dim3(1, count), 1024, v);
+  LST_LAUNCH_PLAIN(lst::kOutputEventOffsets, 1, 1024, v, count, dOffsets);
+  LST_CUDA(cudaMemcpyAsync(out->event_tc_offsets, dOffsets, sizeof(uint64_t) * (count + 1), cudaMemcpyDeviceToHost,
+                           s));
+  LST_CUDA(cudaMemcpyAsync(out->event_hit_offsets, dOffsets + count + 1, sizeof(uint64_t) * (count + 1),
+                           cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaStreamSynchronize(s));
+  const size_t nTC = out->event_tc_offsets[count], nHits = out->event_hit_offsets[count];
+  if (nTC > out->tc_capacity || nHits > out->hits_capacity)
+    return setError("lst_batch_get_output_static: output capacity too small (" + std::to_string(nTC) +
+                    " candidates, " + std::to_string(nHits) + " hits needed)");
+  Carver need;
+  need.take<unsigned int>(nHits);
+  need.take<unsigned int>(nTC);
+  need.take<int>(nTC);
+  need.take<short>(nTC);
+  if (kStaticOffsetBytes + need.off > kStaticOutputBytes)
+    return setError("lst_batch_get_output_static: the output of these events needs " +
+                    std::to_string(kStaticOffsetBytes + need.off) + " bytes of staging, more than the " +
+                    std::to_string(kStaticOutputBytes) + "-byte static buffer (split the slot range)");
+  if (nTC == 0)
+    return 0;
+  if (!out->hits || !out->len || !out->seedIdx || !out->type)
+    return setError("lst_batch_get_output_static: null output array");
+  Carver d;
+  d.base = reinterpret_cast<char*>(scratch + kStaticOffsetBytes);
+  unsigned int* dHits = d.take<unsigned int>(nHits);
+  unsigned int* dLen = d.take<unsigned int>(nTC);
+  int* dSeed = d.take<int>(nTC);
+  short* dType = d.take<short>(nTC);
+  LST_LAUNCH_PLAIN(lst::kOutputGather, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, v, count,
+                   dOffsets, dHits, dLen, dSeed, dType);
   LST_CUDA(cudaMemcpyAsync(out->hits, dHits, nHits * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
   LST_CUDA(cudaMemcpyAsync(out->len, dLen, nTC * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
   LST_CUDA(cudaMemcpyAsync(out->seedIdx, dSeed, nTC * sizeof(int), cudaMemcpyDeviceToHost, s));
