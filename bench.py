@@ -77,6 +77,23 @@ def dist_env():
     return rank, world, local
 
 
+def rank_first_event(rank: int, batch: int) -> int:
+    """First generator index of a rank's batch: ranks take disjoint events."""
+    return rank * batch
+
+
+def reduce_max(value: float, world: int, device=None) -> float:
+    """Max of `value` over the ranks (the timing rule for N > 1)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as tdist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def generate(config: int, first: int, n: int, workers: int):
     from tracklooper_b200 import gen
 
@@ -241,11 +258,7 @@ def run_ours(args, rank, world, local, events):
         l1 = eset.launches()
         clocks = sampler.stop() if sampler else None
         torch.cuda.synchronize()
-        ms = start.elapsed_time(stop)
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = reduce_max(start.elapsed_time(stop), world, dev)
         return ms, l1 - l0, clocks
 
     # warm-up
@@ -457,7 +470,7 @@ def main():
         import datetime
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    events = generate(args.config, rank * args.batch, args.batch, ncpu)
+    events = generate(args.config, rank_first_event(rank, args.batch), args.batch, ncpu)
     res = run_ours(args, rank, world, local, events)
 
     cpu = None

@@ -116,6 +116,15 @@ int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_thre
  * (SDL/LSTESData.h:79-80, SDL/LSTESData.cc:79-126). */
 int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out);
 void lst_es_free(lst_es* es);
+/* Loads the geometry on the host only (no device, no upload): for inspecting
+ * the event setup.  Such a handle cannot create event sets. */
+int lst_es_load_host(const char* geometry_dir, lst_es** out);
+/* Host copy of one event-setup array by the reference's name
+ * (modules.<field> of SDL/Module.h:161-262, pixelmap.<field> of
+ * SDL/PixelMap.h:16-29, endcap.geoMapDetId / endcap.geoMapPhi of
+ * SDL/EndcapGeometry.h) or caps.<mdOffset|mdCap|lsOffset|lsCap|t3CapIfUsed|
+ * t5CapIfEligible> (the static per-module offsets and occupancy caps). */
+int lst_es_host_array(const lst_es* es, const char* name, const void** data, size_t* n_elems, size_t* elem_size);
 int lst_es_get_info(const lst_es* es, lst_es_info* out);
 /* Replaces the T5 DNN weights (same layout as the file).  The weights live
  * in constant memory of the ES's device and are shared by every event set on

@@ -176,3 +176,35 @@ def stage_fields(all_names, stages):
     for st in stages:
         stores.update(STAGE_STORES[st])
     return [n for n in all_names if n.split(".", 1)[0] in stores or n.startswith("ranges.")]
+
+
+# Fields whose live entries are digested for the golden fixtures: every
+# object's identity (its hits / constituents) and one float per object type.
+DIGEST_FIELDS = (
+    "md.anchorHitIndices", "md.outerHitIndices", "md.anchorPhi",
+    "ls.mdIndices", "ls.dPhiChanges",
+    "t3.segmentIndices", "t3.betaIn",
+    "t5.tripletIndices", "t5.score_rphisum", "t5.TightCutFlag", "t5.isDup",
+    "pt3.pixelSegmentIndices", "pt3.tripletIndices", "pt3.score", "pt3.isDup",
+    "pt5.pixelIndices", "pt5.T5Indices", "pt5.score", "pt5.isDup",
+    "tc.trackCandidateType", "tc.hitIndices", "tc.pixelSeedIndex", "tc.objectIndices",
+)
+
+
+def store_digests(get, n_lower: int, n_hits: int, sizes: dict) -> dict:
+    """sha256 of the live entries of DIGEST_FIELDS (bit patterns for floats)."""
+    import hashlib
+
+    si = StoreIndex(get, n_lower, n_hits)
+    out = {}
+    for name in DIGEST_FIELDS:
+        a = get(name)
+        store = name.split(".", 1)[0]
+        sel = _object_index(store, name, a.size, si, sizes)
+        if sel is None:
+            v = a
+        else:
+            idx, mult = sel
+            v = a[_expand(idx, mult)]
+        out[name] = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()[:32]
+    return out

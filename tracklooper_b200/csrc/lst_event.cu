@@ -595,6 +595,76 @@ int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int de
   return 0;
 }
 
+int lst_es_load_host(const char* geometry_dir, lst_es** out) {
+  if (!geometry_dir || !out)
+    return setError("lst_es_load_host: null argument");
+  *out = nullptr;
+  std::unique_ptr<lst_es> es(new (std::nothrow) lst_es());
+  if (!es)
+    return setError("out of host memory");
+  es->device = -1;
+  std::string err = lst::loadEsHost(geometry_dir, es->host);
+  if (!err.empty())
+    return setError(err);
+  *out = es.release();
+  return 0;
+}
+
+int lst_es_host_array(const lst_es* es, const char* name, const void** data, size_t* n_elems, size_t* elem_size) {
+  if (!es || !name || !data)
+    return setError("lst_es_host_array: null argument");
+  const lst::EsHost& h = es->host;
+  const std::string key(name);
+#define LST_ES_ARRAY(prefix, vec)                 \
+  if (key == prefix #vec) {                       \
+    *data = h.vec.data();                         \
+    if (n_elems)                                  \
+      *n_elems = h.vec.size();                    \
+    if (elem_size)                                \
+      *elem_size = sizeof(h.vec[0]);              \
+    return 0;                                     \
+  }
+  LST_ES_ARRAY("modules.", detIds)
+  LST_ES_ARRAY("modules.", moduleMap)
+  LST_ES_ARRAY("modules.", mapdetId)
+  LST_ES_ARRAY("modules.", mapIdx)
+  LST_ES_ARRAY("modules.", nConnectedModules)
+  LST_ES_ARRAY("modules.", drdzs)
+  LST_ES_ARRAY("modules.", dxdys)
+  LST_ES_ARRAY("modules.", partnerModuleIndices)
+  LST_ES_ARRAY("modules.", layers)
+  LST_ES_ARRAY("modules.", rings)
+  LST_ES_ARRAY("modules.", modules)
+  LST_ES_ARRAY("modules.", rods)
+  LST_ES_ARRAY("modules.", subdets)
+  LST_ES_ARRAY("modules.", sides)
+  LST_ES_ARRAY("modules.", eta)
+  LST_ES_ARRAY("modules.", r)
+  LST_ES_ARRAY("modules.", isInverted)
+  LST_ES_ARRAY("modules.", isLower)
+  LST_ES_ARRAY("modules.", isAnchor)
+  LST_ES_ARRAY("modules.", moduleType)
+  LST_ES_ARRAY("modules.", moduleLayerType)
+  LST_ES_ARRAY("modules.", sdlLayers)
+  LST_ES_ARRAY("modules.", connectedPixels)
+  LST_ES_ARRAY("pixelmap.", connectedPixelsIndex)
+  LST_ES_ARRAY("pixelmap.", connectedPixelsSizes)
+  LST_ES_ARRAY("pixelmap.", connectedPixelsIndexPos)
+  LST_ES_ARRAY("pixelmap.", connectedPixelsSizesPos)
+  LST_ES_ARRAY("pixelmap.", connectedPixelsIndexNeg)
+  LST_ES_ARRAY("pixelmap.", connectedPixelsSizesNeg)
+  LST_ES_ARRAY("endcap.", geoMapDetId)
+  LST_ES_ARRAY("endcap.", geoMapPhi)
+  LST_ES_ARRAY("caps.", mdOffset)
+  LST_ES_ARRAY("caps.", mdCap)
+  LST_ES_ARRAY("caps.", lsOffset)
+  LST_ES_ARRAY("caps.", lsCap)
+  LST_ES_ARRAY("caps.", t3CapIfUsed)
+  LST_ES_ARRAY("caps.", t5CapIfEligible)
+#undef LST_ES_ARRAY
+  return setError("unknown event-setup array " + key);
+}
+
 void lst_es_free(lst_es* es) {
   if (!es)
     return;
@@ -631,6 +701,8 @@ int lst_es_set_t5dnn_weights(lst_es* es, const float* weights, size_t n) {
 int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, lst_event** out) {
   if (!es || !out || n_slots <= 0 || max_hits == 0)
     return setError("lst_event_create: bad argument");
+  if (es->device < 0 || !es->arena)
+    return setError("lst_event_create: the event setup was loaded on the host only");
   *out = nullptr;
   std::unique_ptr<lst_event> ev(new (std::nothrow) lst_event());
   if (!ev)

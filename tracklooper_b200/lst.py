@@ -66,6 +66,8 @@ EXPORTS = (
     "lst_kernel_attributes",
     "lst_es_load",
     "lst_es_free",
+    "lst_es_load_host",
+    "lst_es_host_array",
     "lst_es_get_info",
     "lst_es_set_t5dnn_weights",
     "lst_event_create",
@@ -201,6 +203,8 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_es_free.argtypes = [vp]
         lib.lst_es_free.restype = None
         lib.lst_es_get_info.argtypes = [vp, ctypes.POINTER(EsInfo)]
+        lib.lst_es_load_host.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]
+        lib.lst_es_host_array.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp), ctypes.POINTER(sz), ctypes.POINTER(sz)]
         lib.lst_es_set_t5dnn_weights.argtypes = [vp, vp, sz]
         lib.lst_event_create.argtypes = [vp, i32, u32, vp, ctypes.POINTER(vp)]
         lib.lst_event_destroy.argtypes = [vp]
@@ -301,6 +305,44 @@ class ES:
     def set_t5dnn_weights(self, w: np.ndarray):
         w = np.ascontiguousarray(w, dtype=np.float32).ravel()
         _check(library().lst_es_set_t5dnn_weights(self._h, w.ctypes.data, w.size), "lst_es_set_t5dnn_weights")
+
+    def close(self):
+        if self._h:
+            library().lst_es_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostES:
+    """Event setup loaded on the host only (lst_es_load_host), for inspection."""
+
+    def __init__(self, geometry_dir: str | None = None):
+        lib = library()
+        h = ctypes.c_void_p()
+        gdir = geometry_dir or geometry.geometry_dir()
+        _check(lib.lst_es_load_host(gdir.encode(), ctypes.byref(h)), "lst_es_load_host")
+        self._h = h
+        info = EsInfo()
+        _check(lib.lst_es_get_info(h, ctypes.byref(info)), "lst_es_get_info")
+        self.info = {n: int(getattr(info, n)) for n, _ in EsInfo._fields_}
+
+    def array(self, name: str, dtype) -> np.ndarray:
+        lib = library()
+        p, n, esz = ctypes.c_void_p(), ctypes.c_size_t(), ctypes.c_size_t()
+        _check(lib.lst_es_host_array(self._h, name.encode(), ctypes.byref(p), ctypes.byref(n), ctypes.byref(esz)),
+               f"es array {name}")
+        dt = np.dtype(dtype)
+        if dt.itemsize != esz.value:
+            raise LSTError(f"{name}: element size {esz.value}, asked for {dt}")
+        if n.value == 0:
+            return np.zeros(0, dt)
+        buf = (ctypes.c_char * (n.value * esz.value)).from_address(p.value)
+        return np.frombuffer(buf, dtype=dt).copy()
 
     def close(self):
         if self._h:
