@@ -27,7 +27,9 @@ def es():
 
 @pytest.fixture(scope="module")
 def event(es):
-    return lst.Event(es, max_hits=300000)
+    ev = lst.Event(es, max_hits=300000)
+    yield ev
+    ev.event_set.close()
 
 
 @pytest.mark.parametrize("rec", PINS["events"], ids=lambda r: f"cfg{r['config']}-ev{r['index']}")

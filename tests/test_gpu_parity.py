@@ -34,7 +34,9 @@ def es():
 
 @pytest.fixture(scope="module")
 def event(es):
-    return lst.Event(es, max_hits=400000)
+    ev = lst.Event(es, max_hits=400000)
+    yield ev
+    ev.event_set.close()
 
 
 def _sizes(es, event):

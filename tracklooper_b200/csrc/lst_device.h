@@ -84,6 +84,16 @@ namespace lst {
     uint8_t* plsFlag;  // removal marks of the second pLS cleaning pass
     unsigned int* tcOutLen;     // output hits per track candidate
     unsigned int* tcOutOffset;  // offset of a candidate's hits in the event's output
+    // MD-keyed indices: per module, segments / triplets grouped by their first
+    // MD (module-relative indices), with per-MD start and count
+    uint16_t* lsByMD;
+    uint16_t* mdLSStart;
+    uint16_t* mdLSCount;
+    uint16_t* t3ByMD;
+    uint16_t* mdT3Start;
+    uint16_t* mdT3Count;
+    unsigned int* plsOrder;     // pLS indices sorted by eta bin
+    unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
     unsigned int maxHits;
   };
 

@@ -49,6 +49,7 @@ namespace {
   // same stream (see lst_event_set_profiling).
 #define LST_LAUNCH(kernel, grid, block, ...)                   \
   do {                                                         \
+    cudaGetLastError(); /* drop a stale non-sticky error */    \
     cudaEvent_t p0_ = nullptr;                                 \
     if (ev->profiling && (p0_ = profEvent(ev)))                \
       cudaEventRecord(p0_, s);                                 \
@@ -263,6 +264,7 @@ namespace {
 
 struct lst_event {
   lst_es* es = nullptr;
+  int device = 0;
   int nSlots = 0;
   unsigned int maxHits = 0;
   cudaStream_t stream = nullptr;
@@ -375,11 +377,13 @@ namespace {
       case LST_STAGE_SEGMENTS:
         LST_LAUNCH(lst::kCreateLS, warpGrid(nLower, lst::kLSWarps, count), 32 * lst::kLSWarps, d, v);
         LST_LAUNCH(lst::kLSRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kLSByMD, warpGrid(nLower, lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
       case LST_STAGE_TRIPLETS:
         LST_LAUNCH(lst::kT3Offsets, one, 1024, d, v);
         LST_LAUNCH(lst::kCreateT3, warpGrid(nLower, lst::kT3Warps, count), 32 * lst::kT3Warps, d, v);
         LST_LAUNCH(lst::kT3Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kT3ByMD, warpGrid(nLower, lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
       case LST_STAGE_QUINTUPLETS: {
         if (ev->t5Method == LST_T5_DNN && !ev->es->haveDnn)
@@ -392,6 +396,7 @@ namespace {
         break;
       }
       case LST_STAGE_PLS_CLEANING:
+        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
         LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, false);
         break;
       case LST_STAGE_PIXEL_QUINTUPLETS:
@@ -399,7 +404,8 @@ namespace {
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 0);
         LST_LAUNCH(lst::kPT5Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
-        LST_LAUNCH(lst::kPT5Dedup, dim3(blocksFor(lst::kMaxPixelQuintuplets, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPT5Dedup, dim3(blocksFor(lst::kMaxPixelQuintuplets, count, lst::kDedupTile), count),
+                   lst::kDedupTile, d, v);
         LST_LAUNCH(lst::kAddPT5TC, one, 1024, d, v);
         break;
       case LST_STAGE_PIXEL_TRIPLETS:
@@ -421,6 +427,7 @@ namespace {
         LST_LAUNCH(lst::kT5TCScan, one, 1024, d, v);
         LST_LAUNCH(lst::kT5TCEmit, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kT5TCFinish, one, 32, d, v);
+        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
         LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, true);
         LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kCrossCleanPLS, dim3(blocksFor(P, count), count), kThreads, d, v);
@@ -488,11 +495,14 @@ namespace {
         {"kLSRanges", (const void*)lst::kLSRanges},
         {"kT3Offsets", (const void*)lst::kT3Offsets},
         {"kCreateT3", (const void*)lst::kCreateT3},
+        {"kLSByMD", (const void*)lst::kLSByMD},
+        {"kT3ByMD", (const void*)lst::kT3ByMD},
         {"kT3Ranges", (const void*)lst::kT3Ranges},
         {"kT5Eligible", (const void*)lst::kT5Eligible},
         {"kCreateT5", (const void*)lst::kCreateT5},
         {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
         {"kT5Ranges", (const void*)lst::kT5Ranges},
+        {"kPLSBin", (const void*)lst::kPLSBin},
         {"kPLSClean", (const void*)lst::kPLSClean},
         {"kMergePLSFlag", (const void*)lst::kMergePLSFlag},
         {"kPixelConnect", (const void*)lst::kPixelConnect},
@@ -708,6 +718,7 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
   if (!ev)
     return setError("out of host memory");
   ev->es = es;
+  ev->device = es->device;
   ev->nSlots = n_slots;
   ev->maxHits = max_hits;
   ev->t5Method = es->haveDnn ? LST_T5_DNN : LST_T5_CUTS;
@@ -768,7 +779,7 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
 void lst_event_destroy(lst_event* ev) {
   if (!ev)
     return;
-  cudaSetDevice(ev->es->device);
+  cudaSetDevice(ev->device);
   cudaStreamSynchronize(ev->stream);
   cudaFree(ev->arena);
   cudaFree(ev->dv);
@@ -1189,6 +1200,7 @@ namespace {
   // Launch without the profiling hook (which creates CUDA events on demand).
 #define LST_LAUNCH_PLAIN(kernel, grid, block, ...)             \
   do {                                                         \
+    cudaGetLastError(); /* drop a stale non-sticky error */    \
     kernel<<<(grid), (block), 0, s>>>(__VA_ARGS__);            \
     cudaError_t e_ = cudaGetLastError();                       \
     if (e_ != cudaSuccess)                                     \

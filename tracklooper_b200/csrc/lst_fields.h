@@ -224,4 +224,12 @@
   X(t5Flag, uint8_t, T5)                              \
   X(plsFlag, uint8_t, P)                              \
   X(tcOutLen, unsigned int, TC)                       \
-  X(tcOutOffset, unsigned int, TC)
+  X(tcOutOffset, unsigned int, TC)                    \
+  X(lsByMD, uint16_t, LS)                             \
+  X(mdLSStart, uint16_t, MD)                          \
+  X(mdLSCount, uint16_t, MD)                          \
+  X(t3ByMD, uint16_t, T3)                             \
+  X(mdT3Start, uint16_t, MD)                          \
+  X(mdT3Count, uint16_t, MD)                          \
+  X(plsOrder, unsigned int, P)                        \
+  X(plsBinStart, unsigned int, 128)

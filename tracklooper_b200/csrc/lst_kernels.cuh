@@ -420,6 +420,107 @@ namespace lst {
     }
   }
 
+  // ================================================= MD-keyed indices
+  // For one module: the objects [0, n) of the module (segments or triplets,
+  // in storage order) grouped by the module-local index of their first
+  // mini-doublet, stably, so that each group keeps storage order.  Written:
+  // start[md] / count[md] for every MD of the module, perm[] the object
+  // indices (module-relative).  One warp; `bins` / `cursor` are warp-private
+  // shared arrays of kMaxModuleMDs entries.
+  constexpr int kMaxModuleMDs = 128;
+
+  template <typename FirstMD>
+  __device__ __forceinline__ void buildByMD(unsigned int n, unsigned int nBins, FirstMD firstMD, uint16_t* start,
+                                            uint16_t* count, uint16_t* perm, unsigned int* bins,
+                                            unsigned int* cursor) {
+    for (unsigned int b = laneId(); b < nBins; b += 32)
+      bins[b] = 0;
+    __syncwarp();
+    for (unsigned int k = laneId(); k < n; k += 32)
+      atomicAdd(&bins[firstMD(k)], 1u);
+    __syncwarp();
+    // exclusive scan of the bins
+    unsigned int carry = 0;
+    for (unsigned int b0 = 0; b0 < nBins; b0 += 32) {
+      unsigned int b = b0 + laneId();
+      unsigned int c = b < nBins ? bins[b] : 0u;
+      unsigned int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(kFullMask, incl, o);
+        if (int(laneId()) >= o)
+          incl += y;
+      }
+      if (b < nBins) {
+        cursor[b] = carry + incl - c;
+        start[b] = static_cast<uint16_t>(carry + incl - c);
+        count[b] = static_cast<uint16_t>(c);
+      }
+      carry += __shfl_sync(kFullMask, incl, 31);
+    }
+    __syncwarp();
+    // stable placement, 32 objects at a time
+    for (unsigned int k0 = 0; k0 < n; k0 += 32) {
+      unsigned int k = k0 + laneId();
+      bool valid = k < n;
+      unsigned int b = valid ? firstMD(k) : 0xffffffffu;
+      unsigned int active = __ballot_sync(kFullMask, valid);
+      unsigned int peers = __match_any_sync(kFullMask, b) & active;
+      if (valid) {
+        unsigned int rank = __popc(peers & lanesBelowMask());
+        perm[cursor[b] + rank] = static_cast<uint16_t>(k);
+      }
+      __syncwarp();
+      if (valid && laneId() == 31u - __clz(peers))
+        cursor[b] += __popc(peers);
+      __syncwarp();
+    }
+  }
+
+  // Segments of each lower module grouped by inner MD (after kCreateLS).
+  constexpr int kIdxWarps = 4;
+  __global__ void kLSByMD(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sBins[kIdxWarps][kMaxModuleMDs];
+    __shared__ unsigned int sCursor[kIdxWarps][kMaxModuleMDs];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    for (int w = blockIdx.x * kIdxWarps + wib; w < es.nLowerModules; w += gridDim.x * kIdxWarps) {
+      __syncwarp();
+      const unsigned int n = ev.ls.nSegments[w];
+      if (n == 0)
+        continue;
+      const unsigned int mdBase = es.mdOffset[w];
+      const unsigned int nMD = ev.md.nMDs[w];
+      const unsigned int segBase = es.lsOffset[w];
+      const unsigned int* mdIdx = ev.ls.mdIndices;
+      buildByMD(
+          n, nMD, [&](unsigned int k) { return mdIdx[2 * (segBase + k)] - mdBase; }, ev.mdLSStart + mdBase,
+          ev.mdLSCount + mdBase, ev.lsByMD + segBase, sBins[wib], sCursor[wib]);
+    }
+  }
+
+  // Triplets of each lower module grouped by first MD (after kCreateT3).
+  __global__ void kT3ByMD(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sBins[kIdxWarps][kMaxModuleMDs];
+    __shared__ unsigned int sCursor[kIdxWarps][kMaxModuleMDs];
+    const EventView& ev = evs[blockIdx.y];
+    const int wib = threadIdx.x >> 5;
+    for (int w = blockIdx.x * kIdxWarps + wib; w < es.nLowerModules; w += gridDim.x * kIdxWarps) {
+      __syncwarp();
+      const unsigned int n = ev.t3.nTriplets[w];
+      if (n == 0)
+        continue;
+      const unsigned int mdBase = es.mdOffset[w];
+      const unsigned int nMD = ev.md.nMDs[w];
+      const unsigned int t3Base = ev.rg.tripletModuleIndices[w];
+      const unsigned int* segIdx = ev.t3.segmentIndices;
+      const unsigned int* mdIdx = ev.ls.mdIndices;
+      buildByMD(
+          n, nMD, [&](unsigned int k) { return mdIdx[2 * segIdx[2 * (t3Base + k)]] - mdBase; },
+          ev.mdT3Start + mdBase, ev.mdT3Count + mdBase, ev.t3ByMD + t3Base, sBins[wib], sCursor[wib]);
+    }
+  }
+
   // ============================================================ triplets
   // Per-module triplet offsets (SDL/Triplet.h:1007-1102); one block per event.
   __global__ void __launch_bounds__(1024) kT3Offsets(DeviceES es, const EventView* evs) {
@@ -456,9 +557,15 @@ namespace lst {
       return;
     const unsigned int segBase = es.lsOffset[lm1];
     const Segments& ls = ev.ls;
+    // Only outer segments whose inner MD is the inner segment's outer MD can
+    // pass (the first test of the reference's triplet algorithm); they are
+    // enumerated through the MD-keyed segment index in storage order, so
+    // candidates keep the reference's (inner, outer) order.
     const unsigned int total = warpPrefix(pre, int(nInner), [&](int i) {
       uint16_t middle = ls.outerLowerModuleIndices[segBase + i];
-      return ls.nSegments[middle];
+      if (ls.nSegments[middle] == 0)
+        return 0u;
+      return static_cast<unsigned int>(ev.mdLSCount[ls.mdIndices[2 * (segBase + i) + 1]]);
     });
     const int cap = ev.rg.tripletModuleOccupancy[lm1];
     const unsigned int base = ev.rg.tripletModuleIndices[lm1];
@@ -474,7 +581,9 @@ namespace lst {
         int i = findSlot(pre, int(nInner), f);
         innerSeg = segBase + i;
         middle = ls.outerLowerModuleIndices[innerSeg];
-        outerSeg = es.lsOffset[middle] + (f - pre[i]);
+        const unsigned int mdMid = ls.mdIndices[2 * innerSeg + 1];
+        const unsigned int outerBase = es.lsOffset[middle];
+        outerSeg = outerBase + ev.lsByMD[outerBase + ev.mdLSStart[mdMid] + (f - pre[i])];
         outerOuter = ls.outerLowerModuleIndices[outerSeg];
         ok = t3Select(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg, v);
       }
@@ -556,9 +665,15 @@ namespace lst {
     const unsigned int nInner = ev.t3.nTriplets[lm1];
     const unsigned int t3Base = ev.rg.tripletModuleIndices[lm1];
     const Triplets& t3r = ev.t3;
+    // Only outer triplets whose first MD is the inner triplet's third MD can
+    // pass (the first test of the reference's quintuplet algorithm); they are
+    // enumerated through the MD-keyed triplet index in storage order.
     const unsigned int total = warpPrefix(pre, int(nInner), [&](int i) {
       uint16_t lm3 = t3r.lowerModuleIndices[3 * (t3Base + i) + 2];
-      return t3r.nTriplets[lm3];
+      if (t3r.nTriplets[lm3] == 0)
+        return 0u;
+      const unsigned int seg2 = t3r.segmentIndices[2 * (t3Base + i) + 1];
+      return static_cast<unsigned int>(ev.mdT3Count[ev.ls.mdIndices[2 * seg2 + 1]]);
     });
     const int cap = ev.rg.quintupletModuleOccupancy[lm1];
     const unsigned int base = ev.rg.quintupletModuleIndices[lm1];
@@ -577,7 +692,9 @@ namespace lst {
         innerT3 = t3Base + i;
         lm[1] = t3.lowerModuleIndices[3 * innerT3 + 1];
         lm[2] = t3.lowerModuleIndices[3 * innerT3 + 2];
-        outerT3 = ev.rg.tripletModuleIndices[lm[2]] + (f - pre[i]);
+        const unsigned int mdMid = ev.ls.mdIndices[2 * t3.segmentIndices[2 * innerT3 + 1] + 1];
+        const unsigned int outerBase = ev.rg.tripletModuleIndices[lm[2]];
+        outerT3 = outerBase + ev.t3ByMD[outerBase + ev.mdT3Start[mdMid] + (f - pre[i])];
         lm[3] = t3.lowerModuleIndices[3 * outerT3 + 1];
         lm[4] = t3.lowerModuleIndices[3 * outerT3 + 2];
         ok = t5Select(m, ev.md, ev.ls, t3, dnn.get(), useDnn, lm, innerT3, outerT3, v);
@@ -677,12 +794,118 @@ namespace lst {
   // SDL/Kernels.h:384-473.  Pass 1 sets bit 1 of isDup directly; pass 2 marks
   // plsFlag and kMergePLSFlag folds it into bit 2 afterwards, so that pass 2
   // reads the pass-1 bit while other threads mark removals.
+  // pLS binned by eta: bins of width 0.1 over [-6, 6) (clamped at both ends)
+  // plus a last bin for non-finite eta, which must meet every pLS because a
+  // NaN never satisfies the reference's |deta| > 0.1 skip.
+  constexpr int kPLSBins = 120;
+  LST_DEV int plsEtaBin(float eta) {
+    if (!(fabsf(eta) <= 3.0e38f))
+      return kPLSBins;
+    float t = (eta + 6.0f) * 10.0f;
+    if (t < 0.f)
+      return 0;
+    if (t >= float(kPLSBins))
+      return kPLSBins - 1;
+    return static_cast<int>(t);
+  }
+
+  // Counting sort of the pLS by eta bin; one block per event.
+  __global__ void __launch_bounds__(1024) kPLSBin(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sCount[kPLSBins + 1];
+    __shared__ unsigned int sCursor[kPLSBins + 1];
+    const EventView& ev = evs[blockIdx.y];
+    unsigned int nPix = ev.ls.nSegments[es.pixelModule];
+    if (nPix > kMaxPixelSegments)
+      nPix = kMaxPixelSegments;
+    for (int b = threadIdx.x; b <= kPLSBins; b += blockDim.x)
+      sCount[b] = 0;
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
+      atomicAdd(&sCount[plsEtaBin(ev.ls.eta[i])], 1u);
+    __syncthreads();
+    unsigned int c = threadIdx.x <= kPLSBins ? sCount[threadIdx.x] : 0u;
+    unsigned int tot;
+    unsigned int ex = blockExclusiveScan(c, tot);
+    if (threadIdx.x <= kPLSBins) {
+      sCursor[threadIdx.x] = ex;
+      ev.plsBinStart[threadIdx.x] = ex;
+    }
+    if (threadIdx.x == 0)
+      ev.plsBinStart[kPLSBins + 1] = tot;
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
+      ev.plsOrder[atomicAdd(&sCursor[plsEtaBin(ev.ls.eta[i])], 1u)] = i;
+  }
+
+  // One (ix, jx) pair of the pLS duplicate check (SDL/Kernels.h:384-473).
+  LST_DEV void plsPair(const EventView& ev, unsigned int ix, unsigned int jx, const unsigned int* phits1,
+                       float eta_pix1, float phi_pix1, bool secondpass) {
+    const Segments& s = ev.ls;
+    float eta_pix2 = s.eta[jx];
+    float phi_pix2 = s.phi[jx];
+    if (fabs_(eta_pix2 - eta_pix1) > 0.1f)
+      return;
+    if (secondpass && (!s.isQuad[jx] || (s.isDup[jx] & 1)))
+      return;
+    int8_t quad_diff = s.isQuad[ix] - s.isQuad[jx];
+    float score_diff = s.score[ix] - s.score[jx];
+    unsigned int idxToRemove;
+    if (quad_diff > 0)
+      idxToRemove = jx;
+    else if (quad_diff < 0)
+      idxToRemove = ix;
+    else if (score_diff < 0)
+      idxToRemove = jx;
+    else if (score_diff > 0)
+      idxToRemove = ix;
+    else
+      idxToRemove = ix;
+    int npMatched = 0;
+    for (int i = 0; i < 4; i++) {
+      bool pmatched = false;
+      for (int j = 0; j < 4; j++) {
+        if (phits1[i] == s.pLSHitsIdxs[4 * jx + j]) {
+          pmatched = true;
+          break;
+        }
+      }
+      if (pmatched) {
+        npMatched++;
+        if (secondpass)
+          break;
+      }
+    }
+    bool remove = npMatched >= 3;
+    if (secondpass) {
+      float dEta = fabs_(eta_pix1 - eta_pix2);
+      float dPhi = wrapDPhi(phi_pix1, phi_pix2);
+      float dR2 = dEta * dEta + dPhi * dPhi;
+      if ((npMatched >= 1) || (dR2 < 1e-5f))
+        remove = true;
+    }
+    if (remove) {
+      if (secondpass)
+        ev.plsFlag[idxToRemove] = 1;
+      else
+        s.isDup[idxToRemove] = 1;
+    }
+  }
+
+  // pLS duplicate removal (SDL/Kernels.h:384-473).  Pass 1 sets bit 1 of
+  // isDup directly; pass 2 marks plsFlag and kMergePLSFlag folds it into bit 2
+  // afterwards, so that pass 2 reads the pass-1 bit while other threads mark
+  // removals.  Every pair ix < jx that can pass the |deta| <= 0.1 test is
+  // visited once through the eta bins (neighbouring bins plus the non-finite
+  // bin); the outcome does not depend on the visiting order because marks are
+  // only ever set.
   __global__ void kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
     const EventView& ev = evs[blockIdx.y];
     unsigned int nPix = ev.ls.nSegments[es.pixelModule];
     if (nPix > kMaxPixelSegments)
       nPix = kMaxPixelSegments;
     const Segments& s = ev.ls;
+    const unsigned int* order = ev.plsOrder;
+    const unsigned int* binStart = ev.plsBinStart;
     for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < nPix; ix += gridDim.x * blockDim.x) {
       if (secondpass && (!s.isQuad[ix] || (s.isDup[ix] & 1)))
         continue;
@@ -690,55 +913,23 @@ namespace lst {
                                 s.pLSHitsIdxs[4 * ix + 3]};
       float eta_pix1 = s.eta[ix];
       float phi_pix1 = s.phi[ix];
-      for (unsigned int jx = ix + 1; jx < nPix; jx++) {
-        float eta_pix2 = s.eta[jx];
-        float phi_pix2 = s.phi[jx];
-        if (fabs_(eta_pix2 - eta_pix1) > 0.1f)
-          continue;
-        if (secondpass && (!s.isQuad[jx] || (s.isDup[jx] & 1)))
-          continue;
-        int8_t quad_diff = s.isQuad[ix] - s.isQuad[jx];
-        float score_diff = s.score[ix] - s.score[jx];
-        unsigned int idxToRemove;
-        if (quad_diff > 0)
-          idxToRemove = jx;
-        else if (quad_diff < 0)
-          idxToRemove = ix;
-        else if (score_diff < 0)
-          idxToRemove = jx;
-        else if (score_diff > 0)
-          idxToRemove = ix;
-        else
-          idxToRemove = ix;
-        int npMatched = 0;
-        for (int i = 0; i < 4; i++) {
-          bool pmatched = false;
-          for (int j = 0; j < 4; j++) {
-            if (phits1[i] == s.pLSHitsIdxs[4 * jx + j]) {
-              pmatched = true;
-              break;
-            }
-          }
-          if (pmatched) {
-            npMatched++;
-            if (secondpass)
-              break;
-          }
-        }
-        bool remove = npMatched >= 3;
-        if (secondpass) {
-          float dEta = fabs_(eta_pix1 - eta_pix2);
-          float dPhi = wrapDPhi(phi_pix1, phi_pix2);
-          float dR2 = dEta * dEta + dPhi * dPhi;
-          if ((npMatched >= 1) || (dR2 < 1e-5f))
-            remove = true;
-        }
-        if (remove) {
-          if (secondpass)
-            ev.plsFlag[idxToRemove] = 1;
-          else
-            s.isDup[idxToRemove] = 1;
-        }
+      const int b = plsEtaBin(eta_pix1);
+      if (b == kPLSBins) {
+        for (unsigned int jx = ix + 1; jx < nPix; jx++)
+          plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
+        continue;
+      }
+      const int b0 = b >= 2 ? b - 2 : 0;
+      const int b1 = b + 2 < kPLSBins ? b + 2 : kPLSBins - 1;
+      for (unsigned int k = binStart[b0]; k < binStart[b1 + 1]; ++k) {
+        unsigned int jx = order[k];
+        if (jx > ix)
+          plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
+      }
+      for (unsigned int k = binStart[kPLSBins]; k < binStart[kPLSBins + 1]; ++k) {
+        unsigned int jx = order[k];
+        if (jx > ix)
+          plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
       }
     }
   }
@@ -892,42 +1083,65 @@ namespace lst {
     }
   }
 
-  // Number of hits two pT5s share (SDL/Kernels.h:86-136).
-  LST_DEV int sharedHitsPT5(const PixelQuintuplets& p, unsigned int ix, unsigned int jx) {
-    int nMatched = 0;
-    for (int i = 0; i < 14; i++) {
-      unsigned int a = p.hitIndices[14 * ix + i];
-      bool matched = false;
-      for (int j = 0; j < 14; j++)
-        if (a == p.hitIndices[14 * jx + j]) {
-          matched = true;
-          break;
-        }
-      if (matched)
-        nMatched++;
-    }
-    return nMatched;
-  }
-
-  // SDL/Kernels.h:358-382
-  __global__ void kPT5Dedup(DeviceES es, const EventView* evs) {
+  // pT5 duplicate removal (SDL/Kernels.h:358-382): a pT5 is dropped if
+  // another shares >= 7 of its 14 hits and has a lower score (ties: the
+  // higher index is dropped).  The other candidates' hits are staged in
+  // shared memory 128 at a time; the outcome per pT5 is an "any" over the
+  // others, so the visiting order does not matter.
+  constexpr int kDedupTile = 128;
+  __global__ void __launch_bounds__(kDedupTile) kPT5Dedup(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sHits[kDedupTile * 14];
+    __shared__ float sScore[kDedupTile];
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt5.nPixelQuintuplets;
     PixelQuintuplets p = ev.pt5;
-    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < n; ix += gridDim.x * blockDim.x) {
-      float score1 = p.score[ix];
-      for (unsigned int jx = 0; jx < n; jx++) {
-        if (ix == jx)
+    for (unsigned int ixBase = blockIdx.x * kDedupTile; ixBase < n; ixBase += gridDim.x * kDedupTile) {
+      const unsigned int ix = ixBase + threadIdx.x;
+      const bool valid = ix < n;
+      unsigned int mine[14];
+      float score1 = 0.f;
+      if (valid) {
+#pragma unroll
+        for (int i = 0; i < 14; ++i)
+          mine[i] = p.hitIndices[14 * ix + i];
+        score1 = p.score[ix];
+      }
+      bool dup = false;
+      for (unsigned int jBase = 0; jBase < n; jBase += kDedupTile) {
+        const unsigned int tile = (n - jBase < kDedupTile) ? n - jBase : kDedupTile;
+        __syncthreads();
+        for (unsigned int t = threadIdx.x; t < tile * 14; t += blockDim.x)
+          sHits[t] = p.hitIndices[14 * jBase + t];
+        for (unsigned int t = threadIdx.x; t < tile; t += blockDim.x)
+          sScore[t] = p.score[jBase + t];
+        __syncthreads();
+        if (!valid || dup)
           continue;
-        int nMatched = sharedHitsPT5(p, ix, jx);
-        float score2 = p.score[jx];
-        if (nMatched >= 7) {
-          if (score1 > score2 or ((score1 == score2) and (ix > jx))) {
-            p.isDup[ix] = 1;
-            break;
+        for (unsigned int jj = 0; jj < tile; ++jj) {
+          const unsigned int jx = jBase + jj;
+          if (jx == ix)
+            continue;
+          const unsigned int* other = sHits + 14 * jj;
+          int nMatched = 0;
+#pragma unroll
+          for (int i = 0; i < 14; ++i) {
+            bool matched = false;
+#pragma unroll
+            for (int j = 0; j < 14; ++j)
+              matched |= (mine[i] == other[j]);
+            nMatched += matched ? 1 : 0;
+          }
+          const float score2 = sScore[jj];
+          if (nMatched >= 7) {
+            if (score1 > score2 or ((score1 == score2) and (ix > jx))) {
+              dup = true;
+              break;
+            }
           }
         }
       }
+      if (valid && dup)
+        p.isDup[ix] = 1;
     }
   }
 

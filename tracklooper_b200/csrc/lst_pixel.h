@@ -33,7 +33,9 @@ namespace lst {
     float x_InLo = md.anchorX[md1], x_InUp = md.anchorX[md2], x_OutLo = md.anchorX[md3], x_OutUp = md.anchorX[md4];
     float y_InLo = md.anchorY[md1], y_InUp = md.anchorY[md2], y_OutLo = md.anchorY[md3], y_OutUp = md.anchorY[md4];
     float rt_InOut = rt_InUp;
-    if (!(fabs_(deltaPhi(x_InUp, y_InUp, x_OutLo, y_OutLo)) <= 0.5f * float(M_PI)))
+    // deltaPhi of two anchor hits, from their stored phi (hits.phis is phi()
+    // of the same coordinates, so the value is identical)
+    if (!(fabs_(phiMpiPi(md.anchorPhi[md3] - md.anchorPhi[md2])) <= 0.5f * float(M_PI)))
       return false;
 
     unsigned int pls = innerSeg - rg.segmentModuleIndices[pixelModule];
@@ -91,13 +93,14 @@ namespace lst {
     float alpha_InLo = s.dPhiChanges[innerSeg];
     float alpha_OutLo = s.dPhiChanges[outerSeg];
     bool isEC_lastLayer = m.subdets[lmOO] == Endcap and m.moduleType[lmOO] == TwoS;
-    float alpha_OutUp = deltaPhi(x_OutUp, y_OutUp, x_OutUp - x_OutLo, y_OutUp - y_OutLo);
+    float alpha_OutUp = phiMpiPi(phiOf(x_OutUp - x_OutLo, y_OutUp - y_OutLo) - md.anchorPhi[md4]);
     float tl_axis_x = x_OutUp - x_InUp;
     float tl_axis_y = y_OutUp - y_InUp;
-    float betaIn = -deltaPhi(px, py, tl_axis_x, tl_axis_y);
+    const float phiTlAxis = phiOf(tl_axis_x, tl_axis_y);
+    float betaIn = -phiMpiPi(phiTlAxis - phiOf(px, py));
     float betaInRHmin = betaIn;
     float betaInRHmax = betaIn;
-    float betaOut = -alpha_OutUp + deltaPhi(x_OutUp, y_OutUp, tl_axis_x, tl_axis_y);
+    float betaOut = -alpha_OutUp + phiMpiPi(phiTlAxis - md.anchorPhi[md4]);
     float betaOutRHmin = betaOut;
     float betaOutRHmax = betaOut;
     if (isEC_lastLayer) {
@@ -237,13 +240,14 @@ namespace lst {
     float alpha_InLo = s.dPhiChanges[innerSeg];
     float alpha_OutLo = s.dPhiChanges[outerSeg];
     bool isEC_lastLayer = m.subdets[lmOO] == Endcap and m.moduleType[lmOO] == TwoS;
-    float alpha_OutUp = deltaPhi(x_OutUp, y_OutUp, x_OutUp - x_OutLo, y_OutUp - y_OutLo);
+    float alpha_OutUp = phiMpiPi(phiOf(x_OutUp - x_OutLo, y_OutUp - y_OutLo) - md.anchorPhi[md4]);
     float tl_axis_x = x_OutUp - x_InUp;
     float tl_axis_y = y_OutUp - y_InUp;
-    float betaIn = -deltaPhi(px, py, tl_axis_x, tl_axis_y);
+    const float phiTlAxis = phiOf(tl_axis_x, tl_axis_y);
+    float betaIn = -phiMpiPi(phiTlAxis - phiOf(px, py));
     float betaInRHmin = betaIn;
     float betaInRHmax = betaIn;
-    float betaOut = -alpha_OutUp + deltaPhi(x_OutUp, y_OutUp, tl_axis_x, tl_axis_y);
+    float betaOut = -alpha_OutUp + phiMpiPi(phiTlAxis - md.anchorPhi[md4]);
     float betaOutRHmin = betaOut;
     float betaOutRHmax = betaOut;
     if (isEC_lastLayer) {
@@ -539,32 +543,34 @@ namespace lst {
     uint16_t pixelModule = s.innerLowerModuleIndices[plsIndex];
     uint16_t lmL = t.lowerModuleIndices[3 * t3], lmM = t.lowerModuleIndices[3 * t3 + 1],
              lmU = t.lowerModuleIndices[3 * t3 + 2];
+    unsigned int pls = plsIndex - rg.segmentModuleIndices[pixelModule];
+    float pixelSegmentPt = s.ptIn[pls];
+    float pixelSegmentPtError = s.ptErr[pls];
+    v.pixelRadius = pixelSegmentPt * kR1GeVf;
+    v.pixelRadiusError = pixelSegmentPtError * kR1GeVf;
+    v.tripletRadius = t.circleRadius[t3];
+    // The radius criterion is the reference's third test; every test here is
+    // a pure function of the pair, so testing this cheap one first changes no
+    // outcome and skips the two tracklet algorithms for most pairs.
+    int kind = (m.subdets[lmL] == Endcap) ? 3 : (m.subdets[lmM] == Endcap) ? 2 : (m.subdets[lmU] == Endcap) ? 1 : 0;
+    if (!pt3RadiusCriterion(kind, v.pixelRadius, v.pixelRadiusError, v.tripletRadius))
+      return false;
     if (!ptPixelTracklet(m, rg, md, s, pixelModule, lmL, lmM, plsIndex, t.segmentIndices[2 * t3]))
       return false;
     if (!ptPixelTracklet(m, rg, md, s, pixelModule, lmM, lmU, plsIndex, t.segmentIndices[2 * t3 + 1]))
       return false;
 
-    unsigned int pls = plsIndex - rg.segmentModuleIndices[pixelModule];
-    float pixelSegmentPt = s.ptIn[pls];
-    float pixelSegmentPtError = s.ptErr[pls];
     float pixelG = s.circleCenterX[pls];
     float pixelF = s.circleCenterY[pls];
     float pixelRadiusPCA = s.circleRadius[pls];
     unsigned int pixelInnerMD = s.mdIndices[2 * plsIndex];
     unsigned int pixelOuterMD = s.mdIndices[2 * plsIndex + 1];
-    v.pixelRadius = pixelSegmentPt * kR1GeVf;
-    v.pixelRadiusError = pixelSegmentPtError * kR1GeVf;
     unsigned int innerSeg = t.segmentIndices[2 * t3], outerSeg = t.segmentIndices[2 * t3 + 1];
     unsigned int md1 = s.mdIndices[2 * innerSeg], md2 = s.mdIndices[2 * innerSeg + 1], md3 = s.mdIndices[2 * outerSeg + 1];
     float xs[3] = {md.anchorX[md1], md.anchorX[md2], md.anchorX[md3]};
     float ys[3] = {md.anchorY[md1], md.anchorY[md2], md.anchorY[md3]};
-    v.tripletRadius = t.circleRadius[t3];
     float g = t.circleCenterX[t3];
     float f = t.circleCenterY[t3];
-
-    int kind = (m.subdets[lmL] == Endcap) ? 3 : (m.subdets[lmM] == Endcap) ? 2 : (m.subdets[lmU] == Endcap) ? 1 : 0;
-    if (!pt3RadiusCriterion(kind, v.pixelRadius, v.pixelRadiusError, v.tripletRadius))
-      return false;
 
     uint16_t lm3[3] = {lmL, lmM, lmU};
     if (runChiSquaredCuts and pixelSegmentPt < 5.0f) {

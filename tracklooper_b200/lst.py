@@ -307,9 +307,20 @@ class ES:
         _check(library().lst_es_set_t5dnn_weights(self._h, w.ctypes.data, w.size), "lst_es_set_t5dnn_weights")
 
     def close(self):
-        if self._h:
+        """Frees the event setup; event sets still using it keep it alive
+        until they are closed."""
+        self._closing = True
+        if self._h and not getattr(self, "_users", 0):
             library().lst_es_free(self._h)
             self._h = None
+
+    def _retain(self):
+        self._users = getattr(self, "_users", 0) + 1
+
+    def _release(self):
+        self._users -= 1
+        if self._users == 0 and getattr(self, "_closing", False):
+            self.close()
 
     def __del__(self):
         try:
@@ -365,6 +376,7 @@ class EventSet:
         _check(lib.lst_event_create(es.handle, n_slots, max_hits, stream, ctypes.byref(h)), "lst_event_create")
         self._h = h
         self.es = es
+        es._retain()
         self.n_slots = n_slots
         self.max_hits = max_hits
 
@@ -376,6 +388,7 @@ class EventSet:
         if self._h:
             library().lst_event_destroy(self._h)
             self._h = None
+            self.es._release()
 
     def __del__(self):
         try:
