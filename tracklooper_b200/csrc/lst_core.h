@@ -20,9 +20,13 @@
 #if defined(__CUDACC__)
 #define LST_HD __host__ __device__ __forceinline__
 #define LST_DEV __device__ __forceinline__
+// Large cut algorithms stay out of line on the device: inlined at every call
+// site they overflow the instruction cache of the warps that diverge into them.
+#define LST_HD_BIG __host__ __device__ __noinline__
 #else
 #define LST_HD inline
 #define LST_DEV inline
+#define LST_HD_BIG inline
 #endif
 
 namespace lst {

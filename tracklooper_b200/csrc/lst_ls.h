@@ -76,7 +76,7 @@ namespace lst {
 
   // Barrel-barrel segment (SDL/Segment.h:455-565).  dPhiMin/Max and
   // dPhiChangeMin/Max keep their initial value 0.
-  LST_HD bool lsBarrel(const Modules& m,
+  LST_HD_BIG bool lsBarrel(const Modules& m,
                        const MiniDoublets& md,
                        uint16_t innerLM,
                        uint16_t outerLM,
@@ -121,7 +121,7 @@ namespace lst {
   }
 
   // Segment with at least one endcap module (SDL/Segment.h:567-705).
-  LST_HD bool lsEndcap(const Modules& m,
+  LST_HD_BIG bool lsEndcap(const Modules& m,
                        const MiniDoublets& md,
                        uint16_t innerLM,
                        uint16_t outerLM,

@@ -185,7 +185,7 @@ namespace lst {
   };
 
   // Barrel mini-doublet (SDL/MiniDoublet.h:645-777).
-  LST_HD bool mdBarrel(const Modules& m,
+  LST_HD_BIG bool mdBarrel(const Modules& m,
                        uint16_t lm,
                        float xLower,
                        float yLower,
@@ -252,7 +252,7 @@ namespace lst {
 
   // Endcap mini-doublet (SDL/MiniDoublet.h:779-892).  The stored "dz" of an
   // endcap mini-doublet is the transverse-radius difference.
-  LST_HD bool mdEndcap(const Modules& m,
+  LST_HD_BIG bool mdEndcap(const Modules& m,
                        uint16_t lm,
                        float xLower,
                        float yLower,

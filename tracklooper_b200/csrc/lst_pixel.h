@@ -14,7 +14,7 @@ namespace lst {
 
   // Pixel segment against a pair of outer-tracker mini-doublets, barrel outer
   // modules (SDL/PixelTriplet.h:1264-1553).
-  LST_HD bool ptPPBB(const Modules& m,
+  LST_HD_BIG bool ptPPBB(const Modules& m,
                      const Ranges& rg,
                      const MiniDoublets& md,
                      const Segments& s,
@@ -160,7 +160,7 @@ namespace lst {
   }
 
   // Pixel segment against an endcap pair (SDL/PixelTriplet.h:1555-1862).
-  LST_HD bool ptPPEE(const Modules& m,
+  LST_HD_BIG bool ptPPEE(const Modules& m,
                      const Ranges& rg,
                      const MiniDoublets& md,
                      const Segments& s,
@@ -447,7 +447,7 @@ namespace lst {
 
   // Helix r-z residuals of the triplet hits from the pixel state
   // (SDL/PixelTriplet.h:736-823).
-  LST_HD float pt3RZChi2(const Modules& m,
+  LST_HD_BIG float pt3RZChi2(const Modules& m,
                          const uint16_t* lm,
                          const float* rtPix,
                          const float* xPix,
@@ -836,7 +836,7 @@ namespace lst {
   }
 
   // Straight-line r-z residuals from the two pixel anchors (SDL/PixelTriplet.h:2636-2677).
-  LST_HD float pt5RZChi2(const Modules& m, const uint16_t* lm, const float* rtPix, const float* zPix, const float* rts,
+  LST_HD_BIG float pt5RZChi2(const Modules& m, const uint16_t* lm, const float* rtPix, const float* zPix, const float* rts,
                          const float* zs) {
     float slope = (zPix[1] - zPix[0]) / (rtPix[1] - rtPix[0]);
     float residual = 0;

@@ -58,7 +58,7 @@ namespace lst {
   }
 
   // Barrel-barrel-barrel pointing and first beta cut (SDL/Triplet.h:301-402).
-  LST_HD bool t3PointingBBB(const Modules& m,
+  LST_HD_BIG bool t3PointingBBB(const Modules& m,
                             const MiniDoublets& md,
                             const Segments& s,
                             uint16_t lm1,
@@ -112,7 +112,7 @@ namespace lst {
   }
 
   // Barrel-barrel-endcap / barrel-endcap-endcap (SDL/Triplet.h:404-531).
-  LST_HD bool t3PointingBBE(const Modules& m,
+  LST_HD_BIG bool t3PointingBBE(const Modules& m,
                             const MiniDoublets& md,
                             const Segments& s,
                             uint16_t lm1,
@@ -186,7 +186,7 @@ namespace lst {
   }
 
   // Endcap-endcap-endcap (SDL/Triplet.h:533-658).
-  LST_HD bool t3PointingEEE(const Modules& m,
+  LST_HD_BIG bool t3PointingEEE(const Modules& m,
                             const MiniDoublets& md,
                             const Segments& s,
                             uint16_t lm1,

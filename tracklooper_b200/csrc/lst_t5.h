@@ -84,7 +84,7 @@ namespace lst {
   };
 
   // Barrel-barrel-barrel-(barrel|endcap) (SDL/Quintuplet.h:1467-1746).
-  LST_HD bool t4BBBB(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
+  LST_HD_BIG bool t4BBBB(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
     bool isPS_InLo = (m.moduleType[q.lmII] == PS);
     bool isPS_OutLo = (m.moduleType[q.lmOI] == PS);
     float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
@@ -217,7 +217,7 @@ namespace lst {
 
   // Barrel-barrel-endcap-endcap and barrel-endcap-endcap-endcap
   // (SDL/Quintuplet.h:1748-2029).
-  LST_HD bool t4BBEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
+  LST_HD_BIG bool t4BBEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
     bool isPS_InLo = (m.moduleType[q.lmII] == PS);
     bool isPS_OutLo = (m.moduleType[q.lmOI] == PS);
     float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
@@ -363,7 +363,7 @@ namespace lst {
   }
 
   // Endcap-endcap-endcap-endcap (SDL/Quintuplet.h:2031-2297).
-  LST_HD bool t4EEEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
+  LST_HD_BIG bool t4EEEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
     float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
     float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
     float alpha1GeV_OutLo = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
@@ -590,7 +590,7 @@ namespace lst {
   // --------------------------------------------------------- r-z chi-square
   // Helix r-z residuals of the outer hits (SDL/Quintuplet.h:302-736); sets
   // tightCutFlag for the T5-in-TC selection.
-  LST_HD bool t5PassRZ(const Modules& m,
+  LST_HD_BIG bool t5PassRZ(const Modules& m,
                        const MiniDoublets& md,
                        const unsigned int* mdIdx,
                        const uint16_t* lm,
@@ -991,7 +991,7 @@ namespace lst {
 
   // --------------------------------------------------- circle regression
   // Per-hit resolution model (SDL/Quintuplet.h:1136-1221).
-  LST_HD void regressionSigmas(const Modules& m,
+  LST_HD_BIG void regressionSigmas(const Modules& m,
                                const uint16_t* lm,
                                float* delta1,
                                float* delta2,
@@ -1063,7 +1063,7 @@ namespace lst {
   }
 
   // Weighted circle regression (SDL/Quintuplet.h:1223-1321).
-  LST_HD float circleRegression(int nPoints,
+  LST_HD_BIG float circleRegression(int nPoints,
                                 const float* xs,
                                 const float* ys,
                                 const float* delta1,
@@ -1114,7 +1114,7 @@ namespace lst {
 
   // Chi-squared of points against a given circle (SDL/Quintuplet.h:1323-1368,
   // identical to SDL/PixelTriplet.h:370-417 and :2219-2264).
-  LST_HD float circleChi2(int nPoints,
+  LST_HD_BIG float circleChi2(int nPoints,
                           const float* xs,
                           const float* ys,
                           const float* delta1,
@@ -1137,7 +1137,7 @@ namespace lst {
 
   // ------------------------------------------------------------- T5 DNN
   // Raw (unstandardised) input features (SDL/NeuralNetwork.h:63-114).
-  LST_HD void t5DnnFeatures(const Modules& m,
+  LST_HD_BIG void t5DnnFeatures(const Modules& m,
                             const MiniDoublets& md,
                             const Segments& s,
                             const Triplets& t,
@@ -1185,6 +1185,7 @@ namespace lst {
   template <typename W>
   LST_HD float t5DnnForward(const W& w, const float* x) {
     float h1[32];
+#pragma unroll 1
     for (int col = 0; col < 32; ++col) {
       float acc = 0;
       for (int in = 0; in < 38; ++in)
@@ -1193,6 +1194,7 @@ namespace lst {
       h1[col] = (acc > 0.f) ? acc : 0.f;
     }
     float h2[32];
+#pragma unroll 1
     for (int col = 0; col < 32; ++col) {
       float acc = 0;
       for (int in = 0; in < 32; ++in)
