@@ -51,7 +51,10 @@ namespace lst {
     unsigned int nPT5Total;
     unsigned int nPT3Total;
     unsigned int nOutHits;  // output hit-list length of the event's track candidates
-    unsigned int pad[2];
+    unsigned int t5CandTotal;     // quintuplet candidates of the event
+    unsigned int t5CandOverflow;  // more candidates than the flag buffer holds
+    unsigned int t5PassCount;     // passing candidates found by kT5Eval
+    unsigned int pad[3];
   };
 
   // All device pointers of one event.
@@ -92,6 +95,11 @@ namespace lst {
     uint16_t* t3ByMD;
     uint16_t* mdT3Start;
     uint16_t* mdT3Count;
+    unsigned int* t5CandPre;    // per inner triplet: its first candidate within the module
+    unsigned int* t5ModCand;    // per eligible module: candidates
+    unsigned int* t5ModOff;     // per eligible module: first candidate of the event
+    unsigned int* t5CandFlag;   // per candidate: 0 = fails, else 1 + slot of its values in t5PassValues
+    T5Values* t5PassValues;     // selection values of passing candidates
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
     unsigned int maxHits;

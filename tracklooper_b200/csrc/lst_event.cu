@@ -390,7 +390,12 @@ namespace {
           return setError("the DNN T5 method needs weights (lst_es_load or lst_es_set_t5dnn_weights)");
         bool useDnn = ev->t5Method == LST_T5_DNN;
         LST_LAUNCH(lst::kT5Eligible, one, 1024, d, v);
-        LST_LAUNCH(lst::kCreateT5, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v, useDnn);
+        LST_LAUNCH(lst::kT5Prefix, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v);
+        LST_LAUNCH(lst::kT5ModScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kT5Eval, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v, useDnn);
+        LST_LAUNCH(lst::kT5Walk, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v,
+                   useDnn);
+        LST_LAUNCH(lst::kT5Emit, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v, useDnn);
         LST_LAUNCH(lst::kT5DedupAfterBuild, dim3(ceilDiv(nLower * 32, 256), count), 256, d, v);
         LST_LAUNCH(lst::kT5Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;
@@ -499,7 +504,11 @@ namespace {
         {"kT3ByMD", (const void*)lst::kT3ByMD},
         {"kT3Ranges", (const void*)lst::kT3Ranges},
         {"kT5Eligible", (const void*)lst::kT5Eligible},
-        {"kCreateT5", (const void*)lst::kCreateT5},
+        {"kT5Prefix", (const void*)lst::kT5Prefix},
+        {"kT5ModScan", (const void*)lst::kT5ModScan},
+        {"kT5Eval", (const void*)lst::kT5Eval},
+        {"kT5Emit", (const void*)lst::kT5Emit},
+        {"kT5Walk", (const void*)lst::kT5Walk},
         {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
         {"kT5Ranges", (const void*)lst::kT5Ranges},
         {"kPLSBin", (const void*)lst::kPLSBin},

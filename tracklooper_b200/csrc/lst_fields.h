@@ -231,5 +231,10 @@
   X(t3ByMD, uint16_t, T3)                             \
   X(mdT3Start, uint16_t, MD)                          \
   X(mdT3Count, uint16_t, MD)                          \
+  X(t5CandPre, unsigned int, T3)                      \
+  X(t5ModCand, unsigned int, L)                       \
+  X(t5ModOff, unsigned int, L + 1)                    \
+  X(t5CandFlag, unsigned int, lst::kT5CandCap)        \
+  X(t5PassValues, lst::T5Values, lst::kT5PassCap)     \
   X(plsOrder, unsigned int, P)                        \
   X(plsBinStart, unsigned int, 128)

@@ -713,14 +713,203 @@ namespace lst {
     }
   }
 
-  __global__ void kCreateT5(DeviceES es, const EventView* evs, bool useDnn) {
+  // ------------------------------------------ T5 as a candidate work list
+  // The warp-per-module walk above leaves most lanes idle: a few modules own
+  // most candidates and the candidates diverge early.  The batched path
+  // instead (1) stores each module's candidate prefix over its inner
+  // triplets, (2) scans module totals, (3) evaluates every candidate on its
+  // own thread, and (4) walks each module's pass flags in candidate order,
+  // re-evaluating only the passing candidates to store them at their rank.
+  // Candidate c of module w is the c-th (inner, outer) pair of the walk, so
+  // ranks, caps and stored values are those of the walk.  Events with more
+  // candidates than the flag buffer holds take the walk instead.
+  constexpr unsigned int kT5CandCap = 1u << 21;  // candidates per event
+  constexpr unsigned int kT5PassCap = 1u << 16;  // passing candidates per event whose values are kept
+
+  __device__ __forceinline__ unsigned int t5CandidatesOf(const EventView& ev, unsigned int innerT3) {
+    const Triplets& t3 = ev.t3;
+    uint16_t lm3 = t3.lowerModuleIndices[3 * innerT3 + 2];
+    if (t3.nTriplets[lm3] == 0)
+      return 0u;
+    const unsigned int seg2 = t3.segmentIndices[2 * innerT3 + 1];
+    return static_cast<unsigned int>(ev.mdT3Count[ev.ls.mdIndices[2 * seg2 + 1]]);
+  }
+
+  // (inner, outer) triplets of candidate f of module lm1.
+  __device__ __forceinline__ void t5Candidate(const EventView& ev, unsigned int t3Base, unsigned int nInner, unsigned int f,
+                                              unsigned int& innerT3, unsigned int& outerT3) {
+    const unsigned int* pre = ev.t5CandPre + t3Base;
+    int lo = 0, hi = int(nInner);
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (pre[mid] <= f)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    innerT3 = t3Base + lo;
+    const Triplets& t3 = ev.t3;
+    const unsigned int mdMid = ev.ls.mdIndices[2 * t3.segmentIndices[2 * innerT3 + 1] + 1];
+    const unsigned int outerBase = ev.rg.tripletModuleIndices[t3.lowerModuleIndices[3 * innerT3 + 2]];
+    outerT3 = outerBase + ev.t3ByMD[outerBase + ev.mdT3Start[mdMid] + (f - pre[lo])];
+  }
+
+  __global__ void kT5Prefix(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const int wpb = blockDim.x >> 5;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nE; w += gridDim.x * wpb) {
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[w];
+      const int layer = es.m.layers[lm1];
+      unsigned int carry = 0;
+      if (layer == 1 || layer == 2) {
+        const unsigned int nInner = ev.t3.nTriplets[lm1];
+        const unsigned int t3Base = ev.rg.tripletModuleIndices[lm1];
+        for (unsigned int b = 0; b < nInner; b += 32) {
+          unsigned int i = b + laneId();
+          unsigned int c = i < nInner ? t5CandidatesOf(ev, t3Base + i) : 0u;
+          unsigned int incl = c;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            unsigned int y = __shfl_up_sync(kFullMask, incl, o);
+            if (int(laneId()) >= o)
+              incl += y;
+          }
+          if (i < nInner)
+            ev.t5CandPre[t3Base + i] = carry + incl - c;
+          carry += __shfl_sync(kFullMask, incl, 31);
+        }
+      }
+      if (laneId() == 0)
+        ev.t5ModCand[w] = carry;
+    }
+  }
+
+  __global__ void __launch_bounds__(1024) kT5ModScan(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nE = *ev.rg.nEligibleT5Modules;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < nE; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int c = i < nE ? ev.t5ModCand[i] : 0u;
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(c, tot);
+      if (i < nE)
+        ev.t5ModOff[i] = carry + ex;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      ev.t5ModOff[nE] = carry;
+      ev.sc->t5CandTotal = carry;
+      ev.sc->t5CandOverflow = carry > kT5CandCap ? 1u : 0u;
+      ev.sc->t5PassCount = 0;
+    }
+  }
+
+  __global__ void kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
+    const EventView& ev = evs[blockIdx.y];
+    if (ev.sc->t5CandOverflow)
+      return;
+    const unsigned int total = ev.sc->t5CandTotal;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    const unsigned int* off = ev.t5ModOff;
+    ConstDnn dnn;
+    for (unsigned int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+      int lo = 0, hi = nE;  // largest w with off[w] <= c
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= c)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
+      unsigned int innerT3, outerT3;
+      t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
+      uint16_t lm[5] = {lm1,
+                        ev.t3.lowerModuleIndices[3 * innerT3 + 1],
+                        ev.t3.lowerModuleIndices[3 * innerT3 + 2],
+                        ev.t3.lowerModuleIndices[3 * outerT3 + 1],
+                        ev.t3.lowerModuleIndices[3 * outerT3 + 2]};
+      T5Values v;
+      unsigned int flag = 0;
+      if (t5Select(es.m, ev.md, ev.ls, ev.t3, dnn.get(), useDnn, lm, innerT3, outerT3, v)) {
+        // keep the values of a passing candidate (flag = slot + 1), or mark
+        // it for re-evaluation (flag = kT5PassCap + 1) when the buffer is full
+        const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
+        if (slot < kT5PassCap) {
+          ev.t5PassValues[slot] = v;
+          flag = slot + 1;
+        } else {
+          flag = kT5PassCap + 1;
+        }
+      }
+      ev.t5CandFlag[c] = flag;
+    }
+  }
+
+  // The warp-per-module walk, for events whose candidates overflow the flag
+  // buffer (a no-op for the others).
+  __global__ void kT5Walk(DeviceES es, const EventView* evs, bool useDnn) {
     __shared__ unsigned int sPre[kT5Warps][kT5MaxInner + 1];
     const EventView& ev = evs[blockIdx.y];
+    if (!ev.sc->t5CandOverflow)
+      return;
     const int wib = threadIdx.x >> 5;
     const int nE = *ev.rg.nEligibleT5Modules;
     for (int w = blockIdx.x * kT5Warps + wib; w < nE; w += gridDim.x * kT5Warps) {
       __syncwarp();
       t5Module(es, ev, ev.rg.indicesOfEligibleT5Modules[w], sPre[wib], useDnn);
+    }
+  }
+
+  __global__ void kT5Emit(DeviceES es, const EventView* evs, bool useDnn) {
+    const EventView& ev = evs[blockIdx.y];
+    if (ev.sc->t5CandOverflow)
+      return;
+    const int wpb = blockDim.x >> 5;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    ConstDnn dnn;
+    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < nE; w += gridDim.x * wpb) {
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[w];
+      const int layer = es.m.layers[lm1];
+      if (layer != 1 && layer != 2)
+        continue;
+      const unsigned int total = ev.t5ModCand[w];
+      const unsigned int off = ev.t5ModOff[w];
+      const unsigned int t3Base = ev.rg.tripletModuleIndices[lm1];
+      const unsigned int nInner = ev.t3.nTriplets[lm1];
+      const int cap = ev.rg.quintupletModuleOccupancy[lm1];
+      const unsigned int base = ev.rg.quintupletModuleIndices[lm1];
+      Triplets t3 = ev.t3;
+      Quintuplets t5 = ev.t5;
+      unsigned int count = 0;
+      for (unsigned int start = 0; start < total; start += 32) {
+        const unsigned int f = start + laneId();
+        const unsigned int flag = f < total ? ev.t5CandFlag[off + f] : 0u;
+        const bool ok = flag != 0;
+        unsigned int tot;
+        const unsigned int r = count + warpRank(ok, tot);
+        if (ok && int(r) < cap) {
+          unsigned int innerT3, outerT3;
+          t5Candidate(ev, t3Base, nInner, f, innerT3, outerT3);
+          uint16_t lm[5] = {lm1, t3.lowerModuleIndices[3 * innerT3 + 1], t3.lowerModuleIndices[3 * innerT3 + 2],
+                            t3.lowerModuleIndices[3 * outerT3 + 1], t3.lowerModuleIndices[3 * outerT3 + 2]};
+          T5Values v;
+          if (flag <= kT5PassCap)
+            v = ev.t5PassValues[flag - 1];
+          else
+            t5Select(es.m, ev.md, ev.ls, t3, dnn.get(), useDnn, lm, innerT3, outerT3, v);
+          storeT5(ev.md, ev.ls, t3, t5, innerT3, outerT3, lm, layer, v, base + r);
+        }
+        count += tot;
+      }
+      if (laneId() == 0) {
+        t5.nQuintuplets[lm1] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
+        t5.totOccupancyQuintuplets[lm1] = count;
+        if (int(count) > cap)
+          atomicOr(&ev.sc->status, kStatusCapOverflow);
+      }
     }
   }
 

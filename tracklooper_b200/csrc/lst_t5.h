@@ -509,14 +509,18 @@ namespace lst {
   // ------------------------------------------------------- radius checks
   // Spread of the circle radius when 2S endcap hits move along their strips
   // (SDL/Quintuplet.h:753-783).
-  LST_HD void radiusSpread(const float* x1, const float* y1, const float* x2, const float* y2, const float* x3,
-                           const float* y3, float& minimumRadius, float& maximumRadius) {
+  // Min and max circle radius over the 3 x 3 x 3 choices of the three points'
+  // positions (SDL/Quintuplet.h:753-783).  n1..n3 = 1 for a point whose three
+  // candidate positions coincide: repeated candidates leave fmin / fmax
+  // unchanged, so the result equals the full 27-fit loop.
+  LST_HD void radiusSpread(const float* x1, const float* y1, int n1, const float* x2, const float* y2, int n2,
+                           const float* x3, const float* y3, int n3, float& minimumRadius, float& maximumRadius) {
     float g, f;
     minimumRadius = kInf;
     maximumRadius = 0.f;
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++)
-        for (int k = 0; k < 3; k++) {
+    for (int i = 0; i < n1; i++)
+      for (int j = 0; j < n2; j++)
+        for (int k = 0; k < n3; k++) {
           float candidateRadius = circleFrom3(x1[i], y1[i], x2[j], y2[j], x3[k], y3[k], g, f);
           maximumRadius = fmax_(candidateRadius, maximumRadius);
           minimumRadius = fmin_(candidateRadius, minimumRadius);
@@ -1243,51 +1247,23 @@ namespace lst {
                              s.mdIndices[2 * seg3 + 1],
                              s.mdIndices[2 * seg4 + 1]};
 
-    T4Input q1{lm[0], lm[1], lm[2], lm[3], seg1, seg3, mdIdx[0], mdIdx[1], mdIdx[2], mdIdx[3]};
-    if (!t4Select(m, md, s, q1))
-      return false;
-    T4Input q2{lm[0], lm[1], lm[3], lm[4], seg1, seg4, mdIdx[0], mdIdx[1], mdIdx[3], mdIdx[4]};
-    if (!t4Select(m, md, s, q2))
-      return false;
-
     float xs[5], ys[5];
     for (int i = 0; i < 5; ++i) {
       xs[i] = md.anchorX[mdIdx[i]];
       ys[i] = md.anchorY[mdIdx[i]];
     }
-    // Candidate positions of each anchor hit: the hit itself, or the two strip
-    // ends for 2S endcap modules.
-    float px[5][3], py[5][3];
-    for (int i = 0; i < 5; ++i) {
-      px[i][0] = px[i][1] = px[i][2] = xs[i];
-      py[i][0] = py[i][1] = py[i][2] = ys[i];
-      if (m.subdets[lm[i]] == Endcap and m.moduleType[lm[i]] == TwoS) {
-        px[i][1] = md.anchorLowEdgeX[mdIdx[i]];
-        px[i][2] = md.anchorHighEdgeX[mdIdx[i]];
-        py[i][1] = md.anchorLowEdgeY[mdIdx[i]];
-        py[i][2] = md.anchorHighEdgeY[mdIdx[i]];
-      }
-    }
-    float innerRadiusMin2S, innerRadiusMax2S, bridgeRadiusMin2S, bridgeRadiusMax2S, outerRadiusMin2S, outerRadiusMax2S;
-    radiusSpread(px[0], py[0], px[1], py[1], px[2], py[2], innerRadiusMin2S, innerRadiusMax2S);
-    radiusSpread(px[1], py[1], px[2], py[2], px[3], py[3], bridgeRadiusMin2S, bridgeRadiusMax2S);
-    radiusSpread(px[2], py[2], px[3], py[3], px[4], py[4], outerRadiusMin2S, outerRadiusMax2S);
-    (void)outerRadiusMin2S;
-    (void)outerRadiusMax2S;
-
     float g, f;
     v.outerRadius = t.circleRadius[outerT3];
     v.bridgeRadius = circleFrom3(xs[1], ys[1], xs[2], ys[2], xs[3], ys[3], g, f);
     v.innerRadius = t.circleRadius[innerT3];
-    g = t.circleCenterX[innerT3];
-    f = t.circleCenterY[innerT3];
 
-    float inner_pt = 2 * k2Rinv1GeVf * v.innerRadius;
-    bool tight = false;
-    if (!t5PassRZ(m, md, mdIdx, lm, v.rzChiSquared, inner_pt, v.innerRadius, g, f, tight))
+    // Every test below is a pure function of the candidate and all must pass,
+    // so they run cheapest first: the radius tests of
+    // SDL/Quintuplet.h:2740-2906 before the two beta algorithms of :2555-2622
+    // and the rz test of :2715-2735.
+    const bool pass = (v.innerRadius >= 0.95f * kPtCut / (2.f * k2Rinv1GeVf));
+    if (!pass)
       return false;
-    bool pass = (v.innerRadius >= 0.95f * kPtCut / (2.f * k2Rinv1GeVf));
-
     short s1 = m.subdets[lm[0]], s2 = m.subdets[lm[1]], s3 = m.subdets[lm[2]], s4 = m.subdets[lm[3]],
           s5 = m.subdets[lm[4]];
     int kind;
@@ -1303,9 +1279,44 @@ namespace lst {
       kind = 6;
     else
       kind = 7;
-    bool tempPass = matchRadii(
-        kind, v.innerRadius, v.bridgeRadius, innerRadiusMin2S, innerRadiusMax2S, bridgeRadiusMin2S, bridgeRadiusMax2S);
-    if (!(pass and tempPass))
+    // Radius spreads over the strip ends of 2S endcap hits; only the tests of
+    // kinds >= 2 read them (the reference's third, outer spread is unused).
+    float innerRadiusMin2S = 0.f, innerRadiusMax2S = 0.f, bridgeRadiusMin2S = 0.f, bridgeRadiusMax2S = 0.f;
+    if (kind >= 2) {
+      float px[5][3], py[5][3];
+      int np[5];
+      for (int i = 0; i < 5; ++i) {
+        px[i][0] = px[i][1] = px[i][2] = xs[i];
+        py[i][0] = py[i][1] = py[i][2] = ys[i];
+        np[i] = 1;
+        if (m.subdets[lm[i]] == Endcap and m.moduleType[lm[i]] == TwoS) {
+          px[i][1] = md.anchorLowEdgeX[mdIdx[i]];
+          px[i][2] = md.anchorHighEdgeX[mdIdx[i]];
+          py[i][1] = md.anchorLowEdgeY[mdIdx[i]];
+          py[i][2] = md.anchorHighEdgeY[mdIdx[i]];
+          np[i] = 3;
+        }
+      }
+      if (kind >= 6)
+        radiusSpread(px[0], py[0], np[0], px[1], py[1], np[1], px[2], py[2], np[2], innerRadiusMin2S, innerRadiusMax2S);
+      radiusSpread(px[1], py[1], np[1], px[2], py[2], np[2], px[3], py[3], np[3], bridgeRadiusMin2S, bridgeRadiusMax2S);
+    }
+    if (!matchRadii(
+            kind, v.innerRadius, v.bridgeRadius, innerRadiusMin2S, innerRadiusMax2S, bridgeRadiusMin2S, bridgeRadiusMax2S))
+      return false;
+
+    T4Input q1{lm[0], lm[1], lm[2], lm[3], seg1, seg3, mdIdx[0], mdIdx[1], mdIdx[2], mdIdx[3]};
+    if (!t4Select(m, md, s, q1))
+      return false;
+    T4Input q2{lm[0], lm[1], lm[3], lm[4], seg1, seg4, mdIdx[0], mdIdx[1], mdIdx[3], mdIdx[4]};
+    if (!t4Select(m, md, s, q2))
+      return false;
+
+    g = t.circleCenterX[innerT3];
+    f = t.circleCenterY[innerT3];
+    float inner_pt = 2 * k2Rinv1GeVf * v.innerRadius;
+    bool tight = false;
+    if (!t5PassRZ(m, md, mdIdx, lm, v.rzChiSquared, inner_pt, v.innerRadius, g, f, tight))
       return false;
 
     float sigmas[5], delta1[5], delta2[5], slopes[5];
