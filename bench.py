@@ -51,18 +51,16 @@ HBM_FALLBACK_GBS = 6650.0
 #   MD: 40 B per hit in (x, y, z, rt, phi, eta, 4 edges) + 134 B per MD out
 #   LS: 44 B per MD in + 80 B per module (module map) + 44 B per LS out
 #   T3: 24 B per LS + 20 B per MD in + 60 B per T3 out
-#   T5: 60 B per T3 + 56 B per MD in + 110 B per T5 out
-#   pT3/pT5: 76 B per pLS + 4 B per connected-module entry + 60 B per T3 (or
-#            110 B per T5) in + 100 B per pT3/pT5 out
+#   T5 (kT5Eval): 60 B per T3 + 56 B per MD in + 110 B per T5 out
+#   pT3/pT5 (kPixEval): 76 B per pLS + 4 B per connected-module entry + 60 B per
+#            T3 (or 110 B per T5) in + 100 B per pT3/pT5 out
 ALGO_BYTES = {
     "kCreateMD": lambda c: 40 * c["nHits"] + 134 * c["nMD"],
     "kCreateLS": lambda c: 44 * c["nMD"] + 80 * c["nLower"] + 44 * c["nLS"],
     "kCreateT3": lambda c: 24 * c["nLS"] + 20 * c["nMD"] + 60 * c["nT3"],
-    "kCreateT5": lambda c: 60 * c["nT3"] + 56 * c["nMD"] + 110 * c["nT5"],
-    "kPT3Count": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 60 * c["nT3"],
-    "kPT3Emit": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 60 * c["nT3"] + 100 * c["nPT3"],
-    "kPT5Count": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 110 * c["nT5"],
-    "kPT5Emit": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 110 * c["nT5"] + 100 * c["nPT5"],
+    "kT5Eval": lambda c: 60 * c["nT3"] + 56 * c["nMD"] + 110 * c["nT5"],
+    "kPixEval<3>": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 60 * c["nT3"] + 100 * c["nPT3"],
+    "kPixEval<5>": lambda c: 76 * c["nPLS"] + 4 * 40 * c["nPLS"] + 110 * c["nT5"] + 100 * c["nPT5"],
 }
 
 

@@ -117,6 +117,11 @@ namespace lst {
 
   LST_HD float deltaPhiChange(float x1, float y1, float x2, float y2) { return deltaPhi(x1, y1, x2 - x1, y2 - y1); }
 
+  // deltaPhiChange(x1, y1, x2, y2) with phi1 = phiOf(x1, y1) already known.
+  LST_HD float deltaPhiChangeFrom(float phi1, float x1, float y1, float x2, float y2) {
+    return phiMpiPi(phiOf(x2 - x1, y2 - y1) - phi1);
+  }
+
   // The reference's sign transfer: |a| with the product of the signs of a and b.
   LST_HD float signTransfer(float a, float b) {
     int sign_a = (a < 0) ? -1 : 1;

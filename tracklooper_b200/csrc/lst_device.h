@@ -54,7 +54,9 @@ namespace lst {
     unsigned int t5CandTotal;     // quintuplet candidates of the event
     unsigned int t5CandOverflow;  // more candidates than the flag buffer holds
     unsigned int t5PassCount;     // passing candidates found by kT5Eval
-    unsigned int pad[3];
+    unsigned int pixCandTotal;    // pT5 / pT3 candidates of the current pixel stage
+    unsigned int pixPassCount;    // passing candidates found by kPixEval
+    unsigned int pixFallback;     // the pixel stage overflowed the staging: walk instead
   };
 
   // All device pointers of one event.
@@ -100,6 +102,13 @@ namespace lst {
     unsigned int* t5ModOff;     // per eligible module: first candidate of the event
     unsigned int* t5CandFlag;   // per candidate: 0 = fails, else 1 + slot of its values in t5PassValues
     T5Values* t5PassValues;     // selection values of passing candidates
+    unsigned int* plsModPre;    // per pLS: candidate prefix over its connected modules (41 entries)
+    unsigned int* plsCand;      // per pLS: candidates
+    unsigned int* plsCandOff;   // per pLS: first candidate (nPLS + 1 entries)
+    unsigned int* pixPassC;     // passing candidates: candidate index
+    unsigned int* pixPassObj;   //   the T5 / T3 index
+    unsigned int* pixPassPLS;   //   the pLS index
+    float* pixPassV;            //   the selection values (8 per candidate)
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
     unsigned int maxHits;

@@ -406,6 +406,10 @@ namespace {
         break;
       case LST_STAGE_PIXEL_QUINTUPLETS:
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPixPrefix<5>, warpGrid(P, 8, count), 256, d, v);
+        LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kPixEval<5>, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v);
+        LST_LAUNCH(lst::kPixRankEmit<5>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 0);
         LST_LAUNCH(lst::kPT5Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
@@ -415,6 +419,10 @@ namespace {
         break;
       case LST_STAGE_PIXEL_TRIPLETS:
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPixPrefix<3>, warpGrid(P, 8, count), 256, d, v);
+        LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kPixEval<3>, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v);
+        LST_LAUNCH(lst::kPixRankEmit<3>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT3Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 1);
         LST_LAUNCH(lst::kPT3Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
@@ -515,6 +523,13 @@ namespace {
         {"kPLSClean", (const void*)lst::kPLSClean},
         {"kMergePLSFlag", (const void*)lst::kMergePLSFlag},
         {"kPixelConnect", (const void*)lst::kPixelConnect},
+        {"kPixPrefix<5>", (const void*)lst::kPixPrefix<5>},
+        {"kPixPrefix<3>", (const void*)lst::kPixPrefix<3>},
+        {"kPixScan", (const void*)lst::kPixScan},
+        {"kPixEval<5>", (const void*)lst::kPixEval<5>},
+        {"kPixEval<3>", (const void*)lst::kPixEval<3>},
+        {"kPixRankEmit<5>", (const void*)lst::kPixRankEmit<5>},
+        {"kPixRankEmit<3>", (const void*)lst::kPixRankEmit<3>},
         {"kPT5Count", (const void*)lst::kPT5Count},
         {"kPT5Emit", (const void*)lst::kPT5Emit},
         {"kPLSScan", (const void*)lst::kPLSScan},

@@ -236,5 +236,12 @@
   X(t5ModOff, unsigned int, L + 1)                    \
   X(t5CandFlag, unsigned int, lst::kT5CandCap)        \
   X(t5PassValues, lst::T5Values, lst::kT5PassCap)     \
+  X(plsModPre, unsigned int, P * (lst::kMaxConnectedModules + 1)) \
+  X(plsCand, unsigned int, P)                         \
+  X(plsCandOff, unsigned int, P + 1)                  \
+  X(pixPassC, unsigned int, lst::kPixPassCap)         \
+  X(pixPassObj, unsigned int, lst::kPixPassCap)       \
+  X(pixPassPLS, unsigned int, lst::kPixPassCap)       \
+  X(pixPassV, float, 8 * lst::kPixPassCap)            \
   X(plsOrder, unsigned int, P)                        \
   X(plsBinStart, unsigned int, 128)

@@ -305,6 +305,8 @@ namespace lst {
                         h.ys[upperIdx],
                         h.zs[upperIdx],
                         h.rts[upperIdx],
+                        h.phis[lowerIdx],
+                        h.phis[upperIdx],
                         v);
         }
       }
@@ -1218,6 +1220,8 @@ namespace lst {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
+    if (!ev.sc->pixFallback)
+      return;
     const int wib = threadIdx.x >> 5;
     const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
     for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
@@ -1232,6 +1236,8 @@ namespace lst {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
+    if (!ev.sc->pixFallback)
+      return;
     const int wib = threadIdx.x >> 5;
     const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
     for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
@@ -1246,6 +1252,8 @@ namespace lst {
   // which = 0: pT5 (cap 15000), 1: pT3 (cap 5000).
   __global__ void __launch_bounds__(1024) kPLSScan(DeviceES es, const EventView* evs, int which) {
     const EventView& ev = evs[blockIdx.y];
+    if (!ev.sc->pixFallback)
+      return;
     const unsigned int n = ev.ls.nSegments[es.pixelModule];
     unsigned int carry = 0;
     for (unsigned int base = 0; base < n; base += blockDim.x) {
@@ -1458,6 +1466,8 @@ namespace lst {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
+    if (!ev.sc->pixFallback)
+      return;
     const int wib = threadIdx.x >> 5;
     const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
     for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
@@ -1472,6 +1482,8 @@ namespace lst {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
+    if (!ev.sc->pixFallback)
+      return;
     const int wib = threadIdx.x >> 5;
     const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
     for (unsigned int i = blockIdx.x * kPixWarps + wib; i < nPLS; i += gridDim.x * kPixWarps) {
@@ -1479,6 +1491,233 @@ namespace lst {
       if (ev.plsCount[i] == 0 || ev.plsOffset[i] >= kMaxPixelTriplets)
         continue;
       pt3Walk<true>(es, ev, i, sPre[wib], sMods[wib]);
+    }
+  }
+
+  // ------------------------------------- pT5 / pT3 as candidate lists
+  // Candidate c of the event is the c-th (pLS, connected module, object) of
+  // the reference's loop nest (SDL/PixelTriplet.h:1043-1158, :2697-2786), so
+  // the global rank of a passing candidate is the number of passing
+  // candidates with a smaller c.  Every candidate is evaluated on its own
+  // thread; the passing ones are appended with their values and one block
+  // per event ranks them by c and stores the first 15000 (pT5) / 5000 (pT3).
+  // Events with more passing candidates than the staging holds take the
+  // per-pLS count/emit walk instead.
+  constexpr unsigned int kPixPassCap = 8192;
+  constexpr int kConnStride = kMaxConnectedModules + 1;
+
+  template <int K>
+  __device__ __forceinline__ unsigned int pixModuleCount(DeviceES const& es, const EventView& ev, uint16_t mod) {
+    return K == 5 ? pt5ModuleCount(es, ev, mod) : pt3ModuleCount(es, ev, mod);
+  }
+
+  template <int K>
+  __device__ __forceinline__ bool pixSkipPLS(const EventView& ev, unsigned int i) {
+    return K == 5 ? (ev.ls.isDup[i] != 0) : (ev.ls.isDup[i] || ev.ls.partOfPT5[i]);
+  }
+
+  template <int K>
+  __global__ void kPixPrefix(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const int wpb = blockDim.x >> 5;
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    for (unsigned int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < nPLS; i += gridDim.x * wpb) {
+      unsigned int carry = 0;
+      unsigned int* pre = ev.plsModPre + size_t(i) * kConnStride;
+      if (!pixSkipPLS<K>(ev, i)) {
+        const unsigned int nConn = ev.plsConnSize[i];
+        const unsigned int cidx = ev.plsConnIndex[i];
+        for (unsigned int b = 0; b < nConn; b += 32) {
+          const unsigned int k = b + laneId();
+          const unsigned int c =
+              k < nConn ? pixModuleCount<K>(es, ev, static_cast<uint16_t>(es.m.connectedPixels[cidx + k])) : 0u;
+          unsigned int incl = c;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            unsigned int y = __shfl_up_sync(kFullMask, incl, o);
+            if (int(laneId()) >= o)
+              incl += y;
+          }
+          if (k < nConn)
+            pre[k] = carry + incl - c;
+          carry += __shfl_sync(kFullMask, incl, 31);
+        }
+      }
+      if (laneId() == 0)
+        ev.plsCand[i] = carry;
+    }
+  }
+
+  __global__ void __launch_bounds__(1024) kPixScan(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = ev.ls.nSegments[es.pixelModule];
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int c = i < n ? ev.plsCand[i] : 0u;
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(c, tot);
+      if (i < n)
+        ev.plsCandOff[i] = carry + ex;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      ev.plsCandOff[n] = carry;
+      ev.sc->pixCandTotal = carry;
+      ev.sc->pixPassCount = 0;
+    }
+  }
+
+  // (pLS, object) of candidate c.
+  template <int K>
+  __device__ __forceinline__ void pixCandidate(DeviceES const& es, const EventView& ev, unsigned int c, unsigned int& iPLS,
+                                               unsigned int& obj, uint16_t& mod) {
+    const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
+    const unsigned int* off = ev.plsCandOff;
+    int lo = 0, hi = int(nPLS);
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (off[mid] <= c)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    iPLS = lo;
+    const unsigned int f = c - off[lo];
+    const unsigned int* pre = ev.plsModPre + size_t(lo) * kConnStride;
+    int klo = 0, khi = int(ev.plsConnSize[lo]);
+    while (khi - klo > 1) {
+      int mid = (klo + khi) >> 1;
+      if (pre[mid] <= f)
+        klo = mid;
+      else
+        khi = mid;
+    }
+    mod = static_cast<uint16_t>(es.m.connectedPixels[ev.plsConnIndex[lo] + klo]);
+    obj = (K == 5 ? static_cast<unsigned int>(ev.rg.quintupletModuleIndices[mod])
+                  : static_cast<unsigned int>(ev.rg.tripletModuleIndices[mod])) +
+          (f - pre[klo]);
+  }
+
+  template <int K>
+  __global__ void kPixEval(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int total = ev.sc->pixCandTotal;
+    const unsigned int plsBase = es.lsOffset[es.nLowerModules];
+    for (unsigned int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+      unsigned int iPLS, obj;
+      uint16_t mod;
+      pixCandidate<K>(es, ev, c, iPLS, obj, mod);
+      float vals[8];
+      bool ok;
+      if (K == 5) {
+        PT5Values v;
+        ok = !ev.t5.isDup[obj] && pt5Select(es.m, ev.rg, ev.md, ev.ls, ev.t3, ev.t5, plsBase + iPLS, obj, iPLS, v);
+        vals[0] = v.rzChiSquared;
+        vals[1] = v.rPhiChiSquared;
+        vals[2] = v.rPhiChiSquaredInwards;
+        vals[3] = v.pixelRadius;
+        vals[4] = v.quintupletRadius;
+        vals[5] = v.centerX;
+        vals[6] = v.centerY;
+        vals[7] = 0.f;
+      } else {
+        PT3Values v;
+        ok = es.m.moduleType[ev.t3.lowerModuleIndices[3 * obj + 1]] != TwoS && !ev.t3.partOfPT5[obj] &&
+             pt3Select(es.m, ev.rg, ev.md, ev.ls, ev.t3, plsBase + iPLS, obj, true, v);
+        vals[0] = v.pixelRadius;
+        vals[1] = v.pixelRadiusError;
+        vals[2] = v.tripletRadius;
+        vals[3] = v.centerX;
+        vals[4] = v.centerY;
+        vals[5] = v.rzChiSquared;
+        vals[6] = v.rPhiChiSquared;
+        vals[7] = v.rPhiChiSquaredInwards;
+      }
+      if (ok) {
+        const unsigned int slot = atomicAdd(&ev.sc->pixPassCount, 1u);
+        if (slot < kPixPassCap) {
+          ev.pixPassC[slot] = c;
+          ev.pixPassObj[slot] = obj;
+          ev.pixPassPLS[slot] = iPLS;
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            ev.pixPassV[8 * slot + k] = vals[k];
+        }
+      }
+    }
+  }
+
+  // Ranks the passing candidates by c and stores them; one block per event.
+  template <int K>
+  __global__ void __launch_bounds__(1024) kPixRankEmit(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sKey[kPixPassCap];
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = ev.sc->pixPassCount;
+    const unsigned int capOut = K == 5 ? kMaxPixelQuintuplets : kMaxPixelTriplets;
+    if (n > kPixPassCap) {
+      if (threadIdx.x == 0)
+        ev.sc->pixFallback = 1;
+      return;
+    }
+    for (unsigned int j = threadIdx.x; j < n; j += blockDim.x)
+      sKey[j] = ev.pixPassC[j];
+    __syncthreads();
+    const unsigned int plsBase = es.lsOffset[es.nLowerModules];
+    Segments ls = ev.ls;
+    Triplets t3 = ev.t3;
+    Quintuplets t5 = ev.t5;
+    for (unsigned int sIdx = threadIdx.x; sIdx < n; sIdx += blockDim.x) {
+      const unsigned int key = sKey[sIdx];
+      unsigned int rank = 0;
+      for (unsigned int j = 0; j < n; ++j)
+        rank += sKey[j] < key ? 1u : 0u;
+      if (rank >= capOut)
+        continue;
+      const unsigned int obj = ev.pixPassObj[sIdx];
+      const unsigned int iPLS = ev.pixPassPLS[sIdx];
+      const float* vals = ev.pixPassV + 8 * sIdx;
+      if (K == 5) {
+        PT5Values v;
+        v.rzChiSquared = vals[0];
+        v.rPhiChiSquared = vals[1];
+        v.rPhiChiSquaredInwards = vals[2];
+        v.pixelRadius = vals[3];
+        v.quintupletRadius = vals[4];
+        v.centerX = vals[5];
+        v.centerY = vals[6];
+        PixelQuintuplets pt5 = ev.pt5;
+        storePT5(ev.md, ls, t3, t5, pt5, plsBase + iPLS, iPLS, obj, v, rank);
+      } else {
+        PT3Values v;
+        v.pixelRadius = vals[0];
+        v.pixelRadiusError = vals[1];
+        v.tripletRadius = vals[2];
+        v.centerX = vals[3];
+        v.centerY = vals[4];
+        v.rzChiSquared = vals[5];
+        v.rPhiChiSquared = vals[6];
+        v.rPhiChiSquaredInwards = vals[7];
+        PixelTriplets pt3 = ev.pt3;
+        const short adj = es.m.layers[t3.lowerModuleIndices[3 * obj]] == 1 ? 1 : 0;
+        storePT3(es.m, ev.md, ls, t3, pt3, plsBase + iPLS, iPLS, obj, adj, v, rank);
+        t3.partOfPT3[obj] = 1;
+      }
+    }
+    if (threadIdx.x == 0) {
+      ev.sc->pixFallback = 0;
+      const unsigned int stored = n < capOut ? n : capOut;
+      if (K == 5) {
+        ev.sc->nPT5Total = n;
+        *ev.pt5.totOccupancyPixelQuintuplets = n;
+        *ev.pt5.nPixelQuintuplets = stored;
+      } else {
+        ev.sc->nPT3Total = n;
+        *ev.pt3.totOccupancyPixelTriplets = n;
+        *ev.pt3.nPixelTriplets = stored;
+      }
+      if (n > capOut)
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
     }
   }
 

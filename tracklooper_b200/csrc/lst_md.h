@@ -195,6 +195,8 @@ namespace lst {
                        float yUpper,
                        float zUpper,
                        float rtUpper,
+                       float phiLower,
+                       float phiUpper,
                        MDValues& v) {
     v.dz = zLower - zUpper;
     const float dzCut = m.moduleType[lm] == PS ? 2.f : 10.f;
@@ -216,17 +218,17 @@ namespace lst {
       shiftedRt = fsqrt(xn * xn + yn * yn);
       if (lowerIsPixel) {
         v.shiftedZ = zUpper;
-        v.dphi = deltaPhi(xLower, yLower, v.shiftedX, v.shiftedY);
+        v.dphi = phiMpiPi(phiOf(v.shiftedX, v.shiftedY) - phiLower);
       } else {
         v.shiftedZ = zLower;
-        v.dphi = deltaPhi(v.shiftedX, v.shiftedY, xUpper, yUpper);
+        v.dphi = phiMpiPi(phiUpper - phiOf(v.shiftedX, v.shiftedY));
       }
-      v.noShiftedDphi = deltaPhi(xLower, yLower, xUpper, yUpper);
+      v.noShiftedDphi = phiMpiPi(phiUpper - phiLower);
     } else {
       v.shiftedX = 0;
       v.shiftedY = 0;
       v.shiftedZ = 0;
-      v.dphi = deltaPhi(xLower, yLower, xUpper, yUpper);
+      v.dphi = phiMpiPi(phiUpper - phiLower);
       v.noShiftedDphi = v.dphi;
     }
     if (!(fabs_(v.dphi) < miniCut))
@@ -234,16 +236,16 @@ namespace lst {
 
     if (tilted) {
       if (!lowerIsPixel) {
-        v.dphichange = (rtLower < shiftedRt) ? deltaPhiChange(xLower, yLower, v.shiftedX, v.shiftedY)
+        v.dphichange = (rtLower < shiftedRt) ? deltaPhiChangeFrom(phiLower, xLower, yLower, v.shiftedX, v.shiftedY)
                                              : deltaPhiChange(v.shiftedX, v.shiftedY, xLower, yLower);
       } else {
         v.dphichange = (shiftedRt < rtUpper) ? deltaPhiChange(v.shiftedX, v.shiftedY, xUpper, yUpper)
-                                             : deltaPhiChange(xUpper, yUpper, v.shiftedX, v.shiftedY);
+                                             : deltaPhiChangeFrom(phiUpper, xUpper, yUpper, v.shiftedX, v.shiftedY);
       }
-      v.noShiftedDphiChange = rtLower < rtUpper ? deltaPhiChange(xLower, yLower, xUpper, yUpper)
-                                                : deltaPhiChange(xUpper, yUpper, xLower, yLower);
+      v.noShiftedDphiChange = rtLower < rtUpper ? deltaPhiChangeFrom(phiLower, xLower, yLower, xUpper, yUpper)
+                                                : deltaPhiChangeFrom(phiUpper, xUpper, yUpper, xLower, yLower);
     } else {
-      v.dphichange = deltaPhiChange(xLower, yLower, xUpper, yUpper);
+      v.dphichange = deltaPhiChangeFrom(phiLower, xLower, yLower, xUpper, yUpper);
       v.noShiftedDphiChange = v.dphichange;
     }
     v.noShiftedDz = 0;
@@ -262,6 +264,8 @@ namespace lst {
                        float yUpper,
                        float zUpper,
                        float rtUpper,
+                       float phiLower,
+                       float phiUpper,
                        MDValues& v) {
     float dz = zLower - zUpper;
     const float dzCut = 1.f;
@@ -281,16 +285,16 @@ namespace lst {
     if (isPS) {
       if (lowerIsPixel) {
         v.shiftedZ = zUpper;
-        v.dphi = deltaPhi(xLower, yLower, v.shiftedX, v.shiftedY);
+        v.dphi = phiMpiPi(phiOf(v.shiftedX, v.shiftedY) - phiLower);
       } else {
         v.shiftedZ = zLower;
-        v.dphi = deltaPhi(v.shiftedX, v.shiftedY, xUpper, yUpper);
+        v.dphi = phiMpiPi(phiUpper - phiOf(v.shiftedX, v.shiftedY));
       }
     } else {
       v.shiftedZ = zUpper;
-      v.dphi = deltaPhi(xLower, yLower, xn, yn);
+      v.dphi = phiMpiPi(phiOf(xn, yn) - phiLower);
     }
-    v.noShiftedDphi = deltaPhi(xLower, yLower, xUpper, yUpper);
+    v.noShiftedDphi = phiMpiPi(phiUpper - phiLower);
 
     if (isPS)
       dz = lowerIsPixel ? zLower - zn : zUpper - zn;
@@ -307,6 +311,8 @@ namespace lst {
     return fabs_(v.dphichange) < miniCut;
   }
 
+  // phiLower / phiUpper are the hits' stored phi (hits.phis, phi() of the same
+  // coordinates), used wherever the reference takes deltaPhi of a hit itself.
   LST_HD bool mdSelect(const Modules& m,
                        uint16_t lm,
                        float xLower,
@@ -317,10 +323,12 @@ namespace lst {
                        float yUpper,
                        float zUpper,
                        float rtUpper,
+                       float phiLower,
+                       float phiUpper,
                        MDValues& v) {
     if (m.subdets[lm] == Barrel)
-      return mdBarrel(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, v);
-    return mdEndcap(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, v);
+      return mdBarrel(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, phiLower, phiUpper, v);
+    return mdEndcap(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, phiLower, phiUpper, v);
   }
 
   // Writes a mini-doublet record (SDL/MiniDoublet.h:193-266).  On PS modules
