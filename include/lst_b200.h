@@ -148,6 +148,12 @@ void* lst_event_stream(lst_event* ev);
 /* Selects the T5 method (default LST_T5_DNN when weights were loaded). */
 int lst_event_set_t5_method(lst_event* ev, int method);
 
+/* The quintuplet and pixel stages evaluate their candidates as flat lists and
+ * fall back to one warp per module / pLS for events whose candidates overflow
+ * the list buffers.  on = 1 makes every event take the fallback (same
+ * results; for testing it). */
+int lst_event_set_walk(lst_event* ev, int on);
+
 /* Event::resetEvent (SDL/Event.cc:45): clears slot `slot`'s objects.  Adding
  * hits resets the slot as well. */
 int lst_event_reset(lst_event* ev, int slot);
@@ -226,6 +232,11 @@ int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, siz
 int lst_batch_ingest(lst_event* ev, int first, int count);
 /* Runs stages [first_stage, last_stage] for slots [first, first + count). */
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage);
+/* As lst_batch_run, replayed from a CUDA graph: the first call for a given
+ * (first, count, stage range, T5 method) captures the launches on the set's
+ * stream into a graph and every later call replays it with one launch.  The
+ * first call must not run while another capture is active on the stream. */
+int lst_batch_run_graph(lst_event* ev, int first, int count, int first_stage, int last_stage);
 /* Copies the counts of slots [first, first + count) into out[count]. */
 int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out);
 

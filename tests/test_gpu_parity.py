@@ -151,3 +151,45 @@ def test_batched_uneven_events_match_reference(ref, es):
         assert np.array_equal(ln[a:b], l1) and np.array_equal(seed[a:b], s1) and np.array_equal(typ[a:b], t1)
         assert np.array_equal(hits[int(hco[slot]):int(hco[slot + 1])], h1)
     eset.close()
+
+
+def test_fallback_walks_match_reference(ref, es):
+    """The warp-per-module / per-pLS walks (taken for overflowing events) give
+    the same objects as the candidate lists."""
+    inp = gen.generate_event(2, 3)
+    ev = lst.Event(es, max_hits=inp.n_hits + 1024)
+    ev.event_set.set_walk(True)
+    problems = _compare_event(ref, es, ev, inp)
+    ev.event_set.close()
+    assert not problems, _fmt(problems)
+
+
+def test_cut_only_method_matches_reference(es):
+    if not reflib.available("cr_cuts"):
+        pytest.skip("cut-only reference variant not built")
+    ref_cuts = reflib.RefLST("cr_cuts")
+    inp = gen.generate_event(2, 4)
+    ev = lst.Event(es, max_hits=inp.n_hits + 1024)
+    ev.event_set.set_t5_method(lst.T5_CUTS)
+    problems = _compare_event(ref_cuts, es, ev, inp)
+    ev.event_set.close()
+    ref_cuts.close()
+    assert not problems, _fmt(problems)
+
+
+def test_graph_replay_matches_direct_launches(es):
+    inputs = [gen.generate_event(3, 10 + i) for i in range(3)]
+    eset = lst.EventSet(es, n_slots=3, max_hits=max(i.n_hits for i in inputs) + 1024)
+    blob, offsets = lst.pack_events(inputs)
+    eset.upload_packed(0, blob, offsets)
+    eset.run(0, 3)
+    direct = eset.output(0, 3, tc_capacity=3 * 31000, hits_capacity=3 * 31000 * 14)
+    direct_counts = eset.batch_counts(0, 3)
+    for _ in range(2):  # capture, then replay
+        eset.ingest(0, 3)
+        eset.run_graph(0, 3)
+        out = eset.output(0, 3, tc_capacity=3 * 31000, hits_capacity=3 * 31000 * 14)
+        assert eset.batch_counts(0, 3) == direct_counts
+        for a, b in zip(direct, out):
+            assert np.array_equal(a, b)
+    eset.close()

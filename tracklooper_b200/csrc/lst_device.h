@@ -112,6 +112,7 @@ namespace lst {
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
     unsigned int maxHits;
+    unsigned int forceWalk;  // take the warp-per-object walks instead of the candidate lists
   };
 
 }  // namespace lst

@@ -11,10 +11,12 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -295,6 +297,12 @@ struct lst_event {
   std::vector<cudaEvent_t> eventPool;
   size_t poolUsed = 0;
   std::vector<ProfRecord> profile;
+  // CUDA graphs of lst_batch_run_graph, keyed by (first, count, stages, method)
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels = 0;
+  };
+  std::map<std::tuple<int, int, int, int, int, unsigned int>, GraphEntry> graphs;
 };
 
 namespace {
@@ -816,6 +824,8 @@ void lst_event_destroy(lst_event* ev) {
   cudaFreeHost(ev->hOutOffsets);
   for (cudaEvent_t e : ev->eventPool)
     cudaEventDestroy(e);
+  for (auto& g : ev->graphs)
+    cudaGraphExecDestroy(g.second.exec);
   if (ev->dOut)
     cudaFree(ev->dOut);
   if (ev->ownStream)
@@ -847,6 +857,16 @@ int lst_event_set_t5_method(lst_event* ev, int method) {
   if (method == LST_T5_DNN && !ev->es->haveDnn)
     return setError("the DNN T5 method needs weights");
   ev->t5Method = method;
+  return 0;
+}
+
+int lst_event_set_walk(lst_event* ev, int on) {
+  if (!ev)
+    return setError("null event set");
+  LST_CUDA(cudaStreamSynchronize(ev->stream));
+  for (auto& v : ev->hv)
+    v.forceWalk = on ? 1u : 0u;
+  LST_CUDA(cudaMemcpy(ev->dv, ev->hv.data(), sizeof(lst::EventView) * ev->nSlots, cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -1096,6 +1116,40 @@ int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last
     if (rc)
       return rc;
   }
+  return 0;
+}
+
+int lst_batch_run_graph(lst_event* ev, int first, int count, int first_stage, int last_stage) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (count == 0)
+    return 0;
+  if (ev->profiling)  // timing events cannot be read back from graph replays
+    return lst_batch_run(ev, first, count, first_stage, last_stage);
+  const auto key = std::make_tuple(first, count, first_stage, last_stage, ev->t5Method, ev->hv[first].forceWalk);
+  auto it = ev->graphs.find(key);
+  if (it == ev->graphs.end()) {
+    cudaGraph_t graph = nullptr;
+    LST_CUDA(cudaStreamBeginCapture(ev->stream, cudaStreamCaptureModeThreadLocal));
+    const unsigned long long before = ev->launches;
+    rc = lst_batch_run(ev, first, count, first_stage, last_stage);
+    cudaError_t e = cudaStreamEndCapture(ev->stream, &graph);
+    if (rc)
+      return rc;
+    if (e != cudaSuccess)
+      return cudaFail(e, "cudaStreamEndCapture");
+    lst_event::GraphEntry entry;
+    entry.kernels = ev->launches - before;
+    ev->launches = before;
+    e = cudaGraphInstantiate(&entry.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+      return cudaFail(e, "cudaGraphInstantiate");
+    it = ev->graphs.emplace(key, entry).first;
+  }
+  LST_CUDA(cudaGraphLaunch(it->second.exec, ev->stream));
+  ev->launches += it->second.kernels;
   return 0;
 }
 

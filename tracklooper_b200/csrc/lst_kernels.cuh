@@ -803,7 +803,7 @@ namespace lst {
     if (threadIdx.x == 0) {
       ev.t5ModOff[nE] = carry;
       ev.sc->t5CandTotal = carry;
-      ev.sc->t5CandOverflow = carry > kT5CandCap ? 1u : 0u;
+      ev.sc->t5CandOverflow = (carry > kT5CandCap || ev.forceWalk) ? 1u : 0u;
       ev.sc->t5PassCount = 0;
     }
   }
@@ -1655,7 +1655,7 @@ namespace lst {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = ev.sc->pixPassCount;
     const unsigned int capOut = K == 5 ? kMaxPixelQuintuplets : kMaxPixelTriplets;
-    if (n > kPixPassCap) {
+    if (n > kPixPassCap || ev.forceWalk) {
       if (threadIdx.x == 0)
         ev.sc->pixFallback = 1;
       return;

@@ -76,6 +76,7 @@ EXPORTS = (
     "lst_event_sync",
     "lst_event_stream",
     "lst_event_set_t5_method",
+    "lst_event_set_walk",
     "lst_event_reset",
     "lst_event_add_hits",
     "lst_event_add_pixel_segments",
@@ -98,6 +99,7 @@ EXPORTS = (
     "lst_batch_upload",
     "lst_batch_ingest",
     "lst_batch_run",
+    "lst_batch_run_graph",
     "lst_batch_get_counts",
     "lst_batch_get_output",
     "lst_event_launches",
@@ -214,6 +216,7 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_event_stream.argtypes = [vp]
         lib.lst_event_stream.restype = vp
         lib.lst_event_set_t5_method.argtypes = [vp, i32]
+        lib.lst_event_set_walk.argtypes = [vp, i32]
         lib.lst_event_reset.argtypes = [vp, i32]
         lib.lst_event_add_hits.argtypes = [vp, i32, u32] + [vp] * 5
         lib.lst_event_add_pixel_segments.argtypes = [vp, i32, u32] + [vp] * 18
@@ -231,6 +234,7 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_batch_upload.argtypes = [vp, i32, i32, vp, sz, vp]
         lib.lst_batch_ingest.argtypes = [vp, i32, i32]
         lib.lst_batch_run.argtypes = [vp, i32, i32, i32, i32]
+        lib.lst_batch_run_graph.argtypes = [vp, i32, i32, i32, i32]
         lib.lst_batch_get_counts.argtypes = [vp, i32, i32, ctypes.POINTER(Counts)]
         lib.lst_batch_get_output.argtypes = [vp, i32, i32, ctypes.POINTER(Output)]
         lib.lst_event_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
@@ -407,6 +411,9 @@ class EventSet:
     def sync(self):
         _check(library().lst_event_sync(self._h), "lst_event_sync")
 
+    def set_walk(self, on: bool):
+        _check(library().lst_event_set_walk(self._h, int(bool(on))), "lst_event_set_walk")
+
     def set_t5_method(self, method: int):
         _check(library().lst_event_set_t5_method(self._h, method), "lst_event_set_t5_method")
 
@@ -500,6 +507,10 @@ class EventSet:
         n = ctypes.c_int()
         _check(library().lst_event_get_profile(self._h, arr, 128, ctypes.byref(n)), "lst_event_get_profile")
         return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(min(n.value, 128))}
+
+    def run_graph(self, first: int, count: int, first_stage: int = STAGE_MINI_DOUBLETS,
+                  last_stage: int = STAGE_TRACK_CANDIDATES):
+        _check(library().lst_batch_run_graph(self._h, first, count, first_stage, last_stage), "lst_batch_run_graph")
 
     def batch_counts(self, first: int, count: int) -> list[dict]:
         arr = (Counts * count)()
