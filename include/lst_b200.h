@@ -126,6 +126,10 @@ int lst_es_load_host(const char* geometry_dir, lst_es** out);
  * t5CapIfEligible> (the static per-module offsets and occupancy caps). */
 int lst_es_host_array(const lst_es* es, const char* name, const void** data, size_t* n_elems, size_t* elem_size);
 int lst_es_get_info(const lst_es* es, lst_es_info* out);
+/* Sets the T5 DNN working point (the score a candidate must exceed; the
+ * reference's is 0.6177366, SDL/Constants.h:145), for every event set on the
+ * ES's device. */
+int lst_es_set_t5dnn_threshold(lst_es* es, float wp);
 /* Replaces the T5 DNN weights (same layout as the file).  The weights live
  * in constant memory of the ES's device and are shared by every event set on
  * that device; call between events. */
@@ -289,6 +293,33 @@ typedef struct lst_kernel_time {
 } lst_kernel_time;
 int lst_event_set_profiling(lst_event* ev, int on);
 int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int* n_kernels);
+
+/* ---------------------------------------------------------- T5 classifier */
+/* Classifier-stage probe (no reference counterpart; it serves retraining the
+ * T5 DNN of SDL/NeuralNetwork.h): after createQuintuplets, every quintuplet
+ * candidate of slots [first, first + count) that passes all cuts before the
+ * DNN decision is appended to the DEVICE buffers given: its 38 DNN inputs
+ * (feat, capacity x 38, in the order of SDL/NeuralNetwork.h:74-114), the
+ * loaded weights' score, the cut-only method's decision, the rz-fit tight
+ * flag, its 10 hit indices (event-local) and its slot.  *n_found receives the
+ * number of candidates found (entries beyond capacity are dropped). */
+int lst_batch_t5_probe(lst_event* ev, int first, int count, float* feat, float* score, uint8_t* cut_pass,
+                       uint8_t* rz_tight, uint32_t* hits, int32_t* event_index, uint32_t capacity,
+                       uint32_t* n_found);
+
+/* Forward and backward passes of the T5 DNN (38 -> 32 ReLU -> 32 ReLU -> 1)
+ * for training, on device buffers in the caller's stream (a cudaStream_t).
+ * weights: 2337 floats in the weight-file layout.  Forward: x (n x 38) ->
+ * h1, h2 (n x 32, kept for the backward pass), logit (n).  Backward: from
+ * dlogit (n, the loss gradient w.r.t. the logits) -> grad (2337, same layout
+ * as the weights); scratch needs lst_t5dnn_scratch_floats(n) floats.  The
+ * reductions run in a fixed order, so the gradient is deterministic. */
+int lst_t5dnn_forward(const float* weights, const float* x, int n, float* h1, float* h2, float* logit, void* stream);
+size_t lst_t5dnn_scratch_floats(int n);
+int lst_t5dnn_backward(const float* weights, const float* x, const float* h1, const float* h2, const float* dlogit,
+                       int n, float* grad, float* scratch, void* stream);
+/* Last error message of the two training entry points above. */
+const char* lst_t5dnn_last_error(void);
 
 #ifdef __cplusplus
 }

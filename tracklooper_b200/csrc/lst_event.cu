@@ -291,6 +291,7 @@ struct lst_event {
   unsigned long long* hOutOffsets = nullptr;  // pinned copy
   unsigned char* dOut = nullptr;
   size_t dOutBytes = 0;
+  unsigned int* dProbeCount = nullptr;
   // launch accounting and optional per-launch timing
   unsigned long long launches = 0;
   bool profiling = false;
@@ -525,6 +526,7 @@ namespace {
         {"kT5Eval", (const void*)lst::kT5Eval},
         {"kT5Emit", (const void*)lst::kT5Emit},
         {"kT5Walk", (const void*)lst::kT5Walk},
+        {"kT5Probe", (const void*)lst::kT5Probe},
         {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
         {"kT5Ranges", (const void*)lst::kT5Ranges},
         {"kPLSBin", (const void*)lst::kPLSBin},
@@ -826,6 +828,8 @@ void lst_event_destroy(lst_event* ev) {
     cudaEventDestroy(e);
   for (auto& g : ev->graphs)
     cudaGraphExecDestroy(g.second.exec);
+  if (ev->dProbeCount)
+    cudaFree(ev->dProbeCount);
   if (ev->dOut)
     cudaFree(ev->dOut);
   if (ev->ownStream)
@@ -1150,6 +1154,45 @@ int lst_batch_run_graph(lst_event* ev, int first, int count, int first_stage, in
   }
   LST_CUDA(cudaGraphLaunch(it->second.exec, ev->stream));
   ev->launches += it->second.kernels;
+  return 0;
+}
+
+int lst_batch_t5_probe(lst_event* ev, int first, int count, float* feat, float* score, uint8_t* cut_pass,
+                       uint8_t* rz_tight, uint32_t* hits, int32_t* event_index, uint32_t capacity,
+                       uint32_t* n_found) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (!n_found || (capacity && (!feat || !score || !cut_pass || !rz_tight || !hits || !event_index)))
+    return setError("lst_batch_t5_probe: null argument");
+  if (!ev->es->haveDnn)
+    return setError("lst_batch_t5_probe: needs T5 DNN weights");
+  *n_found = 0;
+  if (count == 0)
+    return 0;
+  if (!ev->dProbeCount)
+    LST_CUDA(cudaMalloc(&ev->dProbeCount, sizeof(unsigned int)));
+  cudaStream_t s = ev->stream;
+  const lst::DeviceES& d = ev->es->view;
+  const lst::EventView* v = ev->dv + first;
+  LST_CUDA(cudaMemsetAsync(ev->dProbeCount, 0, sizeof(unsigned int), s));
+  LST_LAUNCH(lst::kT5Prefix, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v);
+  LST_LAUNCH(lst::kT5ModScan, dim3(1, count), 1024, d, v);
+  lst::T5ProbeOut out{feat, score, cut_pass, rz_tight, hits, event_index, capacity, ev->dProbeCount};
+  LST_LAUNCH(lst::kT5Probe, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v, first, out);
+  unsigned int n = 0;
+  LST_CUDA(cudaMemcpyAsync(&n, ev->dProbeCount, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  LST_CUDA(cudaStreamSynchronize(s));
+  *n_found = n;
+  return 0;
+}
+
+int lst_es_set_t5dnn_threshold(lst_es* es, float wp) {
+  if (!es || es->device < 0)
+    return setError("lst_es_set_t5dnn_threshold: no device event setup");
+  LST_CUDA(cudaSetDevice(es->device));
+  LST_CUDA(cudaMemcpyToSymbol(lst::c_t5dnnWP, &wp, sizeof(float)));
+  LST_CUDA(cudaDeviceSynchronize());
   return 0;
 }
 

@@ -20,6 +20,7 @@ namespace lst {
 
   // T5 classifier weights (uploaded once per process from the weight file).
   __constant__ T5DnnWeights c_t5dnn;
+  __constant__ float c_t5dnnWP = kT5DnnWP;  // DNN working point of the loaded weights
 
   struct ConstDnn {
     __device__ __forceinline__ const T5DnnWeights& get() const { return c_t5dnn; }
@@ -699,7 +700,7 @@ namespace lst {
         outerT3 = outerBase + ev.t3ByMD[outerBase + ev.mdT3Start[mdMid] + (f - pre[i])];
         lm[3] = t3.lowerModuleIndices[3 * outerT3 + 1];
         lm[4] = t3.lowerModuleIndices[3 * outerT3 + 2];
-        ok = t5Select(m, ev.md, ev.ls, t3, dnn.get(), useDnn, lm, innerT3, outerT3, v);
+        ok = t5Select(m, ev.md, ev.ls, t3, dnn.get(), useDnn, c_t5dnnWP, lm, innerT3, outerT3, v);
       }
       unsigned int tot;
       unsigned int r = count + warpRank(ok, tot);
@@ -835,7 +836,7 @@ namespace lst {
                         ev.t3.lowerModuleIndices[3 * outerT3 + 2]};
       T5Values v;
       unsigned int flag = 0;
-      if (t5Select(es.m, ev.md, ev.ls, ev.t3, dnn.get(), useDnn, lm, innerT3, outerT3, v)) {
+      if (t5Select(es.m, ev.md, ev.ls, ev.t3, dnn.get(), useDnn, c_t5dnnWP, lm, innerT3, outerT3, v)) {
         // keep the values of a passing candidate (flag = slot + 1), or mark
         // it for re-evaluation (flag = kT5PassCap + 1) when the buffer is full
         const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
@@ -901,7 +902,7 @@ namespace lst {
           if (flag <= kT5PassCap)
             v = ev.t5PassValues[flag - 1];
           else
-            t5Select(es.m, ev.md, ev.ls, t3, dnn.get(), useDnn, lm, innerT3, outerT3, v);
+            t5Select(es.m, ev.md, ev.ls, t3, dnn.get(), useDnn, c_t5dnnWP, lm, innerT3, outerT3, v);
           storeT5(ev.md, ev.ls, t3, t5, innerT3, outerT3, lm, layer, v, base + r);
         }
         count += tot;
@@ -912,6 +913,63 @@ namespace lst {
         if (int(count) > cap)
           atomicOr(&ev.sc->status, kStatusCapOverflow);
       }
+    }
+  }
+
+  // Classifier-stage probe: every T5 candidate that reaches the DNN decision,
+  // with its features, the loaded weights' score, the cut-only decision and
+  // its 10 hits, appended to the caller's buffers (order not fixed).
+  struct T5ProbeOut {
+    float* feat;      // capacity x 38
+    float* score;     // capacity
+    uint8_t* cutPass; // capacity
+    uint8_t* rzTight; // capacity
+    unsigned int* hits;  // capacity x 10 (event-local hit indices)
+    int* eventIndex;     // capacity (slot)
+    unsigned int capacity;
+    unsigned int* count;
+  };
+
+  __global__ void kT5Probe(DeviceES es, const EventView* evs, int firstSlot, T5ProbeOut out) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int total = ev.sc->t5CandTotal;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    const unsigned int* off = ev.t5ModOff;
+    ConstDnn dnn;
+    for (unsigned int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+      int lo = 0, hi = nE;
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= c)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
+      unsigned int innerT3, outerT3;
+      t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
+      uint16_t lm[5] = {lm1,
+                        ev.t3.lowerModuleIndices[3 * innerT3 + 1],
+                        ev.t3.lowerModuleIndices[3 * innerT3 + 2],
+                        ev.t3.lowerModuleIndices[3 * outerT3 + 1],
+                        ev.t3.lowerModuleIndices[3 * outerT3 + 2]};
+      T5Values v;
+      T5Probe p;
+      if (!t5Select(es.m, ev.md, ev.ls, ev.t3, dnn.get(), true, c_t5dnnWP, lm, innerT3, outerT3, v, &p))
+        continue;
+      const unsigned int slot = atomicAdd(out.count, 1u);
+      if (slot >= out.capacity)
+        continue;
+      for (int k = 0; k < 38; ++k)
+        out.feat[38 * size_t(slot) + k] = p.feat[k];
+      out.score[slot] = p.dnnScore;
+      out.cutPass[slot] = p.cutPass ? 1 : 0;
+      out.rzTight[slot] = p.rzTight ? 1 : 0;
+      for (int k = 0; k < 6; ++k)
+        out.hits[10 * size_t(slot) + k] = ev.t3.hitIndices[6 * innerT3 + k];
+      for (int k = 0; k < 4; ++k)
+        out.hits[10 * size_t(slot) + 6 + k] = ev.t3.hitIndices[6 * outerT3 + 2 + k];
+      out.eventIndex[slot] = firstSlot + int(blockIdx.y);
     }
   }
 

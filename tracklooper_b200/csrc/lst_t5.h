@@ -1214,6 +1214,16 @@ namespace lst {
   }
 
   // ------------------------------------------------------------ T5 driver
+  // What the T5 selection sees at the classifier stage (for training and
+  // studying the classifier): the 38 DNN inputs, the score of the loaded
+  // weights, and the cut-only method's decision on the same candidate.
+  struct T5Probe {
+    float feat[38];
+    float dnnScore;
+    bool cutPass;
+    bool rzTight;
+  };
+
   struct T5Values {
     float innerRadius, outerRadius, bridgeRadius, regressionG, regressionF, regressionRadius, rzChiSquared, chiSquared,
         nonAnchorChiSquared;
@@ -1222,8 +1232,9 @@ namespace lst {
 
   // Full T5 selection for one (inner T3, outer T3) pair
   // (SDL/Quintuplet.h:2508-2984).  useDnn selects the DNN method
-  // (USE_RZCHI2 + USE_T5_DNN), otherwise the cut-only method
-  // (USE_RZCHI2 + USE_RPHICHI2).
+  // (USE_RZCHI2 + USE_T5_DNN) with working point dnnWP (the reference's is
+  // kT5DnnWP), otherwise the cut-only method (USE_RZCHI2 + USE_RPHICHI2).
+  // With a probe, stops at the classifier stage and fills it instead.
   template <typename W>
   LST_HD bool t5Select(const Modules& m,
                        const MiniDoublets& md,
@@ -1231,10 +1242,12 @@ namespace lst {
                        const Triplets& t,
                        const W& dnn,
                        bool useDnn,
+                       float dnnWP,
                        const uint16_t* lm,
                        unsigned int innerT3,
                        unsigned int outerT3,
-                       T5Values& v) {
+                       T5Values& v,
+                       T5Probe* probe = nullptr) {
     unsigned int seg1 = t.segmentIndices[2 * innerT3];
     unsigned int seg2 = t.segmentIndices[2 * innerT3 + 1];
     unsigned int seg3 = t.segmentIndices[2 * outerT3];
@@ -1325,13 +1338,22 @@ namespace lst {
     v.regressionRadius =
         circleRegression(5, xs, ys, delta1, delta2, slopes, isFlat, v.regressionG, v.regressionF, sigmas, v.chiSquared);
 
+    if (probe) {
+      // classifier-stage snapshot: stop before either method decides
+      t5DnnFeatures(m, md, s, t, xs, ys, mdIdx, lm, innerT3, v.innerRadius, v.outerRadius, v.bridgeRadius,
+                    probe->feat);
+      probe->dnnScore = t5DnnForward(dnn, probe->feat);
+      probe->cutPass = v.regressionRadius < 5.0f / (2.f * k2Rinv1GeVf) ? t5PassRPhiChi2(m, lm, v.chiSquared) : true;
+      probe->rzTight = tight;
+      return true;
+    }
     if (useDnn) {
       float feat[38];
       t5DnnFeatures(m, md, s, t, xs, ys, mdIdx, lm, innerT3, v.innerRadius, v.outerRadius, v.bridgeRadius, feat);
       float inference = t5DnnForward(dnn, feat);
-      if (!(inference > kT5DnnWP))
+      if (!(inference > dnnWP))
         return false;
-      tight = tight and (inference > kT5DnnWP);
+      tight = tight and (inference > dnnWP);
     } else {
       if (v.regressionRadius < 5.0f / (2.f * k2Rinv1GeVf)) {
         if (!t5PassRPhiChi2(m, lm, v.chiSquared))

@@ -105,6 +105,12 @@ EXPORTS = (
     "lst_event_launches",
     "lst_event_set_profiling",
     "lst_event_get_profile",
+    "lst_es_set_t5dnn_threshold",
+    "lst_batch_t5_probe",
+    "lst_t5dnn_forward",
+    "lst_t5dnn_scratch_floats",
+    "lst_t5dnn_backward",
+    "lst_t5dnn_last_error",
 )
 
 
@@ -240,6 +246,13 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_event_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
         lib.lst_event_set_profiling.argtypes = [vp, i32]
         lib.lst_event_get_profile.argtypes = [vp, ctypes.POINTER(KernelTime), i32, ctypes.POINTER(i32)]
+        lib.lst_es_set_t5dnn_threshold.argtypes = [vp, ctypes.c_float]
+        lib.lst_batch_t5_probe.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, vp, u32, ctypes.POINTER(u32)]
+        lib.lst_t5dnn_forward.argtypes = [vp, vp, i32, vp, vp, vp, vp]
+        lib.lst_t5dnn_scratch_floats.argtypes = [i32]
+        lib.lst_t5dnn_scratch_floats.restype = sz
+        lib.lst_t5dnn_backward.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp]
+        lib.lst_t5dnn_last_error.restype = ctypes.c_char_p
         _lib = lib
         return lib
 
@@ -305,6 +318,9 @@ class ES:
     @property
     def handle(self):
         return self._h
+
+    def set_t5dnn_threshold(self, wp: float):
+        _check(library().lst_es_set_t5dnn_threshold(self._h, float(wp)), "lst_es_set_t5dnn_threshold")
 
     def set_t5dnn_weights(self, w: np.ndarray):
         w = np.ascontiguousarray(w, dtype=np.float32).ravel()
