@@ -23,6 +23,9 @@ Reported:
                algorithmic bytes per launch over its CUDA-event duration
   cpu_baseline the reference CPU backend (oracle/_ref, reference compiler
                flags) on the host cores, one event per thread
+  t5_classifier  T5 efficiency and fake rate (truth-matched quintuplet
+               candidates at the classifier decision) and batched events/s for
+               the reference-weight DNN, the retrained DNN and cut-only
 
 --impl reference times only the reference CPU backend on this workload.
 """
@@ -305,6 +308,36 @@ def run_ours(args, rank, world, local, events):
     prof = eset.profile()
     eset.set_profiling(False)
 
+    # T5 selection methods in the loop: candidate-level truth-matched
+    # efficiency / fake rate at the classifier stage (the probe) and batched
+    # events/s, for the reference-weight DNN, the retrained DNN and cut-only
+    from tracklooper_b200 import t5dnn
+
+    probe = t5dnn.collect_candidates(es, events, batch=B, eset=eset)
+    w_new, wp_new = t5dnn.retrained_weights()
+    lab = probe["label"]
+    classifier = {"candidates": int(lab.size), "true": int(lab.sum()),
+                  "reference_dnn": t5dnn.metrics(probe["score"] > np.float32(t5dnn.REFERENCE_WP), lab),
+                  "retrained_dnn": t5dnn.metrics(t5dnn.scores(probe, w_new, local) > wp_new, lab),
+                  "cut_only": t5dnn.metrics(probe["cut"] != 0, lab)}
+    eset.upload_packed(0, blob, offsets)
+    k_m = max(2, args.steps // 2)
+    ms_ref, _, _ = timed(batched_step, k_m)
+    es.set_t5dnn_weights(w_new)
+    es.set_t5dnn_threshold(wp_new)
+    batched_step()
+    ms_new, _, _ = timed(batched_step, k_m)
+    es.set_t5dnn_weights(t5dnn.reference_weights())
+    es.set_t5dnn_threshold(t5dnn.REFERENCE_WP)
+    eset.set_t5_method(lst.T5_CUTS)
+    batched_step()
+    ms_cut, _, _ = timed(batched_step, k_m)
+    eset.set_t5_method(lst.T5_DNN)
+    for key, ms_ in (("reference_dnn", ms_ref), ("retrained_dnn", ms_new), ("cut_only", ms_cut)):
+        classifier[key]["events_per_s"] = B * world * k_m / (ms_ * 1e-3)
+    classifier["retrained_working_point"] = wp_new
+    classifier["level"] = "quintuplet candidates reaching the classifier decision, this step's events"
+
     tot = sum(v[1] for v in prof.values())
     top = sorted(prof.items(), key=lambda kv: -kv[1][1])
     agg = {
@@ -353,6 +386,7 @@ def run_ours(args, rank, world, local, events):
                 "mode": "batched C ABI from pinned host buffers (lst_batch_upload, lst_batch_run, lst_batch_get_output)"},
         "e2e_drop_in": {"value": events_all * n_dropin_e2e / (ms_de * 1e-3), "unit": "events/s",
                         "mode": "per-event C ABI from host arrays (add_hits, add_pixel_segments, stages, output)"},
+        "t5_classifier": classifier,
         "gpu_launches": launches_b,
         "clocks": clocks,
         "roofline": roofline,

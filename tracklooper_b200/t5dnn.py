@@ -116,6 +116,16 @@ def reference_weights() -> np.ndarray:
     return np.fromfile(lst.DNN_WEIGHTS, dtype="<f4")
 
 
+RETRAINED_WEIGHTS = lst.DNN_WEIGHTS.replace("t5dnn_reference.bin", "t5dnn_retrained.bin")
+
+
+def retrained_weights() -> tuple[np.ndarray, float]:
+    """The committed retrained weights and their working point."""
+    with open(RETRAINED_WEIGHTS.replace(".bin", ".json")) as f:
+        wp = float(json.load(f)["working_point"])
+    return np.fromfile(RETRAINED_WEIGHTS, dtype="<f4"), wp
+
+
 def random_weights(seed: int = 0) -> np.ndarray:
     """He-initialised weights, zero biases."""
     rng = np.random.default_rng(seed)
@@ -149,15 +159,18 @@ def truth_labels(hits: np.ndarray, hit_sim: np.ndarray) -> np.ndarray:
 
 
 # ------------------------------------------------------------ candidates
-def collect_candidates(es: lst.ES, inputs, batch: int = 32, capacity: int = 1 << 21):
+def collect_candidates(es: lst.ES, inputs, batch: int = 32, capacity: int = 1 << 21, eset: lst.EventSet = None):
     """Runs the chain up to the quintuplet stage on `inputs` and returns the
-    classifier-stage candidates: dict of features, reference score, cut-only
-    decision, rz tight flag, truth label and event index."""
+    classifier-stage candidates: dict of features, loaded weights' score,
+    cut-only decision, rz tight flag, truth label and event index.  Uses
+    `eset` if given (its hit capacity must hold the inputs)."""
     torch = _torch()
     lib = lst.library()
     dev = torch.device("cuda", es.device)
-    max_hits = max(i.n_hits for i in inputs) + 1024
-    eset = lst.EventSet(es, n_slots=min(batch, len(inputs)), max_hits=max_hits)
+    own = eset is None
+    if own:
+        max_hits = max(i.n_hits for i in inputs) + 1024
+        eset = lst.EventSet(es, n_slots=min(batch, len(inputs)), max_hits=max_hits)
     feat = torch.empty(capacity, 38, device=dev)
     score = torch.empty(capacity, device=dev)
     cut = torch.empty(capacity, dtype=torch.uint8, device=dev)
@@ -186,7 +199,8 @@ def collect_candidates(es: lst.ES, inputs, batch: int = 32, capacity: int = 1 <<
         parts.append({"feat": feat[:k].cpu().numpy().copy(), "score": score[:k].cpu().numpy().copy(),
                       "cut": cut[:k].cpu().numpy().copy(), "tight": tight[:k].cpu().numpy().copy(),
                       "label": lab, "event": e + b0})
-    eset.close()
+    if own:
+        eset.close()
     return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
 
 
