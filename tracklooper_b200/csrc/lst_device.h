@@ -57,6 +57,8 @@ namespace lst {
     unsigned int pixCandTotal;    // pT5 / pT3 candidates of the current pixel stage
     unsigned int pixPassCount;    // passing candidates found by kPixEval
     unsigned int pixFallback;     // the pixel stage overflowed the staging: walk instead
+    unsigned int t5DnnCount;      // candidates buffered for kT5Dnn
+    unsigned int pad[3];
   };
 
   // All device pointers of one event.
@@ -102,6 +104,10 @@ namespace lst {
     unsigned int* t5ModOff;     // per eligible module: first candidate of the event
     unsigned int* t5CandFlag;   // per candidate: 0 = fails, else 1 + slot of its values in t5PassValues
     T5Values* t5PassValues;     // selection values of passing candidates
+    float* t5DnnFeat;           // candidates at the classifier: features (38 each)
+    unsigned int* t5DnnCand;    //   candidate index
+    T5Values* t5DnnVals;        //   selection values so far
+    uint8_t* t5DnnTight;        //   rz-fit tight flag
     unsigned int* plsModPre;    // per pLS: candidate prefix over its connected modules (41 entries)
     unsigned int* plsCand;      // per pLS: candidates
     unsigned int* plsCandOff;   // per pLS: first candidate (nPLS + 1 entries)

@@ -402,6 +402,8 @@ namespace {
         LST_LAUNCH(lst::kT5Prefix, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v);
         LST_LAUNCH(lst::kT5ModScan, one, 1024, d, v);
         LST_LAUNCH(lst::kT5Eval, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v, useDnn);
+        if (useDnn)
+          LST_LAUNCH(lst::kT5Dnn, dim3(blocksFor(lst::kT5DnnCap, count, 128), count), 128, d, v);
         LST_LAUNCH(lst::kT5Walk, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v,
                    useDnn);
         LST_LAUNCH(lst::kT5Emit, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v, useDnn);
@@ -526,6 +528,7 @@ namespace {
         {"kT5Eval", (const void*)lst::kT5Eval},
         {"kT5Emit", (const void*)lst::kT5Emit},
         {"kT5Walk", (const void*)lst::kT5Walk},
+        {"kT5Dnn", (const void*)lst::kT5Dnn},
         {"kT5Probe", (const void*)lst::kT5Probe},
         {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
         {"kT5Ranges", (const void*)lst::kT5Ranges},

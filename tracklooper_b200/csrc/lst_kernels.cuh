@@ -325,7 +325,7 @@ namespace lst {
     }
   }
 
-  __global__ void kCreateMD(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(256, 2) kCreateMD(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const int wpb = blockDim.x >> 5;
     for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < es.nLowerModules; w += gridDim.x * wpb) {
@@ -728,6 +728,7 @@ namespace lst {
   // candidates than the flag buffer holds take the walk instead.
   constexpr unsigned int kT5CandCap = 1u << 21;  // candidates per event
   constexpr unsigned int kT5PassCap = 1u << 16;  // passing candidates per event whose values are kept
+  constexpr unsigned int kT5DnnCap = 1u << 14;   // candidates per event classified in kT5Dnn
 
   __device__ __forceinline__ unsigned int t5CandidatesOf(const EventView& ev, unsigned int innerT3) {
     const Triplets& t3 = ev.t3;
@@ -806,6 +807,7 @@ namespace lst {
       ev.sc->t5CandTotal = carry;
       ev.sc->t5CandOverflow = (carry > kT5CandCap || ev.forceWalk) ? 1u : 0u;
       ev.sc->t5PassCount = 0;
+      ev.sc->t5DnnCount = 0;
     }
   }
 
@@ -836,7 +838,26 @@ namespace lst {
                         ev.t3.lowerModuleIndices[3 * outerT3 + 2]};
       T5Values v;
       unsigned int flag = 0;
-      if (t5Select(es.m, ev.md, ev.ls, ev.t3, dnn.get(), useDnn, c_t5dnnWP, lm, innerT3, outerT3, v)) {
+      T5Stage st;
+      if (!t5SelectPre(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st)) {
+        ev.t5CandFlag[c] = 0;
+        continue;
+      }
+      if (useDnn) {
+        // The classifier runs in kT5Dnn over all candidates that reach it;
+        // without room in its buffer, it runs here.
+        const unsigned int k = atomicAdd(&ev.sc->t5DnnCount, 1u);
+        if (k < kT5DnnCap) {
+          t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius, v.outerRadius,
+                        v.bridgeRadius, ev.t5DnnFeat + size_t(k) * 38);
+          ev.t5DnnCand[k] = c;
+          ev.t5DnnVals[k] = v;
+          ev.t5DnnTight[k] = st.tight ? 1 : 0;
+          ev.t5CandFlag[c] = 0;
+          continue;
+        }
+      }
+      if (t5Classify(es.m, ev.md, ev.ls, ev.t3, dnn.get(), useDnn, c_t5dnnWP, lm, innerT3, v, st)) {
         // keep the values of a passing candidate (flag = slot + 1), or mark
         // it for re-evaluation (flag = kT5PassCap + 1) when the buffer is full
         const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
@@ -848,6 +869,64 @@ namespace lst {
         }
       }
       ev.t5CandFlag[c] = flag;
+    }
+  }
+
+  // The DNN decision for the candidates kT5Eval buffered: one thread per
+  // candidate with the weights in shared memory (same arithmetic as the
+  // in-line classifier), then the values stored with a selected candidate.
+  __global__ void __launch_bounds__(128) kT5Dnn(DeviceES es, const EventView* evs) {
+    __shared__ T5DnnWeights sW;
+    const EventView& ev = evs[blockIdx.y];
+    if (ev.sc->t5CandOverflow)
+      return;
+    {
+      const float* src = reinterpret_cast<const float*>(&c_t5dnn);
+      float* dst = reinterpret_cast<float*>(&sW);
+      for (int i = threadIdx.x; i < kT5DnnParams; i += blockDim.x)
+        dst[i] = src[i];
+    }
+    __syncthreads();
+    const unsigned int n = ev.sc->t5DnnCount < kT5DnnCap ? ev.sc->t5DnnCount : kT5DnnCap;
+    const int nE = *ev.rg.nEligibleT5Modules;
+    const unsigned int* off = ev.t5ModOff;
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+      float feat[38];
+#pragma unroll
+      for (int i = 0; i < 38; ++i)
+        feat[i] = ev.t5DnnFeat[size_t(k) * 38 + i];
+      const float inference = t5DnnForward(sW, feat);
+      if (!(inference > c_t5dnnWP))
+        continue;
+      const unsigned int c = ev.t5DnnCand[k];
+      T5Values v = ev.t5DnnVals[k];
+      int lo = 0, hi = nE;
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= c)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
+      unsigned int innerT3, outerT3;
+      t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
+      const Triplets& t3 = ev.t3;
+      uint16_t lm[5] = {lm1, t3.lowerModuleIndices[3 * innerT3 + 1], t3.lowerModuleIndices[3 * innerT3 + 2],
+                        t3.lowerModuleIndices[3 * outerT3 + 1], t3.lowerModuleIndices[3 * outerT3 + 2]};
+      const unsigned int* mi = ev.ls.mdIndices;
+      const unsigned int seg1 = t3.segmentIndices[2 * innerT3], seg2 = t3.segmentIndices[2 * innerT3 + 1];
+      const unsigned int seg3 = t3.segmentIndices[2 * outerT3], seg4 = t3.segmentIndices[2 * outerT3 + 1];
+      const unsigned int mdIdx[5] = {mi[2 * seg1], mi[2 * seg2], mi[2 * seg2 + 1], mi[2 * seg3 + 1], mi[2 * seg4 + 1]};
+      t5NonAnchor(es.m, ev.md, lm, mdIdx, v);
+      v.tightCutFlag = ev.t5DnnTight[k] != 0 and (inference > c_t5dnnWP);
+      const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
+      if (slot < kT5PassCap) {
+        ev.t5PassValues[slot] = v;
+        ev.t5CandFlag[c] = slot + 1;
+      } else {
+        ev.t5CandFlag[c] = kT5PassCap + 1;
+      }
     }
   }
 

@@ -1230,37 +1230,45 @@ namespace lst {
     bool tightCutFlag;
   };
 
-  // Full T5 selection for one (inner T3, outer T3) pair
+  // T5 selection for one (inner T3, outer T3) pair
   // (SDL/Quintuplet.h:2508-2984).  useDnn selects the DNN method
   // (USE_RZCHI2 + USE_T5_DNN) with working point dnnWP (the reference's is
   // kT5DnnWP), otherwise the cut-only method (USE_RZCHI2 + USE_RPHICHI2).
   // With a probe, stops at the classifier stage and fills it instead.
-  template <typename W>
-  LST_HD bool t5Select(const Modules& m,
-                       const MiniDoublets& md,
-                       const Segments& s,
-                       const Triplets& t,
-                       const W& dnn,
-                       bool useDnn,
-                       float dnnWP,
-                       const uint16_t* lm,
-                       unsigned int innerT3,
-                       unsigned int outerT3,
-                       T5Values& v,
-                       T5Probe* probe = nullptr) {
+  // State of a candidate at the classifier decision.
+  struct T5Stage {
+    unsigned int mdIdx[5];
+    float xs[5], ys[5];
+    bool tight;  // the rz fit's tight flag
+  };
+
+  // Every test before the classifier decision, and the circle regression.
+  LST_HD bool t5SelectPre(const Modules& m,
+                          const MiniDoublets& md,
+                          const Segments& s,
+                          const Triplets& t,
+                          const uint16_t* lm,
+                          unsigned int innerT3,
+                          unsigned int outerT3,
+                          T5Values& v,
+                          T5Stage& st) {
     unsigned int seg1 = t.segmentIndices[2 * innerT3];
     unsigned int seg2 = t.segmentIndices[2 * innerT3 + 1];
     unsigned int seg3 = t.segmentIndices[2 * outerT3];
     unsigned int seg4 = t.segmentIndices[2 * outerT3 + 1];
     if (s.mdIndices[2 * seg2 + 1] != s.mdIndices[2 * seg3])
       return false;
-    unsigned int mdIdx[5] = {s.mdIndices[2 * seg1],
+    unsigned int* mdIdx = st.mdIdx;
+    unsigned int mdIdxInit[5] = {s.mdIndices[2 * seg1],
                              s.mdIndices[2 * seg2],
                              s.mdIndices[2 * seg2 + 1],
                              s.mdIndices[2 * seg3 + 1],
                              s.mdIndices[2 * seg4 + 1]};
+    for (int i = 0; i < 5; ++i)
+      mdIdx[i] = mdIdxInit[i];
 
-    float xs[5], ys[5];
+    float* xs = st.xs;
+    float* ys = st.ys;
     for (int i = 0; i < 5; ++i) {
       xs[i] = md.anchorX[mdIdx[i]];
       ys[i] = md.anchorY[mdIdx[i]];
@@ -1337,30 +1345,15 @@ namespace lst {
     regressionSigmas(m, lm, delta1, delta2, slopes, isFlat, 5, true);
     v.regressionRadius =
         circleRegression(5, xs, ys, delta1, delta2, slopes, isFlat, v.regressionG, v.regressionF, sigmas, v.chiSquared);
+    st.tight = tight;
+    return true;
+  }
 
-    if (probe) {
-      // classifier-stage snapshot: stop before either method decides
-      t5DnnFeatures(m, md, s, t, xs, ys, mdIdx, lm, innerT3, v.innerRadius, v.outerRadius, v.bridgeRadius,
-                    probe->feat);
-      probe->dnnScore = t5DnnForward(dnn, probe->feat);
-      probe->cutPass = v.regressionRadius < 5.0f / (2.f * k2Rinv1GeVf) ? t5PassRPhiChi2(m, lm, v.chiSquared) : true;
-      probe->rzTight = tight;
-      return true;
-    }
-    if (useDnn) {
-      float feat[38];
-      t5DnnFeatures(m, md, s, t, xs, ys, mdIdx, lm, innerT3, v.innerRadius, v.outerRadius, v.bridgeRadius, feat);
-      float inference = t5DnnForward(dnn, feat);
-      if (!(inference > dnnWP))
-        return false;
-      tight = tight and (inference > dnnWP);
-    } else {
-      if (v.regressionRadius < 5.0f / (2.f * k2Rinv1GeVf)) {
-        if (!t5PassRPhiChi2(m, lm, v.chiSquared))
-          return false;
-      }
-    }
-
+  // The chi-squared of the non-anchor hits against the regression circle
+  // (SDL/Quintuplet.h:2960-2984), stored with a selected candidate.
+  LST_HD void t5NonAnchor(const Modules& m, const MiniDoublets& md, const uint16_t* lm, const unsigned int* mdIdx,
+                          T5Values& v) {
+    bool isFlat[5];
     float nonAnchorDelta1[5], nonAnchorDelta2[5], nonAnchorSlopes[5];
     float nonAnchorxs[5], nonAnchorys[5];
     for (int i = 0; i < 5; ++i) {
@@ -1378,8 +1371,72 @@ namespace lst {
                                        v.regressionG,
                                        v.regressionF,
                                        v.regressionRadius);
+  }
+
+  // The classifier decision: the DNN with working point dnnWP, or the
+  // cut-only method's r-phi chi-squared table.
+  template <typename W>
+  LST_HD bool t5Classify(const Modules& m,
+                         const MiniDoublets& md,
+                         const Segments& s,
+                         const Triplets& t,
+                         const W& dnn,
+                         bool useDnn,
+                         float dnnWP,
+                         const uint16_t* lm,
+                         unsigned int innerT3,
+                         T5Values& v,
+                         T5Stage& st) {
+    bool tight = st.tight;
+    if (useDnn) {
+      float feat[38];
+      t5DnnFeatures(m, md, s, t, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius, v.outerRadius, v.bridgeRadius,
+                    feat);
+      float inference = t5DnnForward(dnn, feat);
+      if (!(inference > dnnWP))
+        return false;
+      tight = tight and (inference > dnnWP);
+    } else {
+      if (v.regressionRadius < 5.0f / (2.f * k2Rinv1GeVf)) {
+        if (!t5PassRPhiChi2(m, lm, v.chiSquared))
+          return false;
+      }
+    }
+    t5NonAnchor(m, md, lm, st.mdIdx, v);
     v.tightCutFlag = tight;
     return true;
+  }
+
+  // Full T5 selection (SDL/Quintuplet.h:2508-2984).  useDnn selects the DNN
+  // method (USE_RZCHI2 + USE_T5_DNN) with working point dnnWP (the
+  // reference's is kT5DnnWP), otherwise the cut-only method (USE_RZCHI2 +
+  // USE_RPHICHI2).  With a probe, stops at the classifier stage and fills it
+  // instead.
+  template <typename W>
+  LST_HD bool t5Select(const Modules& m,
+                       const MiniDoublets& md,
+                       const Segments& s,
+                       const Triplets& t,
+                       const W& dnn,
+                       bool useDnn,
+                       float dnnWP,
+                       const uint16_t* lm,
+                       unsigned int innerT3,
+                       unsigned int outerT3,
+                       T5Values& v,
+                       T5Probe* probe = nullptr) {
+    T5Stage st;
+    if (!t5SelectPre(m, md, s, t, lm, innerT3, outerT3, v, st))
+      return false;
+    if (probe) {
+      t5DnnFeatures(m, md, s, t, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius, v.outerRadius, v.bridgeRadius,
+                    probe->feat);
+      probe->dnnScore = t5DnnForward(dnn, probe->feat);
+      probe->cutPass = v.regressionRadius < 5.0f / (2.f * k2Rinv1GeVf) ? t5PassRPhiChi2(m, lm, v.chiSquared) : true;
+      probe->rzTight = st.tight;
+      return true;
+    }
+    return t5Classify(m, md, s, t, dnn, useDnn, dnnWP, lm, innerT3, v, st);
   }
 
   // SDL/Quintuplet.h:150-216 with the eta/phi/pt/score formed in
