@@ -112,9 +112,9 @@ def test_probe_counts_match_selected_quintuplets(es, probe_event):
 
 
 def test_training_reduces_loss_and_beats_cut_only(es):
-    train = t5dnn.collect_candidates(es, t5dnn.generate(2, 5000, 48))
-    test = t5dnn.collect_candidates(es, t5dnn.generate(2, 6000, 16))
-    w, hist = t5dnn.train(train, epochs=25, batch=8192)
+    train = t5dnn.collect_candidates(es, t5dnn.generate(2, 5000, 128))
+    test = t5dnn.collect_candidates(es, t5dnn.generate(2, 6000, 32))
+    w, hist = t5dnn.train(train, epochs=30, batch=8192)
     assert hist[-1]["loss"] < hist[0]["loss"]
     cut_eff = t5dnn.metrics(train["cut"] != 0, train["label"])["efficiency"]
     wp = t5dnn.threshold_for_efficiency(t5dnn.scores(train, w), train["label"], cut_eff)

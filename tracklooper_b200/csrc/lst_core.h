@@ -251,6 +251,14 @@ namespace lst {
     float* outerHighEdgeY;
     float* outerLowEdgeX;
     float* outerLowEdgeY;
+    // Derived per mini-doublet from its anchor radius rt (not reference
+    // fields): slope = asin(min(rt k / ptCut, sinAlphaMax)), tanSlope =
+    // tan(slope), slope3 = asin(min(rt k / 3, sinAlphaMax)).  The cut
+    // algorithms evaluate exactly these expressions of a mini-doublet's rt
+    // many times over; stored once, they give the same values.
+    float* slope;
+    float* tanSlope;
+    float* slope3;
   };
 
   struct Segments {

@@ -6,6 +6,8 @@
 
 namespace lst {
 
+  struct TCCleanInfo;
+
   // Event setup resident on the device (read-only during an event).
   struct DeviceES {
     Modules m;
@@ -115,6 +117,7 @@ namespace lst {
     unsigned int* pixPassObj;   //   the T5 / T3 index
     unsigned int* pixPassPLS;   //   the pLS index
     float* pixPassV;            //   the selection values (8 per candidate)
+    struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
     unsigned int maxHits;

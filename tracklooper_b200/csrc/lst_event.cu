@@ -95,6 +95,9 @@ namespace {
 #define LST_CARVE_SCRATCH(field, type, count) v.field = c.take<type>(count);
     LST_SCRATCH_FIELDS(LST_CARVE_SCRATCH)
 #undef LST_CARVE_SCRATCH
+    v.md.slope = c.take<float>(MD);
+    v.md.tanSlope = c.take<float>(MD);
+    v.md.slope3 = c.take<float>(MD);
     v.sc = c.take<lst::EventScalars>(1);
   }
 
@@ -382,6 +385,7 @@ namespace {
       case LST_STAGE_MINI_DOUBLETS:
         LST_LAUNCH(lst::kCreateMD, warpGrid(nLower, 8, count), 256, d, v);
         LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kMDDerived, warpGrid(nLower + 1, 8, count), 256, d, v);
         break;
       case LST_STAGE_SEGMENTS:
         LST_LAUNCH(lst::kCreateLS, warpGrid(nLower, lst::kLSWarps, count), 32 * lst::kLSWarps, d, v);
@@ -454,7 +458,8 @@ namespace {
         LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
         LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, true);
         LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);
-        LST_LAUNCH(lst::kCrossCleanPLS, dim3(blocksFor(P, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kTCCleanInfo, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kCrossCleanPLS, dim3(blocksFor(P, count, lst::kCleanTile), count), lst::kCleanTile, d, v);
         LST_LAUNCH(lst::kAddPLSTC, one, 1024, d, v);
         break;
       }
@@ -515,6 +520,7 @@ namespace {
         {"kPixelIngest", (const void*)lst::kPixelIngest},
         {"kCreateMD", (const void*)lst::kCreateMD},
         {"kMDRanges", (const void*)lst::kMDRanges},
+        {"kMDDerived", (const void*)lst::kMDDerived},
         {"kCreateLS", (const void*)lst::kCreateLS},
         {"kLSRanges", (const void*)lst::kLSRanges},
         {"kT3Offsets", (const void*)lst::kT3Offsets},
@@ -560,6 +566,7 @@ namespace {
         {"kT5TCScan", (const void*)lst::kT5TCScan},
         {"kT5TCEmit", (const void*)lst::kT5TCEmit},
         {"kT5TCFinish", (const void*)lst::kT5TCFinish},
+        {"kTCCleanInfo", (const void*)lst::kTCCleanInfo},
         {"kCrossCleanPLS", (const void*)lst::kCrossCleanPLS},
         {"kAddPLSTC", (const void*)lst::kAddPLSTC},
         {"kCounts", (const void*)lst::kCounts},

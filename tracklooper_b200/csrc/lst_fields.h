@@ -247,5 +247,6 @@
   X(pixPassObj, unsigned int, lst::kPixPassCap)       \
   X(pixPassPLS, unsigned int, lst::kPixPassCap)       \
   X(pixPassV, float, 8 * lst::kPixPassCap)            \
+  X(tcCleanInfo, lst::TCCleanInfo, TC)                \
   X(plsOrder, unsigned int, P)                        \
-  X(plsBinStart, unsigned int, 128)
+  X(plsBinStart, unsigned int, lst::kPLSBins + 2)

@@ -334,6 +334,20 @@ namespace lst {
     }
   }
 
+  // Derived per-MD values for every stored MD (lower modules and the pixel
+  // module); one warp per module.
+  __global__ void kMDDerived(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const int wpb = blockDim.x >> 5;
+    MiniDoublets md = ev.md;
+    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w <= es.nLowerModules; w += gridDim.x * wpb) {
+      const unsigned int n = md.nMDs[w];
+      const unsigned int base = es.mdOffset[w];
+      for (unsigned int k = laneId(); k < n; k += 32)
+        storeMDDerived(md, base + k);
+    }
+  }
+
   // SDL/MiniDoublet.h:1084-1104
   __global__ void kMDRanges(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
@@ -1122,14 +1136,17 @@ namespace lst {
   // SDL/Kernels.h:384-473.  Pass 1 sets bit 1 of isDup directly; pass 2 marks
   // plsFlag and kMergePLSFlag folds it into bit 2 afterwards, so that pass 2
   // reads the pass-1 bit while other threads mark removals.
-  // pLS binned by eta: bins of width 0.1 over [-6, 6) (clamped at both ends)
+  // pLS binned by eta: bins of width 0.02 over [-6, 6) (clamped at both ends)
   // plus a last bin for non-finite eta, which must meet every pLS because a
-  // NaN never satisfies the reference's |deta| > 0.1 skip.
-  constexpr int kPLSBins = 120;
+  // NaN never satisfies the reference's |deta| > 0.1 skip.  Two etas within
+  // 0.1 of each other land at most kPLSBinReach bins apart (5 bin widths plus
+  // the rounding of the bin coordinate).
+  constexpr int kPLSBins = 600;
+  constexpr int kPLSBinReach = 6;
   LST_DEV int plsEtaBin(float eta) {
     if (!(fabsf(eta) <= 3.0e38f))
       return kPLSBins;
-    float t = (eta + 6.0f) * 10.0f;
+    float t = (eta + 6.0f) * 50.0f;
     if (t < 0.f)
       return 0;
     if (t >= float(kPLSBins))
@@ -1247,8 +1264,8 @@ namespace lst {
           plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
         continue;
       }
-      const int b0 = b >= 2 ? b - 2 : 0;
-      const int b1 = b + 2 < kPLSBins ? b + 2 : kPLSBins - 1;
+      const int b0 = b >= kPLSBinReach ? b - kPLSBinReach : 0;
+      const int b1 = b + kPLSBinReach < kPLSBins ? b + kPLSBinReach : kPLSBins - 1;
       for (unsigned int k = binStart[b0]; k < binStart[b1 + 1]; ++k) {
         unsigned int jx = order[k];
         if (jx > ix)
@@ -2154,16 +2171,24 @@ namespace lst {
     }
   }
 
-  // Shared pixel hits of two pLS, through their hit indices (SDL/TrackCandidate.h:165-202).
-  LST_DEV int sharedPixelHits(const Segments& s, const MiniDoublets& md, const Hits& h, unsigned int ix, unsigned int jx) {
-    int phits1[4] = {static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * ix]]]),
-                     static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * ix + 1]]]),
-                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * ix]]]),
-                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * ix + 1]]])};
-    int phits2[4] = {static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * jx]]]),
-                     static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * jx + 1]]]),
-                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * jx]]]),
-                     static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * jx + 1]]])};
+  // Per-TC record for the pLS cross-cleaning (SDL/TrackCandidate.h:302-381):
+  // the candidate's type, the (eta, phi) a pLS is compared with, and the
+  // four pixel hits of its pLS (pT3, pT5).
+  struct TCCleanInfo {
+    float eta, phi;
+    int type;
+    int hits[4];
+  };
+
+  LST_DEV void pixelHitsOf(const Segments& s, const MiniDoublets& md, const Hits& h, unsigned int plsIndex, int* out) {
+    out[0] = static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * plsIndex]]]);
+    out[1] = static_cast<int>(h.idxs[md.anchorHitIndices[s.mdIndices[2 * plsIndex + 1]]]);
+    out[2] = static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * plsIndex]]]);
+    out[3] = static_cast<int>(h.idxs[md.outerHitIndices[s.mdIndices[2 * plsIndex + 1]]]);
+  }
+
+  // Shared pixel hits of two pLS (SDL/TrackCandidate.h:165-202), -1 entries skipped.
+  LST_DEV int sharedPixelHits(const int* phits1, const int* phits2) {
     int npMatched = 0;
     for (int i = 0; i < 4; i++) {
       bool pmatched = false;
@@ -2183,47 +2208,80 @@ namespace lst {
     return npMatched;
   }
 
-  // pLS vs existing TCs (SDL/TrackCandidate.h:302-381).
-  __global__ void kCrossCleanPLS(DeviceES es, const EventView* evs) {
+  __global__ void kTCCleanInfo(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int nTC = *ev.tc.nTrackCandidates;
+    const unsigned int prefix = es.lsOffset[es.nLowerModules];
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < nTC; t += gridDim.x * blockDim.x) {
+      TCCleanInfo info;
+      info.type = ev.tc.trackCandidateType[t];
+      const unsigned int innerIdx = ev.tc.objectIndices[2 * t];
+      info.eta = 0.f;
+      info.phi = 0.f;
+      info.hits[0] = info.hits[1] = info.hits[2] = info.hits[3] = -1;
+      if (info.type == 4) {
+        info.eta = ev.t5.eta[innerIdx];
+        info.phi = ev.t5.phi[innerIdx];
+      } else if (info.type == 5) {
+        info.eta = ev.pt3.eta_pix[innerIdx];
+        info.phi = ev.pt3.phi_pix[innerIdx];
+        pixelHitsOf(ev.ls, ev.md, ev.hits, ev.pt3.pixelSegmentIndices[innerIdx], info.hits);
+      } else if (info.type == 7) {
+        info.eta = ev.ls.eta[innerIdx - prefix];
+        info.phi = ev.ls.phi[innerIdx - prefix];
+        pixelHitsOf(ev.ls, ev.md, ev.hits, innerIdx, info.hits);
+      }
+      ev.tcCleanInfo[t] = info;
+    }
+  }
+
+  // pLS vs existing TCs (SDL/TrackCandidate.h:302-381); the TC records are
+  // staged in shared memory 128 at a time.
+  constexpr int kCleanTile = 128;
+  __global__ void __launch_bounds__(kCleanTile) kCrossCleanPLS(DeviceES es, const EventView* evs) {
+    __shared__ TCCleanInfo sInfo[kCleanTile];
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nPix = ev.ls.nSegments[es.pixelModule];
     const unsigned int prefix = es.lsOffset[es.nLowerModules];
     const unsigned int nTC = *ev.tc.nTrackCandidates;
     Segments s = ev.ls;
-    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPix; i += gridDim.x * blockDim.x) {
-      if (!s.isQuad[i] || s.isDup[i])
-        continue;
-      float eta1 = s.eta[i], phi1 = s.phi[i];
+    for (unsigned int iBase = blockIdx.x * kCleanTile; iBase < nPix; iBase += gridDim.x * kCleanTile) {
+      const unsigned int i = iBase + threadIdx.x;
+      const bool active = i < nPix && s.isQuad[i] && !s.isDup[i];
+      int phits1[4] = {-1, -1, -1, -1};
+      float eta1 = 0.f, phi1 = 0.f;
+      if (active) {
+        pixelHitsOf(s, ev.md, ev.hits, prefix + i, phits1);
+        eta1 = s.eta[i];
+        phi1 = s.phi[i];
+      }
       bool dup = false;
-      for (unsigned int t = 0; t < nTC; t++) {
-        short type = ev.tc.trackCandidateType[t];
-        unsigned int innerIdx = ev.tc.objectIndices[2 * t];
-        if (type == 4) {
-          float dEta = fabs_(eta1 - ev.t5.eta[innerIdx]);
-          float dPhi = wrapDPhi(phi1, ev.t5.phi[innerIdx]);
-          if (dEta * dEta + dPhi * dPhi < 1e-3f)
-            dup = true;
-        }
-        if (type == 5) {
-          int pLSIndex = static_cast<int>(ev.pt3.pixelSegmentIndices[innerIdx]);
-          if (sharedPixelHits(s, ev.md, ev.hits, prefix + i, static_cast<unsigned int>(pLSIndex)) > 0)
-            dup = true;
-          float dEta = fabs_(eta1 - ev.pt3.eta_pix[innerIdx]);
-          float dPhi = wrapDPhi(phi1, ev.pt3.phi_pix[innerIdx]);
-          if (dEta * dEta + dPhi * dPhi < 0.000001f)
-            dup = true;
-        }
-        if (type == 7) {
-          unsigned int pLSIndex = innerIdx;
-          if (sharedPixelHits(s, ev.md, ev.hits, prefix + i, pLSIndex) > 0)
-            dup = true;
-          float dEta = fabs_(eta1 - s.eta[pLSIndex - prefix]);
-          float dPhi = wrapDPhi(phi1, s.phi[pLSIndex - prefix]);
-          if (dEta * dEta + dPhi * dPhi < 0.000001f)
-            dup = true;
+      for (unsigned int tBase = 0; tBase < nTC; tBase += kCleanTile) {
+        const unsigned int tile = (nTC - tBase < kCleanTile) ? nTC - tBase : kCleanTile;
+        __syncthreads();
+        if (threadIdx.x < tile)
+          sInfo[threadIdx.x] = ev.tcCleanInfo[tBase + threadIdx.x];
+        __syncthreads();
+        if (!active || dup)
+          continue;
+        for (unsigned int k = 0; k < tile; ++k) {
+          const TCCleanInfo& info = sInfo[k];
+          if (info.type == 4) {
+            float dEta = fabs_(eta1 - info.eta);
+            float dPhi = wrapDPhi(phi1, info.phi);
+            if (dEta * dEta + dPhi * dPhi < 1e-3f)
+              dup = true;
+          } else if (info.type == 5 || info.type == 7) {
+            if (sharedPixelHits(phits1, info.hits) > 0)
+              dup = true;
+            float dEta = fabs_(eta1 - info.eta);
+            float dPhi = wrapDPhi(phi1, info.phi);
+            if (dEta * dEta + dPhi * dPhi < 0.000001f)
+              dup = true;
+          }
         }
       }
-      if (dup)
+      if (active && dup)
         s.isDup[i] = 1;
     }
   }

@@ -89,9 +89,9 @@ namespace lst {
     float xOut = md.anchorX[outerMD], yOut = md.anchorY[outerMD], zOut = md.anchorZ[outerMD],
           rtOut = md.anchorRt[outerMD];
 
-    float sdSlope = fasin(fmin_(rtOut * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    float sdSlope = md.slope[outerMD];
     float sdPVoff = 0.1f / rtOut;
-    float dzDrtScale = ftan(sdSlope) / sdSlope;
+    float dzDrtScale = md.tanSlope[outerMD] / sdSlope;
     const float zGeom = m.layers[innerLM] <= 2 ? 2.f * kPixelPSZpitch : 2.f * kStrip2SZpitch;
     float zLo = zIn + (zIn - kDeltaZLum) * (rtOut / rtIn - 1.f) * (zIn > 0.f ? 1.f : dzDrtScale) - zGeom;
     float zHi = zIn + (zIn + kDeltaZLum) * (rtOut / rtIn - 1.f) * (zIn < 0.f ? 1.f : dzDrtScale) + zGeom;
@@ -132,7 +132,7 @@ namespace lst {
     float xOut = md.anchorX[outerMD], yOut = md.anchorY[outerMD], zOut = md.anchorZ[outerMD],
           rtOut = md.anchorRt[outerMD];
     bool outerLayerEndcapTwoS = (m.subdets[outerLM] == Endcap) && (m.moduleType[outerLM] == TwoS);
-    float sdSlope = fasin(fmin_(rtOut * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    float sdSlope = md.slope[outerMD];
     float disks2SMinRadius = 60.f;
     float rtGeom = ((rtIn < disks2SMinRadius && rtOut < disks2SMinRadius)
                         ? (2.f * kPixelPSZpitch)
@@ -142,7 +142,7 @@ namespace lst {
       return false;
     float dz = zOut - zIn;
     float dLum = signTransfer(kDeltaZLum, zIn);
-    float drtDzScale = sdSlope / ftan(sdSlope);
+    float drtDzScale = sdSlope / md.tanSlope[outerMD];
     float rtLo = fmax_(rtIn * (1.f + dz / (zIn + dLum) * drtDzScale) - rtGeom, rtIn - 0.5f * rtGeom);
     float rtHi = rtIn * (zOut - dLum) / (zIn - dLum) + rtGeom;
     if (!((rtOut >= rtLo) && (rtOut <= rtHi)))

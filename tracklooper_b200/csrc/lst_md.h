@@ -180,6 +180,15 @@ namespace lst {
     zn = abszn * ((zp > 0) ? 1 : -1);
   }
 
+  // The derived per-MD values of MiniDoublets (slope, tanSlope, slope3).
+  LST_HD void storeMDDerived(MiniDoublets& md, unsigned int idx) {
+    const float rt = md.anchorRt[idx];
+    const float slope = fasin(fmin_(rt * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    md.slope[idx] = slope;
+    md.tanSlope[idx] = ftan(slope);
+    md.slope3[idx] = fasin(fmin_(rt * k2Rinv1GeVf / 3.0f, kSinAlphaMax));
+  }
+
   struct MDValues {
     float dz, dphi, dphichange, shiftedX, shiftedY, shiftedZ, noShiftedDz, noShiftedDphi, noShiftedDphiChange;
   };

@@ -43,9 +43,9 @@ namespace lst {
     float px = s.px[pls], py = s.py[pls], pz = s.pz[pls];
     float etaErr = s.etaErr[pls];
 
-    float alpha1GeV_OutLo = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    float alpha1GeV_OutLo = md.slope[md3];
     const float rtRatio_OutLoInOut = rt_OutLo / rt_InOut;
-    float dzDrtScale = ftan(alpha1GeV_OutLo) / alpha1GeV_OutLo;
+    float dzDrtScale = md.tanSlope[md3] / alpha1GeV_OutLo;
     const float zpitch_InLo = 0.05f;
     const float zpitch_InOut = 0.05f;
     float zpitch_OutLo = (isPS_OutLo ? kPixelPSZpitch : kStrip2SZpitch);
@@ -136,8 +136,8 @@ namespace lst {
     betaOutRHmax *= betaOutMMSF;
 
     const float dBetaMuls = sdlThetaMulsF * 4.f / fmin_(fabs_(pt_beta), kPtBetaMax);
-    const float alphaInAbsReg = fmax_(fabs_(alpha_InLo), fasin(fmin_(rt_InUp * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
-    const float alphaOutAbsReg = fmax_(fabs_(alpha_OutLo), fasin(fmin_(rt_OutLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
+    const float alphaInAbsReg = fmax_(fabs_(alpha_InLo), md.slope3[md2]);
+    const float alphaOutAbsReg = fmax_(fabs_(alpha_OutLo), md.slope3[md3]);
     const float dBetaInLum = lIn < 11 ? 0.0f : fabs_(alphaInAbsReg * kDeltaZLum / z_InUp);
     const float dBetaOutLum = lOut < 11 ? 0.0f : fabs_(alphaOutAbsReg * kDeltaZLum / z_OutLo);
     const float dBetaLum2 = (dBetaInLum + dBetaOutLum) * (dBetaInLum + dBetaOutLum);
@@ -189,8 +189,8 @@ namespace lst {
     const float zpitch_InLo = 0.05f;
     float zpitch_OutLo = (isPS_OutLo ? kPixelPSZpitch : kStrip2SZpitch);
     float zGeom = zpitch_InLo + zpitch_OutLo;
-    const float sdlSlope = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
-    const float dzDrtScale = ftan(sdlSlope) / sdlSlope;
+    const float sdlSlope = md.slope[md3];
+    const float dzDrtScale = md.tanSlope[md3] / sdlSlope;
     const float dLum = signTransfer(kDeltaZLum, z_InUp);
     bool isOutSgInnerMDPS = m.moduleType[lmOI] == PS;
     const float rtGeom1 = isOutSgInnerMDPS ? kPixelPSZpitch : kStrip2SZpitch;
@@ -226,7 +226,7 @@ namespace lst {
     if (!((rt_OutLo >= rtLo_point) && (rt_OutLo <= rtHi_point)))
       return false;
 
-    const float alpha1GeV_OutLo = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    const float alpha1GeV_OutLo = md.slope[md3];
     const float sdlPVoff = 0.1f / rt_OutLo;
     float sdlCut = alpha1GeV_OutLo + fsqrt(sdlMuls * sdlMuls + sdlPVoff * sdlPVoff);
     float midPointX = 0.5f * (x_InLo + x_OutLo);
@@ -283,8 +283,8 @@ namespace lst {
     betaOutRHmax *= betaOutMMSF;
 
     const float dBetaMuls = sdlThetaMulsF * 4.f / fmin_(fabs_(pt_beta), kPtBetaMax);
-    const float alphaInAbsReg = fmax_(fabs_(alpha_InLo), fasin(fmin_(rt_InUp * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
-    const float alphaOutAbsReg = fmax_(fabs_(alpha_OutLo), fasin(fmin_(rt_OutLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
+    const float alphaInAbsReg = fmax_(fabs_(alpha_InLo), md.slope3[md2]);
+    const float alphaOutAbsReg = fmax_(fabs_(alpha_OutLo), md.slope3[md3]);
     const float dBetaInLum = lIn < 11 ? 0.0f : fabs_(alphaInAbsReg * kDeltaZLum / z_InUp);
     const float dBetaOutLum = lOut < 11 ? 0.0f : fabs_(alphaOutAbsReg * kDeltaZLum / z_OutLo);
     const float dBetaLum2 = (dBetaInLum + dBetaOutLum) * (dBetaInLum + dBetaOutLum);

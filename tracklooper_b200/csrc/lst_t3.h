@@ -72,9 +72,9 @@ namespace lst {
     bool isPSOut = (m.moduleType[lm3] == PS);
     float rtIn = md.anchorRt[md1], rtMid = md.anchorRt[md2], rtOut = md.anchorRt[md3];
     float zIn = md.anchorZ[md1], zMid = md.anchorZ[md2], zOut = md.anchorZ[md3];
-    float alpha1GeVOut = fasin(fmin_(rtOut * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    float alpha1GeVOut = md.slope[md3];
     float rtRatio_OutIn = rtOut / rtIn;
-    float dzDrtScale = ftan(alpha1GeVOut) / alpha1GeVOut;
+    float dzDrtScale = md.tanSlope[md3] / alpha1GeVOut;
     float zpitchIn = (isPSIn ? kPixelPSZpitch : kStrip2SZpitch);
     float zpitchOut = (isPSOut ? kPixelPSZpitch : kStrip2SZpitch);
     const float zHi =
@@ -126,8 +126,8 @@ namespace lst {
     bool isPSOut = (m.moduleType[lm3] == PS);
     float rtIn = md.anchorRt[md1], rtMid = md.anchorRt[md2], rtOut = md.anchorRt[md3];
     float zIn = md.anchorZ[md1], zMid = md.anchorZ[md2], zOut = md.anchorZ[md3];
-    float alpha1GeV_OutLo = fasin(fmin_(rtOut * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
-    float dzDrtScale = ftan(alpha1GeV_OutLo) / alpha1GeV_OutLo;
+    float alpha1GeV_OutLo = md.slope[md3];
+    float dzDrtScale = md.tanSlope[md3] / alpha1GeV_OutLo;
     float zpitchIn = (isPSIn ? kPixelPSZpitch : kStrip2SZpitch);
     float zpitchOut = (isPSOut ? kPixelPSZpitch : kStrip2SZpitch);
     float zGeom = zpitchIn + zpitchOut;
@@ -198,8 +198,8 @@ namespace lst {
                             float& betaIn) {
     float rtIn = md.anchorRt[md1], rtMid = md.anchorRt[md2], rtOut = md.anchorRt[md3];
     float zIn = md.anchorZ[md1], zMid = md.anchorZ[md2], zOut = md.anchorZ[md3];
-    float alpha1GeV_Out = fasin(fmin_(rtOut * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
-    float dzDrtScale = ftan(alpha1GeV_Out) / alpha1GeV_Out;
+    float alpha1GeV_Out = md.slope[md3];
+    float dzDrtScale = md.tanSlope[md3] / alpha1GeV_Out;
     if (!(zIn * zOut > 0))
       return false;
     float dLum = signTransfer(kDeltaZLum, zIn);

@@ -89,9 +89,9 @@ namespace lst {
     bool isPS_OutLo = (m.moduleType[q.lmOI] == PS);
     float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
     float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
-    float alpha1GeV_OutLo = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    float alpha1GeV_OutLo = md.slope[q.md3];
     float rtRatio_OutLoInLo = rt_OutLo / rt_InLo;
-    float dzDrtScale = ftan(alpha1GeV_OutLo) / alpha1GeV_OutLo;
+    float dzDrtScale = md.tanSlope[q.md3] / alpha1GeV_OutLo;
     float zpitch_InLo = (isPS_InLo ? kPixelPSZpitch : kStrip2SZpitch);
     float zpitch_OutLo = (isPS_OutLo ? kPixelPSZpitch : kStrip2SZpitch);
     float zHi = z_InLo + (z_InLo + kDeltaZLum) * (rtRatio_OutLoInLo - 1.f) * (z_InLo < 0.f ? 1.f : dzDrtScale) +
@@ -188,10 +188,8 @@ namespace lst {
     betaOutRHmax *= betaOutMMSF;
 
     const float dBetaMuls = sdlThetaMulsF * 4.f / fmin_(fabs_(pt_beta), kPtBetaMax);
-    const float alphaInAbsReg =
-        fmax_(fabs_(alpha_InLo), fasin(fmin_(rt_InLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
-    const float alphaOutAbsReg =
-        fmax_(fabs_(alpha_OutLo), fasin(fmin_(rt_OutLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
+    const float alphaInAbsReg = fmax_(fabs_(alpha_InLo), md.slope3[q.md1]);
+    const float alphaOutAbsReg = fmax_(fabs_(alpha_OutLo), md.slope3[q.md3]);
     const float dBetaInLum = lIn < 11 ? 0.0f : fabs_(alphaInAbsReg * kDeltaZLum / z_InLo);
     const float dBetaOutLum = lOut < 11 ? 0.0f : fabs_(alphaOutAbsReg * kDeltaZLum / z_OutLo);
     const float dBetaLum2 = (dBetaInLum + dBetaOutLum) * (dBetaInLum + dBetaOutLum);
@@ -222,8 +220,8 @@ namespace lst {
     bool isPS_OutLo = (m.moduleType[q.lmOI] == PS);
     float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
     float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
-    float alpha1GeV_OutLo = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
-    float dzDrtScale = ftan(alpha1GeV_OutLo) / alpha1GeV_OutLo;
+    float alpha1GeV_OutLo = md.slope[q.md3];
+    float dzDrtScale = md.tanSlope[q.md3] / alpha1GeV_OutLo;
     float zpitch_InLo = (isPS_InLo ? kPixelPSZpitch : kStrip2SZpitch);
     float zpitch_OutLo = (isPS_OutLo ? kPixelPSZpitch : kStrip2SZpitch);
     float zGeom = zpitch_InLo + zpitch_OutLo;
@@ -337,8 +335,8 @@ namespace lst {
     betaOutRHmax *= betaOutMMSF;
 
     const float dBetaMuls = sdlThetaMulsF * 4.f / fmin_(fabs_(pt_beta), kPtBetaMax);
-    const float alphaInAbsReg = fmax_(fabs_(sdIn_alpha), fasin(fmin_(rt_InLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
-    const float alphaOutAbsReg = fmax_(fabs_(sdOut_alpha), fasin(fmin_(rt_OutLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
+    const float alphaInAbsReg = fmax_(fabs_(sdIn_alpha), md.slope3[q.md1]);
+    const float alphaOutAbsReg = fmax_(fabs_(sdOut_alpha), md.slope3[q.md3]);
     const float dBetaInLum = lIn < 11 ? 0.0f : fabs_(alphaInAbsReg * kDeltaZLum / z_InLo);
     const float dBetaOutLum = lOut < 11 ? 0.0f : fabs_(alphaOutAbsReg * kDeltaZLum / z_OutLo);
     const float dBetaLum2 = (dBetaInLum + dBetaOutLum) * (dBetaInLum + dBetaOutLum);
@@ -366,8 +364,8 @@ namespace lst {
   LST_HD_BIG bool t4EEEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
     float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
     float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
-    float alpha1GeV_OutLo = fasin(fmin_(rt_OutLo * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
-    float dzDrtScale = ftan(alpha1GeV_OutLo) / alpha1GeV_OutLo;
+    float alpha1GeV_OutLo = md.slope[q.md3];
+    float dzDrtScale = md.tanSlope[q.md3] / alpha1GeV_OutLo;
     if (!((z_InLo * z_OutLo) > 0))
       return false;
     float dLum = signTransfer(kDeltaZLum, z_InLo);
@@ -474,8 +472,8 @@ namespace lst {
     betaOutRHmax *= betaOutMMSF;
 
     const float dBetaMuls = sdlThetaMulsF * 4.f / fmin_(fabs_(pt_beta), kPtBetaMax);
-    const float alphaInAbsReg = fmax_(fabs_(sdIn_alpha), fasin(fmin_(rt_InLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
-    const float alphaOutAbsReg = fmax_(fabs_(sdOut_alpha), fasin(fmin_(rt_OutLo * k2Rinv1GeVf / 3.0f, kSinAlphaMax)));
+    const float alphaInAbsReg = fmax_(fabs_(sdIn_alpha), md.slope3[q.md1]);
+    const float alphaOutAbsReg = fmax_(fabs_(sdOut_alpha), md.slope3[q.md3]);
     const float dBetaInLum = lIn < 11 ? 0.0f : fabs_(alphaInAbsReg * kDeltaZLum / z_InLo);
     const float dBetaOutLum = lOut < 11 ? 0.0f : fabs_(alphaOutAbsReg * kDeltaZLum / z_OutLo);
     const float dBetaLum2 = (dBetaInLum + dBetaOutLum) * (dBetaInLum + dBetaOutLum);

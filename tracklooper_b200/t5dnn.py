@@ -201,7 +201,12 @@ def collect_candidates(es: lst.ES, inputs, batch: int = 32, capacity: int = 1 <<
                       "label": lab, "event": e + b0})
     if own:
         eset.close()
-    return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+    data = {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+    # the probe appends in no fixed order: sort by (event, features) so that the
+    # data set, and with it training, is reproducible
+    keys = [data["feat"][:, k] for k in range(37, -1, -1)] + [data["event"]]
+    order = np.lexsort(keys)
+    return {k: v[order] for k, v in data.items()}
 
 
 def generate(config: int, first: int, n: int, workers: int = 16):
