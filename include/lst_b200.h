@@ -231,8 +231,9 @@ size_t lst_packed_size(uint32_t n_hits, uint32_t n_pls);
 int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
                      const uint64_t* blob_offsets);
 /* Repeats the unpacking of the last uploaded inputs of slots [first,
- * first + count) (as lst_batch_upload without the host-to-device copy), for
- * re-running events whose inputs are already resident on the device. */
+ * first + count) (as lst_batch_upload or lst_batch_upload_seeds without the
+ * host-to-device copy), for re-running events whose inputs are already
+ * resident on the device.  The slots must lie inside the last upload. */
 int lst_batch_ingest(lst_event* ev, int first, int count);
 /* Runs stages [first_stage, last_stage] for slots [first, first + count). */
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage);
@@ -243,6 +244,60 @@ int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last
 int lst_batch_run_graph(lst_event* ev, int first, int count, int first_stage, int last_stage);
 /* Copies the counts of slots [first, first + count) into out[count]. */
 int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out);
+
+/* ---------------------------------------------- CMSSW inputs (LST::run) */
+/* The inputs of LST::run / LST::prepareInput (SDL/LST.h:32-52,
+ * SDL/LST.cc:12-32,175-194): per pixel seed its momentum at the point of
+ * closest approach (see_px/py/pz), impact parameters (see_dxy, see_dz),
+ * errors (see_ptErr, see_etaErr), position and momentum at its last hit
+ * (see_stateTrajGlb*), charge (see_q) and pixel-hit indices; the outer-tracker
+ * hits as ph2_detId/x/y/z.  see_hitIdx, a vector<vector<int>> in the
+ * reference, is flattened: seed i's indices are see_hitIdx[see_hitIdx_offsets[i]
+ * .. see_hitIdx_offsets[i + 1]) with see_hitIdx_offsets[0] = 0 (n_seeds + 1
+ * entries).  Kept seeds need at least three indices (the reference reads three
+ * of every kept seed); a kept seed with fewer is dropped and the slot gets
+ * LST_STATUS_INVALID_INPUT. */
+typedef struct lst_seed_input {
+  uint32_t n_seeds;
+  const float* see_px;
+  const float* see_py;
+  const float* see_pz;
+  const float* see_dxy;
+  const float* see_dz;
+  const float* see_ptErr;
+  const float* see_etaErr;
+  const float* see_stateTrajGlbX;
+  const float* see_stateTrajGlbY;
+  const float* see_stateTrajGlbZ;
+  const float* see_stateTrajGlbPx;
+  const float* see_stateTrajGlbPy;
+  const float* see_stateTrajGlbPz;
+  const int32_t* see_q;
+  const uint32_t* see_hitIdx_offsets;
+  const int32_t* see_hitIdx;
+  uint32_t n_ph2;
+  const uint32_t* ph2_detId;
+  const float* ph2_x;
+  const float* ph2_y;
+  const float* ph2_z;
+} lst_seed_input;
+
+/* Packed form of one event's lst_seed_input for lst_batch_upload_seeds:
+ * lst_seed_packed_size bytes (a multiple of 16); lst_seed_pack writes it into
+ * host memory `dst` of `capacity` bytes (-1 if it does not fit or an array is
+ * missing; the offsets are checked to ascend). */
+size_t lst_seed_packed_size(uint32_t n_ph2, uint32_t n_seeds, uint32_t n_seed_hits);
+int lst_seed_pack(const lst_seed_input* in, void* dst, size_t capacity);
+/* As lst_batch_upload for packed seed events: one host-to-device copy, then
+ * on the device the seed conversion of LST::prepareInput (SDL/LST.cc:175-365,
+ * including its phi(r3LH - p3LH) "deltaPhi" of :265) followed by
+ * addHitToEvent + addPixelSegmentToEvent, for slots [first, first + count). */
+int lst_batch_upload_seeds(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                           const uint64_t* blob_offsets);
+/* LST::prepareInput + addHitToEvent + addPixelSegmentToEvent for one slot
+ * (SDL/LST.cc:33-72): the outer-tracker hits, then per kept seed (pT above
+ * 0.8 - 2 ptErr) three or four pseudo-hits and one pixel line segment. */
+int lst_event_prepare_input(lst_event* ev, int slot, const lst_seed_input* in);
 
 /* Track-candidate output of LST::getOutput (SDL/LST.cc:367-427) for slots
  * [first, first + count), flattened over the events: candidate k of the batch
@@ -263,6 +318,13 @@ typedef struct lst_output {
   uint64_t* event_hit_offsets;
 } lst_output;
 int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out);
+
+/* LST::run (SDL/LST.cc:12-161) on one slot: lst_event_prepare_input, all
+ * eight stages, then, if `out` is not NULL, the output accessors hits(),
+ * len(), seedIdx(), trackCandidateType() (SDL/LST.h:53-56) as
+ * lst_batch_get_output with count = 1.  The slot keeps its objects until it
+ * is reset or refilled (the reference discards its Event at the end of run). */
+int lst_run(lst_event* ev, int slot, const lst_seed_input* in, lst_output* out);
 
 /* lst_batch_get_output without any device allocation (no reference
  * counterpart: the reference allocates its host copies in getOutput).

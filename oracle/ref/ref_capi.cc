@@ -28,6 +28,7 @@
 // declarations see the access-specifier override below.
 #define private public
 #include "Event.h"
+#include "LST.h"
 #undef private
 
 namespace {
@@ -467,6 +468,145 @@ int lstref_event_run_stage(void* ev, int stage) {
     default:
       return -1;
   }
+}
+
+// ---------------------------------------------------------------- SDL::LST
+// The CMSSW entry point (SDL/LST.h:25-111).  Seeds come as 13 float arrays in
+// LST::run's argument order (see_px .. see_stateTrajGlbPz), see_q, and
+// see_hitIdx flattened as offsets (n_seeds + 1) plus values.
+namespace {
+  struct RefLSTRun {
+    SDL::LST<SDL::Acc> lst;
+    std::vector<unsigned int> flatHits;  // out_tc_hitIdxs_ concatenated
+  };
+
+  struct SeedVectors {
+    std::vector<float> f[13];
+    std::vector<int> q;
+    std::vector<std::vector<int>> hitIdx;
+    std::vector<unsigned int> detId;
+    std::vector<float> x, y, z;
+  };
+
+  SeedVectors seedVectors(unsigned int nSeeds,
+                          const float* const* f13,
+                          const int* q,
+                          const unsigned int* hitOff,
+                          const int* hitIdx,
+                          unsigned int nPh2,
+                          const unsigned int* detId,
+                          const float* x,
+                          const float* y,
+                          const float* z) {
+    SeedVectors v;
+    for (int k = 0; k < 13; ++k)
+      v.f[k].assign(f13[k], f13[k] + nSeeds);
+    v.q.assign(q, q + nSeeds);
+    v.hitIdx.resize(nSeeds);
+    for (unsigned int i = 0; i < nSeeds; ++i)
+      v.hitIdx[i].assign(hitIdx + hitOff[i], hitIdx + hitOff[i + 1]);
+    v.detId.assign(detId, detId + nPh2);
+    v.x.assign(x, x + nPh2);
+    v.y.assign(y, y + nPh2);
+    v.z.assign(z, z + nPh2);
+    return v;
+  }
+}  // namespace
+
+void* lstref_lst_create() { return new RefLSTRun(); }
+
+void lstref_lst_destroy(void* l) { delete static_cast<RefLSTRun*>(l); }
+
+// LST::prepareInput (SDL/LST.cc:175-365) alone; its results are read with
+// lstref_lst_array ("in_trkX_", "in_hitIndices_vec0_", ...).
+void lstref_lst_prepare(void* l,
+                        unsigned int nSeeds,
+                        const float* const* f13,
+                        const int* q,
+                        const unsigned int* hitOff,
+                        const int* hitIdx,
+                        unsigned int nPh2,
+                        const unsigned int* detId,
+                        const float* x,
+                        const float* y,
+                        const float* z) {
+  auto v = seedVectors(nSeeds, f13, q, hitOff, hitIdx, nPh2, detId, x, y, z);
+  static_cast<RefLSTRun*>(l)->lst.prepareInput(v.f[0], v.f[1], v.f[2], v.f[3], v.f[4], v.f[5], v.f[6], v.f[7],
+                                               v.f[8], v.f[9], v.f[10], v.f[11], v.f[12], v.q, v.hitIdx, v.detId,
+                                               v.x, v.y, v.z);
+}
+
+// LST::run (SDL/LST.cc:12-161): conversion, the whole chain on a fresh Event
+// and getOutput; the outputs are read with lstref_lst_array ("out_tc_len_",
+// "out_tc_seedIdx_", "out_tc_trackCandidateType_", and "out_tc_hitIdxs_" as
+// the per-candidate lists concatenated).
+void lstref_lst_run(void* l,
+                    void* es,
+                    unsigned int nSeeds,
+                    const float* const* f13,
+                    const int* q,
+                    const unsigned int* hitOff,
+                    const int* hitIdx,
+                    unsigned int nPh2,
+                    const unsigned int* detId,
+                    const float* x,
+                    const float* y,
+                    const float* z) {
+  auto* r = static_cast<RefLSTRun*>(l);
+  auto v = seedVectors(nSeeds, f13, q, hitOff, hitIdx, nPh2, detId, x, y, z);
+  SDL::QueueAcc queue(SDL::Dev{});
+  r->lst.run(queue, false, static_cast<RefES*>(es)->dev.get(), v.f[0], v.f[1], v.f[2], v.f[3], v.f[4], v.f[5],
+             v.f[6], v.f[7], v.f[8], v.f[9], v.f[10], v.f[11], v.f[12], v.q, v.hitIdx, v.detId, v.x, v.y, v.z);
+  r->flatHits.clear();
+  for (auto const& h : r->lst.out_tc_hitIdxs_)
+    r->flatHits.insert(r->flatHits.end(), h.begin(), h.end());
+}
+
+const void* lstref_lst_array(void* l, const char* name, long long* n, int* elem_size) {
+  auto* r = static_cast<RefLSTRun*>(l);
+  auto& L = r->lst;
+  std::string key(name);
+  const void* ptr = nullptr;
+  auto take = [&](auto const& vec) {
+    ptr = vec.data();
+    *n = static_cast<long long>(vec.size());
+    *elem_size = static_cast<int>(sizeof(vec[0]));
+  };
+  *n = 0;
+  *elem_size = 0;
+#define LSTREF_V(member) \
+  if (key == #member)    \
+    take(L.member);
+  LSTREF_V(in_trkX_)
+  LSTREF_V(in_trkY_)
+  LSTREF_V(in_trkZ_)
+  LSTREF_V(in_hitId_)
+  LSTREF_V(in_hitIdxs_)
+  LSTREF_V(in_hitIndices_vec0_)
+  LSTREF_V(in_hitIndices_vec1_)
+  LSTREF_V(in_hitIndices_vec2_)
+  LSTREF_V(in_hitIndices_vec3_)
+  LSTREF_V(in_deltaPhi_vec_)
+  LSTREF_V(in_ptIn_vec_)
+  LSTREF_V(in_ptErr_vec_)
+  LSTREF_V(in_px_vec_)
+  LSTREF_V(in_py_vec_)
+  LSTREF_V(in_pz_vec_)
+  LSTREF_V(in_eta_vec_)
+  LSTREF_V(in_etaErr_vec_)
+  LSTREF_V(in_phi_vec_)
+  LSTREF_V(in_charge_vec_)
+  LSTREF_V(in_seedIdx_vec_)
+  LSTREF_V(in_superbin_vec_)
+  LSTREF_V(in_pixelType_vec_)
+  LSTREF_V(in_isQuad_vec_)
+  LSTREF_V(out_tc_len_)
+  LSTREF_V(out_tc_seedIdx_)
+  LSTREF_V(out_tc_trackCandidateType_)
+#undef LSTREF_V
+  if (key == "out_tc_hitIdxs_")
+    take(r->flatHits);
+  return ptr;
 }
 
 // Returns a pointer to the named internal array (e.g. "md.anchorHitIndices"),

@@ -65,6 +65,13 @@ class RefLST:
         lib.lstref_event_run_stage.argtypes = [vp, ctypes.c_int]
         lib.lstref_event_field.restype = vp
         lib.lstref_event_field.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
+        seed_args = [ctypes.c_uint, ctypes.POINTER(vp), vp, vp, vp, ctypes.c_uint, vp, vp, vp, vp]
+        lib.lstref_lst_create.restype = vp
+        lib.lstref_lst_destroy.argtypes = [vp]
+        lib.lstref_lst_prepare.argtypes = [vp] + seed_args
+        lib.lstref_lst_run.argtypes = [vp, vp] + seed_args
+        lib.lstref_lst_array.restype = vp
+        lib.lstref_lst_array.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
         self.lib = lib
         geometry.geometry_dir()
         self.es = lib.lstref_es_load((es_base or geometry.ES_BASE).encode())
@@ -151,3 +158,121 @@ class RefLST:
         buf = (ctypes.c_char * (n.value * sz.value)).from_address(ptr)
         arr = np.frombuffer(buf, dtype=dtype, count=count)
         return arr.copy() if copy else arr
+
+    # ------------------------------------------------------------- SDL::LST
+    def _seed_args(self, seeds, keep):
+        from tracklooper_b200.gen import SEED_FLOAT_FIELDS
+
+        def p(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a.ctypes.data
+
+        f13 = (ctypes.c_void_p * 13)(*[p(seeds.see[k], np.float32) for k in SEED_FLOAT_FIELDS])
+        keep.append(f13)
+        return [
+            seeds.n_seeds,
+            f13,
+            p(seeds.see["see_q"], np.int32),
+            p(seeds.hit_offsets, np.uint32),
+            p(seeds.hit_idx, np.int32),
+            seeds.n_ph2,
+            p(seeds.ph2_detId, np.uint32),
+            p(seeds.ph2_x, np.float32),
+            p(seeds.ph2_y, np.float32),
+            p(seeds.ph2_z, np.float32),
+        ]
+
+    def _lst_arrays(self, handle, names):
+        out = {}
+        for name in names:
+            n, sz = ctypes.c_longlong(), ctypes.c_int()
+            ptr = self.lib.lstref_lst_array(handle, name.encode(), ctypes.byref(n), ctypes.byref(sz))
+            dt = _LST_ARRAY_DTYPES[name]
+            if not ptr or n.value == 0:
+                out[name] = np.zeros(0, dt)
+                continue
+            buf = (ctypes.c_char * (n.value * sz.value)).from_address(ptr)
+            out[name] = np.frombuffer(buf, dtype=dt, count=n.value).copy()
+        return out
+
+    def prepare_input(self, seeds) -> dict:
+        """LST::prepareInput (SDL/LST.cc:175-365) on CMSSW-layout seeds; returns
+        its 23 ``in_*_`` vectors by member name."""
+        keep = []
+        h = self.lib.lstref_lst_create()
+        try:
+            self.lib.lstref_lst_prepare(h, *self._seed_args(seeds, keep))
+            return self._lst_arrays(h, [k for k in _LST_ARRAY_DTYPES if k.startswith("in_")])
+        finally:
+            self.lib.lstref_lst_destroy(h)
+
+    def run_lst(self, seeds) -> dict:
+        """LST::run (SDL/LST.cc:12-161) then its output accessors: returns
+        ``hits`` (all candidates' hit indices concatenated), ``len``,
+        ``seedIdx`` and ``trackCandidateType``."""
+        keep = []
+        h = self.lib.lstref_lst_create()
+        try:
+            self.lib.lstref_lst_run(h, self.es, *self._seed_args(seeds, keep))
+            a = self._lst_arrays(h, [k for k in _LST_ARRAY_DTYPES if k.startswith("out_")])
+        finally:
+            self.lib.lstref_lst_destroy(h)
+        return {
+            "hits": a["out_tc_hitIdxs_"],
+            "len": a["out_tc_len_"],
+            "seedIdx": a["out_tc_seedIdx_"],
+            "trackCandidateType": a["out_tc_trackCandidateType_"],
+        }
+
+
+def prepared_event_input(prep: dict):
+    """The outputs of LST::prepareInput (RefLST.prepare_input) as an
+    EventInput, i.e. the arguments LST::run passes to addHitToEvent and
+    addPixelSegmentToEvent (SDL/LST.cc:53-72)."""
+    from tracklooper_b200.gen import EventInput
+
+    names = {
+        "hitIndices0": "in_hitIndices_vec0_", "hitIndices1": "in_hitIndices_vec1_",
+        "hitIndices2": "in_hitIndices_vec2_", "hitIndices3": "in_hitIndices_vec3_",
+        "dPhiChange": "in_deltaPhi_vec_", "ptIn": "in_ptIn_vec_", "ptErr": "in_ptErr_vec_", "px": "in_px_vec_",
+        "py": "in_py_vec_", "pz": "in_pz_vec_", "eta": "in_eta_vec_", "etaErr": "in_etaErr_vec_",
+        "phi": "in_phi_vec_", "charge": "in_charge_vec_", "seedIdx": "in_seedIdx_vec_",
+        "superbin": "in_superbin_vec_", "pixelType": "in_pixelType_vec_", "isQuad": "in_isQuad_vec_",
+    }
+    pls = {k: prep[v] for k, v in names.items()}
+    n = prep["in_trkX_"].size
+    return EventInput(prep["in_trkX_"], prep["in_trkY_"], prep["in_trkZ_"], prep["in_hitId_"], prep["in_hitIdxs_"],
+                      pls, np.full(n, -1, np.int32), np.full(pls["ptIn"].size, -1, np.int32),
+                      int(np.sum(prep["in_hitId_"] != 1)), np.zeros((0, 7)))
+
+
+_LST_ARRAY_DTYPES = {
+    "in_trkX_": np.float32,
+    "in_trkY_": np.float32,
+    "in_trkZ_": np.float32,
+    "in_hitId_": np.uint32,
+    "in_hitIdxs_": np.uint32,
+    "in_hitIndices_vec0_": np.uint32,
+    "in_hitIndices_vec1_": np.uint32,
+    "in_hitIndices_vec2_": np.uint32,
+    "in_hitIndices_vec3_": np.uint32,
+    "in_deltaPhi_vec_": np.float32,
+    "in_ptIn_vec_": np.float32,
+    "in_ptErr_vec_": np.float32,
+    "in_px_vec_": np.float32,
+    "in_py_vec_": np.float32,
+    "in_pz_vec_": np.float32,
+    "in_eta_vec_": np.float32,
+    "in_etaErr_vec_": np.float32,
+    "in_phi_vec_": np.float32,
+    "in_charge_vec_": np.int32,
+    "in_seedIdx_vec_": np.uint32,
+    "in_superbin_vec_": np.int32,
+    "in_pixelType_vec_": np.int8,
+    "in_isQuad_vec_": np.int8,
+    "out_tc_len_": np.uint32,
+    "out_tc_seedIdx_": np.int32,
+    "out_tc_trackCandidateType_": np.int16,
+    "out_tc_hitIdxs_": np.uint32,
+}

@@ -1,11 +1,18 @@
-"""Generates tests/golden/ref_pins.json: known answers of the reference CPU
-backend (oracle/_ref/liblstref_cr.so, built from the reference sources) on
-seeded synthetic events.
+"""Generates the golden fixtures of tests/golden/: known answers of the
+reference CPU backend (oracle/_ref/liblstref_cr.so, built from the reference
+sources) on seeded synthetic events.
 
-For each event: a digest of the generator's inputs, the reference's object
-counts after every stage, sha256 digests of the live entries of the main
-object fields after the full chain (oracle.compare.DIGEST_FIELDS), and for the
-single-muon events the complete LST::getOutput hit lists.
+ref_pins.json, the Event API: for each event a digest of the generator's
+inputs, the reference's object counts after every stage, sha256 digests of
+the live entries of the main object fields after the full chain
+(oracle.compare.DIGEST_FIELDS), and for the single-muon events the complete
+LST::getOutput hit lists.
+
+seed_pins.json, the CMSSW entry point LST::run: for each event a digest of the
+generator's CMSSW-layout seeds and hits, digests of the 23 vectors
+LST::prepareInput produces, and digests of LST::run's outputs (hits, len,
+seedIdx, trackCandidateType), with the complete outputs for the single-muon
+events.
 
     python tests/golden/make_golden.py
 """
@@ -24,7 +31,9 @@ from tracklooper_b200 import gen  # noqa: E402
 from tracklooper_b200.lst import STAGE_ORDER  # noqa: E402
 
 EVENTS = [(1, i, 0.0) for i in range(4)] + [(2, 0, 0.0), (3, 0, 40.0)]
+SEED_EVENTS = [(1, i, 0.0) for i in range(4)] + [(3, 1, 40.0), (2, 0, 0.0), (5, 0, 0.0)]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_pins.json")
+SEED_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "seed_pins.json")
 
 # element types of the compared fields (as in the CUDA library's field table)
 DTYPES = {
@@ -113,8 +122,50 @@ def pins_for(ref, inp):
     return counts, compare.store_digests(get, ref.n_lower, inp.n_hits, sizes), get
 
 
+def array_digest(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:32]
+
+
+def seed_digest(seeds) -> str:
+    h = hashlib.sha256()
+    for k in gen.SEED_FLOAT_FIELDS + ("see_q",):
+        h.update(np.ascontiguousarray(seeds.see[k]).tobytes())
+    for a in (seeds.hit_offsets, seeds.hit_idx, seeds.ph2_detId, seeds.ph2_x, seeds.ph2_y, seeds.ph2_z):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()[:32]
+
+
+def seed_pins_for(ref, seeds, full_output: bool) -> dict:
+    prep = ref.prepare_input(seeds)
+    run = ref.run_lst(seeds)
+    rec = {"n_seeds": seeds.n_seeds, "n_ph2": seeds.n_ph2, "inputs": seed_digest(seeds),
+           "n_hits": int(prep["in_trkX_"].size), "n_pls": int(prep["in_ptIn_vec_"].size),
+           "prepare": {k: array_digest(v) for k, v in sorted(prep.items())},
+           "n_tc": int(run["len"].size), "run": {k: array_digest(v) for k, v in sorted(run.items())}}
+    if full_output:
+        bounds = np.concatenate(([0], np.cumsum(run["len"].astype(np.int64))))
+        rec["output"] = [[int(run["trackCandidateType"][i]), int(run["seedIdx"][i]),
+                          run["hits"][bounds[i]:bounds[i + 1]].tolist()] for i in range(run["len"].size)]
+    return rec
+
+
+def seed_main(ref):
+    pins = {"reference": "liblstref_cr.so: SDL/LST.cc with ROOT's XYZVector restated (oracle/ref/shim/Math)",
+            "events": []}
+    for config, index, pileup in SEED_EVENTS:
+        seeds = gen.generate_event(config, index, pileup).seeds
+        rec = {"config": config, "index": index, "pileup": pileup}
+        rec.update(seed_pins_for(ref, seeds, config == 1))
+        pins["events"].append(rec)
+        print("seeds", config, index, rec["n_pls"], rec["n_tc"])
+    with open(SEED_OUT, "w") as f:
+        json.dump(pins, f, indent=1)
+    print("wrote", SEED_OUT)
+
+
 def main():
     ref = reflib.RefLST("cr")
+    seed_main(ref)
     pins = {"reference": "liblstref_cr.so (strict IEEE, double-rounded float transcendentals, T5 DNN)",
             "events": []}
     for config, index, pileup in EVENTS:

@@ -30,7 +30,7 @@ NVCC_FLAGS = [
 
 LIB_SOURCES = ["lst_event.cu", "lst_dnn.cu", "es.cc"]
 LIB_DEPS = ["lst_core.h", "lst_md.h", "lst_ls.h", "lst_t3.h", "lst_t5.h", "lst_pixel.h", "lst_device.h",
-            "lst_kernels.cuh", "lst_fields.h", "es.h"]
+            "lst_kernels.cuh", "lst_fields.h", "lst_seed.h", "es.h"]
 
 
 def _nvcc():

@@ -387,6 +387,13 @@ namespace {
     std::vector<int8_t> pixelType;
     std::vector<char> isQuad;
     std::vector<Particle> particles;
+    // The same seeds before conversion, in the CMSSW layout LST::run takes
+    // (SDL/LST.h:32-52), every seed including those the pT cut drops; see_f
+    // holds the 13 float arrays see_px .. see_stateTrajGlbPz in that order.
+    std::vector<float> see_f[13];
+    std::vector<int> see_q, see_sim;
+    std::vector<uint32_t> see_hitOff{0};
+    std::vector<int> see_hitIdx;
   };
 
   struct Config {
@@ -513,6 +520,16 @@ namespace {
       return a;
     };
 
+    {
+      const double raw[13] = {spx, spy, spz, dxy, dz, ptErr, etaErr, pos[0], pos[1], pos[2], pxLH, pyLH, pzLH};
+      for (int k = 0; k < 13; ++k)
+        ev.see_f[k].push_back(f32(raw[k]));
+      ev.see_q.push_back(static_cast<int>(p.q));
+      ev.see_sim.push_back(particle);
+      for (int k = 0; k < (nHits > 3 ? 4 : 3); ++k)
+        ev.see_hitIdx.push_back(static_cast<int>(pixBase + k));
+      ev.see_hitOff.push_back(static_cast<uint32_t>(ev.see_hitIdx.size()));
+    }
     float ptIn = f32(ptOf(pxLH, pyLH));
     float eta = f32(etaOf(pxLH, pyLH, pzLH));
     float fPtErr = f32(ptErr);
@@ -743,6 +760,26 @@ void lstgen_event_pls(void* ev,
   std::memcpy(pixelType, e->pixelType.data(), n);
   std::memcpy(isQuad, e->isQuad.data(), n);
   std::memcpy(simIdx, e->plsSim.data(), n * 4);
+}
+
+// CMSSW-layout seeds (all of them, before the pT cut): sizes, then the 13
+// float arrays see_px .. see_stateTrajGlbPz (each n_seeds), see_q, the
+// see_hitIdx offsets (n_seeds + 1) and values, and the seeds' particle index.
+void lstgen_event_seed_sizes(void* ev, unsigned int* nSeeds, unsigned int* nSeedHits) {
+  auto* e = static_cast<Event*>(ev);
+  *nSeeds = static_cast<unsigned int>(e->see_q.size());
+  *nSeedHits = static_cast<unsigned int>(e->see_hitIdx.size());
+}
+
+void lstgen_event_seeds(void* ev, float* const* f13, int* q, unsigned int* hitOff, int* hitIdx, int* sim) {
+  auto* e = static_cast<Event*>(ev);
+  size_t n = e->see_q.size();
+  for (int k = 0; k < 13; ++k)
+    std::memcpy(f13[k], e->see_f[k].data(), n * 4);
+  std::memcpy(q, e->see_q.data(), n * 4);
+  std::memcpy(hitOff, e->see_hitOff.data(), (n + 1) * 4);
+  std::memcpy(hitIdx, e->see_hitIdx.data(), e->see_hitIdx.size() * 4);
+  std::memcpy(sim, e->see_sim.data(), n * 4);
 }
 
 void lstgen_event_particles(void* ev, double* out7) {

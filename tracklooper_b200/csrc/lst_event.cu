@@ -281,11 +281,17 @@ struct lst_event {
   std::vector<lst::EventView> hv;
   lst::EventView* dv = nullptr;
   int t5Method = LST_T5_DNN;
-  // batched-input staging
+  // batched-input staging: the last upload's packed events (kind 0: the
+  // Event-API layout of lst_batch_upload, 1: CMSSW seeds of
+  // lst_batch_upload_seeds) for slots [inboxFirst, inboxFirst + inboxCount)
   unsigned char* inbox = nullptr;
   size_t inboxBytes = 0;
+  size_t inboxUsed = 0;
   unsigned long long* dOffsets = nullptr;
   bool inboxValid = false;
+  int inboxKind = 0;
+  int inboxFirst = 0, inboxCount = 0;
+  std::vector<unsigned char> hostPack;  // staging of lst_event_prepare_input
   // per-slot counts, contiguous on the device and in pinned host memory
   lst_counts* dCounts = nullptr;
   lst_counts* hCounts = nullptr;
@@ -476,14 +482,20 @@ namespace {
   }
 
   // Resets slots [first, first + count) and unpacks their packed inputs from
-  // the device inbox: the work of addHitToEvent + addPixelSegmentToEvent.
+  // the device inbox: the work of addHitToEvent + addPixelSegmentToEvent,
+  // preceded for seed events by the conversion of LST::prepareInput.
   int ingestInbox(lst_event* ev, int first, int count) {
     int rc = runReset(ev, first, count);
     if (rc)
       return rc;
     cudaStream_t s = ev->stream;
-    LST_LAUNCH(lst::kUnpack, dim3(blocksFor(ev->maxHits, count), count), kThreads, ev->dv + first, ev->inbox,
-               ev->dOffsets + first);
+    const unsigned long long total = ev->inboxUsed;
+    if (ev->inboxKind == 1)
+      LST_LAUNCH(lst::kPrepareInput, dim3(1 + blocksFor(ev->maxHits, count, 1024), count), 1024, ev->dv + first,
+                 ev->inbox, ev->dOffsets + first, total);
+    else
+      LST_LAUNCH(lst::kUnpack, dim3(blocksFor(ev->maxHits, count), count), kThreads, ev->dv + first, ev->inbox,
+                 ev->dOffsets + first, total);
     rc = runHitKernels(ev, first, count);
     if (rc)
       return rc;
@@ -1066,20 +1078,22 @@ int lst_field_info(int i, const char** name, size_t* elem_size, char* kind) {
 
 size_t lst_packed_size(uint32_t n_hits, uint32_t n_pls) { return lst::packedLayout(n_hits, n_pls).end; }
 
-int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
-                     const uint64_t* blob_offsets) {
-  int rc = checkSlots(ev, first, count);
-  if (rc)
-    return rc;
-  if (count == 0)
-    return 0;
-  if (!blobs || !blob_offsets)
-    return setError("lst_batch_upload: null argument");
-  for (int i = 0; i < count; ++i) {
-    if (blob_offsets[i] % 16 != 0 || blob_offsets[i] + 16 > total_bytes)
-      return setError("lst_batch_upload: blob offset misaligned or outside the buffer");
-  }
-  if (total_bytes > ev->inboxBytes) {
+namespace {
+  // Copies packed events into the set's device inbox and ingests them.
+  int uploadInbox(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                  const uint64_t* blob_offsets, int kind, const char* who) {
+    int rc = checkSlots(ev, first, count);
+    if (rc)
+      return rc;
+    if (count == 0)
+      return 0;
+    if (!blobs || !blob_offsets)
+      return setError(std::string(who) + ": null argument");
+    for (int i = 0; i < count; ++i) {
+      if (blob_offsets[i] % 16 != 0 || blob_offsets[i] + 16 > total_bytes)
+        return setError(std::string(who) + ": blob offset misaligned or outside the buffer");
+    }
+    if (total_bytes > ev->inboxBytes) {
     LST_CUDA(cudaStreamSynchronize(ev->stream));
     if (ev->inbox)
       LST_CUDA(cudaFree(ev->inbox));
@@ -1093,7 +1107,22 @@ int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, siz
   LST_CUDA(cudaMemcpyAsync(ev->inbox, blobs, total_bytes, cudaMemcpyDefault, s));
   LST_CUDA(cudaMemcpyAsync(ev->dOffsets + first, blob_offsets, sizeof(uint64_t) * count, cudaMemcpyDefault, s));
   ev->inboxValid = true;
+  ev->inboxUsed = total_bytes;
+  ev->inboxKind = kind;
+  ev->inboxFirst = first;
+  ev->inboxCount = count;
   return ingestInbox(ev, first, count);
+  }
+}  // namespace
+
+int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                     const uint64_t* blob_offsets) {
+  return uploadInbox(ev, first, count, blobs, total_bytes, blob_offsets, 0, "lst_batch_upload");
+}
+
+int lst_batch_upload_seeds(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                           const uint64_t* blob_offsets) {
+  return uploadInbox(ev, first, count, blobs, total_bytes, blob_offsets, 1, "lst_batch_upload_seeds");
 }
 
 int lst_batch_ingest(lst_event* ev, int first, int count) {
@@ -1102,7 +1131,107 @@ int lst_batch_ingest(lst_event* ev, int first, int count) {
     return rc;
   if (!ev->inboxValid)
     return setError("lst_batch_ingest: no packed inputs uploaded");
+  if (count > 0 && (first < ev->inboxFirst || first + count > ev->inboxFirst + ev->inboxCount))
+    return setError("lst_batch_ingest: slots outside the range of the last upload");
   return count == 0 ? 0 : ingestInbox(ev, first, count);
+}
+
+size_t lst_seed_packed_size(uint32_t n_ph2, uint32_t n_seeds, uint32_t n_seed_hits) {
+  return lst::seedLayout(n_ph2, n_seeds, n_seed_hits).end;
+}
+
+int lst_seed_pack(const lst_seed_input* in, void* dst, size_t capacity) {
+  if (!in || !dst)
+    return setError("lst_seed_pack: null argument");
+  const uint32_t nS = in->n_seeds, nH = in->n_ph2;
+  const float* f[lst::kSeedFloatArrays] = {in->see_px,
+                                           in->see_py,
+                                           in->see_pz,
+                                           in->see_dxy,
+                                           in->see_dz,
+                                           in->see_ptErr,
+                                           in->see_etaErr,
+                                           in->see_stateTrajGlbX,
+                                           in->see_stateTrajGlbY,
+                                           in->see_stateTrajGlbZ,
+                                           in->see_stateTrajGlbPx,
+                                           in->see_stateTrajGlbPy,
+                                           in->see_stateTrajGlbPz};
+  if (nS > 0) {
+    for (const float* a : f)
+      if (!a)
+        return setError("lst_seed_pack: null seed array");
+    if (!in->see_q || !in->see_hitIdx_offsets)
+      return setError("lst_seed_pack: null seed array");
+  }
+  if (nH > 0 && (!in->ph2_detId || !in->ph2_x || !in->ph2_y || !in->ph2_z))
+    return setError("lst_seed_pack: null hit array");
+  const uint32_t* off = in->see_hitIdx_offsets;
+  const uint32_t nSH = nS > 0 ? off[nS] : 0;
+  if (nS > 0) {
+    if (off[0] != 0)
+      return setError("lst_seed_pack: see_hitIdx_offsets[0] must be 0");
+    for (uint32_t i = 0; i < nS; ++i)
+      if (off[i + 1] < off[i])
+        return setError("lst_seed_pack: see_hitIdx_offsets not ascending at seed " + std::to_string(i));
+    if (nSH > 0 && !in->see_hitIdx)
+      return setError("lst_seed_pack: null see_hitIdx");
+  }
+  const lst::SeedLayout L = lst::seedLayout(nH, nS, nSH);
+  if (capacity < L.end)
+    return setError("lst_seed_pack: destination holds " + std::to_string(capacity) + " bytes, the event needs " +
+                    std::to_string(L.end));
+  unsigned char* d = static_cast<unsigned char*>(dst);
+  const uint32_t hdr[4] = {nH, nS, nSH, lst::kSeedMagic};
+  std::memcpy(d, hdr, sizeof(hdr));
+  if (nH > 0) {
+    std::memcpy(d + L.detId, in->ph2_detId, 4 * size_t(nH));
+    std::memcpy(d + L.x, in->ph2_x, 4 * size_t(nH));
+    std::memcpy(d + L.y, in->ph2_y, 4 * size_t(nH));
+    std::memcpy(d + L.z, in->ph2_z, 4 * size_t(nH));
+  }
+  if (nS > 0) {
+    for (int k = 0; k < lst::kSeedFloatArrays; ++k)
+      std::memcpy(d + L.f[k], f[k], 4 * size_t(nS));
+    std::memcpy(d + L.q, in->see_q, 4 * size_t(nS));
+    std::memcpy(d + L.hitOff, off, 4 * (size_t(nS) + 1));
+    if (nSH > 0)
+      std::memcpy(d + L.hitIdx, in->see_hitIdx, 4 * size_t(nSH));
+  } else {
+    std::memset(d + L.hitOff, 0, 4);
+  }
+  if (L.end > L.hitIdx + 4 * size_t(nSH))
+    std::memset(d + L.hitIdx + 4 * size_t(nSH), 0, L.end - L.hitIdx - 4 * size_t(nSH));
+  return 0;
+}
+
+int lst_event_prepare_input(lst_event* ev, int slot, const lst_seed_input* in) {
+  int rc = checkSlots(ev, slot, 1);
+  if (rc)
+    return rc;
+  if (!in)
+    return setError("lst_event_prepare_input: null input");
+  const uint32_t nSH = in->n_seeds > 0 && in->see_hitIdx_offsets ? in->see_hitIdx_offsets[in->n_seeds] : 0;
+  const size_t need = lst_seed_packed_size(in->n_ph2, in->n_seeds, nSH);
+  // Pageable staging: cudaMemcpyAsync from pageable memory returns once the
+  // bytes are taken, so the vector can be refilled by the next call.
+  if (ev->hostPack.size() < need)
+    ev->hostPack.resize(need);
+  rc = lst_seed_pack(in, ev->hostPack.data(), ev->hostPack.size());
+  if (rc)
+    return rc;
+  const uint64_t offset = 0;
+  return lst_batch_upload_seeds(ev, slot, 1, ev->hostPack.data(), need, &offset);
+}
+
+int lst_run(lst_event* ev, int slot, const lst_seed_input* in, lst_output* out) {
+  int rc = lst_event_prepare_input(ev, slot, in);
+  if (rc)
+    return rc;
+  rc = lst_batch_run(ev, slot, 1, LST_STAGE_MINI_DOUBLETS, LST_STAGE_TRACK_CANDIDATES);
+  if (rc)
+    return rc;
+  return out ? lst_batch_get_output(ev, slot, 1, out) : 0;
 }
 
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage) {

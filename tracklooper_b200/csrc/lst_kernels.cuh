@@ -2453,12 +2453,20 @@ namespace lst {
   // Unpacks the packed inputs of a batch into the event stores: the hits
   // (addHitToEvent's copies) and the pixel-segment fields
   // (addPixelSegmentToEvent's copies).  blockIdx.y = event within the batch.
-  __global__ void kUnpack(const EventView* evs, const unsigned char* blobs, const unsigned long long* offsets) {
+  __global__ void kUnpack(const EventView* evs, const unsigned char* blobs, const unsigned long long* offsets,
+                          unsigned long long totalBytes) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned char* b = blobs + offsets[blockIdx.y];
     const unsigned int* hdr = reinterpret_cast<const unsigned int*>(b);
     unsigned int nHits = hdr[0], nPLSIn = hdr[1];
     unsigned int status = 0;
+    // A blob whose arrays would end beyond the uploaded bytes is dropped.
+    const bool truncated = offsets[blockIdx.y] + packedLayout(nHits, nPLSIn).end > totalBytes;
+    if (truncated) {
+      status |= kStatusInvalidInput;
+      nHits = 0;
+      nPLSIn = 0;
+    }
     bool reject = nHits > ev.maxHits;
     unsigned int nPLS = nPLSIn;
     if (reject) {
@@ -2474,7 +2482,7 @@ namespace lst {
       status |= kStatusInvalidInput;
       nPLS = 0;
     }
-    const PackedLayout L = packedLayout(reject ? 0u : hdr[0], reject ? 0u : nPLSIn);
+    const PackedLayout L = packedLayout(reject ? 0u : nHits, reject ? 0u : nPLSIn);
     const unsigned int stride = gridDim.x * blockDim.x;
     const unsigned int t0 = blockIdx.x * blockDim.x + threadIdx.x;
     for (unsigned int i = t0; i < nHits; i += stride) {
@@ -2597,3 +2605,5 @@ namespace lst {
   }
 
 }  // namespace lst
+
+#include "lst_seed.h"

@@ -51,6 +51,57 @@ PLS_FIELDS = (
 )
 
 
+# The float inputs of LST::run (SDL/LST.h:32-45), in argument order.
+SEED_FLOAT_FIELDS = (
+    "see_px",
+    "see_py",
+    "see_pz",
+    "see_dxy",
+    "see_dz",
+    "see_ptErr",
+    "see_etaErr",
+    "see_stateTrajGlbX",
+    "see_stateTrajGlbY",
+    "see_stateTrajGlbZ",
+    "see_stateTrajGlbPx",
+    "see_stateTrajGlbPy",
+    "see_stateTrajGlbPz",
+)
+
+
+@dataclasses.dataclass
+class SeedInput:
+    """One event's inputs in the CMSSW layout of LST::run (SDL/LST.h:32-52).
+
+    ``see`` maps the 13 float seed arrays plus ``see_q`` to numpy arrays;
+    ``see_hitIdx`` (a vector<vector<int>> in the reference) is stored flat,
+    seed i owning ``hit_idx[hit_offsets[i]:hit_offsets[i + 1]]``.  ``ph2_*``
+    are the outer-tracker hits.
+    """
+
+    see: dict
+    hit_offsets: np.ndarray
+    hit_idx: np.ndarray
+    ph2_detId: np.ndarray
+    ph2_x: np.ndarray
+    ph2_y: np.ndarray
+    ph2_z: np.ndarray
+    seed_sim: np.ndarray | None = None
+
+    @property
+    def n_seeds(self) -> int:
+        return int(self.see["see_q"].shape[0])
+
+    @property
+    def n_ph2(self) -> int:
+        return int(self.ph2_x.shape[0])
+
+    def hit_lists(self) -> list:
+        """see_hitIdx as a list of per-seed lists."""
+        o = self.hit_offsets
+        return [self.hit_idx[o[i]:o[i + 1]].tolist() for i in range(self.n_seeds)]
+
+
 @dataclasses.dataclass
 class EventInput:
     """One event's inputs in the reference's Event-API layout."""
@@ -65,6 +116,7 @@ class EventInput:
     pls_sim: np.ndarray
     n_ot_hits: int
     particles: np.ndarray  # (n, 7): pt, eta, phi, q, vx, vy, vz
+    seeds: SeedInput | None = None  # the same event before seed conversion
 
     @property
     def n_hits(self) -> int:
@@ -91,6 +143,8 @@ def _lib():
         lib.lstgen_event_hits.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
         lib.lstgen_event_pls.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 19
         lib.lstgen_event_particles.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.lstgen_event_seed_sizes.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_uint)] * 2
+        lib.lstgen_event_seeds.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)] + [ctypes.c_void_p] * 4
         _LIB = lib
     return _LIB
 
@@ -130,6 +184,18 @@ def generate_event(config: int, index: int, pileup: float = 0.0) -> EventInput:
         lib.lstgen_event_pls(h, *[pls[name].ctypes.data for name, _ in PLS_FIELDS], pls_sim.ctypes.data)
         parts = np.empty((n_part, 7), np.float64)
         lib.lstgen_event_particles(h, parts.ctypes.data)
+        ns, nsh = ctypes.c_uint(), ctypes.c_uint()
+        lib.lstgen_event_seed_sizes(h, ctypes.byref(ns), ctypes.byref(nsh))
+        see = {name: np.empty(ns.value, np.float32) for name in SEED_FLOAT_FIELDS}
+        see["see_q"] = np.empty(ns.value, np.int32)
+        hit_off = np.empty(ns.value + 1, np.uint32)
+        hit_idx = np.empty(nsh.value, np.int32)
+        seed_sim = np.empty(ns.value, np.int32)
+        f13 = (ctypes.c_void_p * 13)(*[see[name].ctypes.data for name in SEED_FLOAT_FIELDS])
+        lib.lstgen_event_seeds(h, f13, see["see_q"].ctypes.data, hit_off.ctypes.data, hit_idx.ctypes.data,
+                               seed_sim.ctypes.data)
     finally:
         lib.lstgen_event_free(h)
-    return EventInput(x, y, z, det, idx, pls, sim, pls_sim, n_ot, parts)
+    seeds = SeedInput(see, hit_off, hit_idx, det[:n_ot].copy(), x[:n_ot].copy(), y[:n_ot].copy(), z[:n_ot].copy(),
+                      seed_sim)
+    return EventInput(x, y, z, det, idx, pls, sim, pls_sim, n_ot, parts, seeds)

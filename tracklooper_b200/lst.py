@@ -49,6 +49,14 @@ STAGE_ORDER = ("md", "ls", "t3", "t5", "pls_clean", "pt5", "pt3", "tc")
 T5_DNN = 0
 T5_CUTS = 1
 
+STATUS_UNKNOWN_DETID = 0x1
+STATUS_UNKNOWN_ENDCAP_DETID = 0x2
+STATUS_HIT_CAPACITY = 0x4
+STATUS_PLS_TRUNCATED = 0x8
+STATUS_TC_TRUNCATED = 0x10
+STATUS_CAP_OVERFLOW = 0x20
+STATUS_INVALID_INPUT = 0x40
+
 STATUS_BITS = {
     0x1: "unknown detId",
     0x2: "unknown endcap detId",
@@ -111,6 +119,11 @@ EXPORTS = (
     "lst_t5dnn_scratch_floats",
     "lst_t5dnn_backward",
     "lst_t5dnn_last_error",
+    "lst_seed_packed_size",
+    "lst_seed_pack",
+    "lst_batch_upload_seeds",
+    "lst_event_prepare_input",
+    "lst_run",
 )
 
 
@@ -170,6 +183,44 @@ class Output(ctypes.Structure):
         ("event_tc_offsets", ctypes.c_void_p),
         ("event_hit_offsets", ctypes.c_void_p),
     ]
+
+
+class SeedInputC(ctypes.Structure):
+    """lst_seed_input (include/lst_b200.h): the CMSSW inputs of LST::run."""
+
+    _fields_ = [("n_seeds", ctypes.c_uint32)] + [
+        (name, ctypes.c_void_p)
+        for name in ("see_px", "see_py", "see_pz", "see_dxy", "see_dz", "see_ptErr", "see_etaErr",
+                     "see_stateTrajGlbX", "see_stateTrajGlbY", "see_stateTrajGlbZ", "see_stateTrajGlbPx",
+                     "see_stateTrajGlbPy", "see_stateTrajGlbPz", "see_q", "see_hitIdx_offsets", "see_hitIdx")
+    ] + [("n_ph2", ctypes.c_uint32)] + [(name, ctypes.c_void_p) for name in ("ph2_detId", "ph2_x", "ph2_y", "ph2_z")]
+
+
+def seed_struct(seeds) -> tuple[SeedInputC, list]:
+    """A SeedInputC over a gen.SeedInput's arrays (plus the arrays it points
+    into, which must stay alive while the struct is used)."""
+    from .gen import SEED_FLOAT_FIELDS
+
+    keep = []
+
+    def p(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    c = SeedInputC()
+    c.n_seeds = seeds.n_seeds
+    for name in SEED_FLOAT_FIELDS:
+        setattr(c, name, p(seeds.see[name], np.float32))
+    c.see_q = p(seeds.see["see_q"], np.int32)
+    c.see_hitIdx_offsets = p(seeds.hit_offsets, np.uint32)
+    c.see_hitIdx = p(seeds.hit_idx, np.int32)
+    c.n_ph2 = seeds.n_ph2
+    c.ph2_detId = p(seeds.ph2_detId, np.uint32)
+    c.ph2_x = p(seeds.ph2_x, np.float32)
+    c.ph2_y = p(seeds.ph2_y, np.float32)
+    c.ph2_z = p(seeds.ph2_z, np.float32)
+    return c, keep
 
 
 class KernelTime(ctypes.Structure):
@@ -253,6 +304,12 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_t5dnn_scratch_floats.restype = sz
         lib.lst_t5dnn_backward.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp]
         lib.lst_t5dnn_last_error.restype = ctypes.c_char_p
+        lib.lst_seed_packed_size.argtypes = [u32, u32, u32]
+        lib.lst_seed_packed_size.restype = sz
+        lib.lst_seed_pack.argtypes = [ctypes.POINTER(SeedInputC), vp, sz]
+        lib.lst_batch_upload_seeds.argtypes = [vp, i32, i32, vp, sz, vp]
+        lib.lst_event_prepare_input.argtypes = [vp, i32, ctypes.POINTER(SeedInputC)]
+        lib.lst_run.argtypes = [vp, i32, ctypes.POINTER(SeedInputC), ctypes.POINTER(Output)]
         _lib = lib
         return lib
 
@@ -488,6 +545,17 @@ class EventSet:
         _check(library().lst_batch_upload(self._h, first, offsets.size, blobs.ctypes.data, blobs.nbytes,
                                           offsets.ctypes.data), "lst_batch_upload")
 
+    def upload_seeds(self, first: int, blobs: np.ndarray, offsets: np.ndarray):
+        """lst_batch_upload_seeds: packed CMSSW seed events (pack_seed_events)."""
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        _check(library().lst_batch_upload_seeds(self._h, first, offsets.size, blobs.ctypes.data, blobs.nbytes,
+                                                offsets.ctypes.data), "lst_batch_upload_seeds")
+
+    def prepare_input(self, slot: int, seeds):
+        """lst_event_prepare_input: LST::prepareInput + addHitToEvent + addPixelSegmentToEvent."""
+        c, keep = seed_struct(seeds)
+        _check(library().lst_event_prepare_input(self._h, slot, ctypes.byref(c)), "lst_event_prepare_input")
+
     def ingest(self, first: int, count: int):
         _check(library().lst_batch_ingest(self._h, first, count), "lst_batch_ingest")
 
@@ -559,6 +627,25 @@ def pack_event(inp, out: np.ndarray | None = None, offset: int = 0) -> np.ndarra
     buf[:flat.size] = flat
     buf[flat.size:] = 0
     return out
+
+
+def seed_packed_size(n_ph2: int, n_seeds: int, n_seed_hits: int) -> int:
+    return int(library().lst_seed_packed_size(n_ph2, n_seeds, n_seed_hits))
+
+
+def pack_seed_events(seed_inputs) -> tuple[np.ndarray, np.ndarray]:
+    """Packs several events' CMSSW seeds (gen.SeedInput) back to back with
+    lst_seed_pack; returns (blob bytes, offsets) for EventSet.upload_seeds."""
+    lib = library()
+    sizes = [seed_packed_size(s.n_ph2, s.n_seeds, int(s.hit_offsets[-1]) if s.n_seeds else 0) for s in seed_inputs]
+    offsets = np.zeros(len(seed_inputs), np.uint64)
+    if seed_inputs:
+        offsets[1:] = np.cumsum(sizes[:-1])
+    blob = np.zeros(int(sum(sizes)), np.uint8)
+    for s, off, size in zip(seed_inputs, offsets, sizes):
+        c, keep = seed_struct(s)
+        _check(lib.lst_seed_pack(ctypes.byref(c), blob.ctypes.data + int(off), size), "lst_seed_pack")
+    return blob, offsets
 
 
 def pack_events(inputs) -> tuple[np.ndarray, np.ndarray]:
@@ -679,3 +766,74 @@ class Event:
             self._set.run_stage(self._slot, st)
             if st == upto:
                 break
+
+
+class LST:
+    """SDL::LST<Acc> (SDL/LST.h:25-111): ``run`` takes the CMSSW seed and hit
+    vectors, converts them (LST::prepareInput), runs the chain and keeps the
+    output that ``hits()``, ``len()``, ``seedIdx()`` and
+    ``trackCandidateType()`` return."""
+
+    def __init__(self, es: ES, max_hits: int = 1 << 20, event_set: EventSet | None = None, slot: int = 0):
+        self._set = event_set or EventSet(es, 1, max_hits)
+        self._slot = slot
+        self._out = ([], np.zeros(0, np.uint32), np.zeros(0, np.int32), np.zeros(0, np.int16))
+
+    @property
+    def event_set(self) -> EventSet:
+        return self._set
+
+    def run(self, see_px, see_py, see_pz, see_dxy, see_dz, see_ptErr, see_etaErr, see_stateTrajGlbX,
+            see_stateTrajGlbY, see_stateTrajGlbZ, see_stateTrajGlbPx, see_stateTrajGlbPy, see_stateTrajGlbPz, see_q,
+            see_hitIdx, ph2_detId, ph2_x, ph2_y, ph2_z, tc_capacity: int = 31000):
+        """LST::run with the reference's argument list; see_hitIdx is a list
+        of per-seed index lists."""
+        from .gen import SEED_FLOAT_FIELDS, SeedInput
+
+        vals = (see_px, see_py, see_pz, see_dxy, see_dz, see_ptErr, see_etaErr, see_stateTrajGlbX, see_stateTrajGlbY,
+                see_stateTrajGlbZ, see_stateTrajGlbPx, see_stateTrajGlbPy, see_stateTrajGlbPz)
+        see = {k: np.asarray(v, np.float32) for k, v in zip(SEED_FLOAT_FIELDS, vals)}
+        see["see_q"] = np.asarray(see_q, np.int32)
+        lens = np.array([len(h) for h in see_hitIdx], np.int64)
+        off = np.zeros(len(lens) + 1, np.uint32)
+        off[1:] = np.cumsum(lens)
+        flat = np.concatenate([np.asarray(h, np.int32) for h in see_hitIdx]) if len(lens) else np.zeros(0, np.int32)
+        seeds = SeedInput(see, off, flat, np.asarray(ph2_detId, np.uint32), np.asarray(ph2_x, np.float32),
+                          np.asarray(ph2_y, np.float32), np.asarray(ph2_z, np.float32))
+        return self.run_seeds(seeds, tc_capacity)
+
+    def run_seeds(self, seeds, tc_capacity: int = 31000):
+        """LST::run on a gen.SeedInput (flattened see_hitIdx)."""
+        c, keep = seed_struct(seeds)
+        hits = np.empty(tc_capacity * 14, np.uint32)
+        ln = np.empty(tc_capacity, np.uint32)
+        seed = np.empty(tc_capacity, np.int32)
+        typ = np.empty(tc_capacity, np.int16)
+        tco = np.empty(2, np.uint64)
+        hco = np.empty(2, np.uint64)
+        o = Output(hits.ctypes.data, hits.size, ln.ctypes.data, seed.ctypes.data, typ.ctypes.data, ln.size,
+                   tco.ctypes.data, hco.ctypes.data)
+        _check(library().lst_run(self._set.handle, self._slot, ctypes.byref(c), ctypes.byref(o)), "lst_run")
+        ntc, nh = int(tco[-1]), int(hco[-1])
+        ln = ln[:ntc].copy()
+        bounds = np.concatenate(([0], np.cumsum(ln.astype(np.int64))))
+        self._flat = hits[:nh].copy()
+        self._out = ([self._flat[bounds[i]:bounds[i + 1]].tolist() for i in range(ntc)], ln, seed[:ntc].copy(),
+                     typ[:ntc].copy())
+        return self
+
+    def hits(self) -> list:
+        return self._out[0]
+
+    def len(self) -> np.ndarray:
+        return self._out[1]
+
+    def seedIdx(self) -> np.ndarray:
+        return self._out[2]
+
+    def trackCandidateType(self) -> np.ndarray:
+        return self._out[3]
+
+    def flat_hits(self) -> np.ndarray:
+        """hits() concatenated over the candidates."""
+        return getattr(self, "_flat", np.zeros(0, np.uint32))
