@@ -68,17 +68,25 @@ namespace lst {
   constexpr float kT5DnnWP = 0.6177366f;
 
   // --------------------------------------------------- math binding (see top)
-  LST_HD float fsin(float x) { return static_cast<float>(::sin(static_cast<double>(x))); }
-  LST_HD float fcos(float x) { return static_cast<float>(::cos(static_cast<double>(x))); }
-  LST_HD float ftan(float x) { return static_cast<float>(::tan(static_cast<double>(x))); }
-  LST_HD float fasin(float x) { return static_cast<float>(::asin(static_cast<double>(x))); }
-  LST_HD float facos(float x) { return static_cast<float>(::acos(static_cast<double>(x))); }
-  LST_HD float fatan(float x) { return static_cast<float>(::atan(static_cast<double>(x))); }
-  LST_HD float fsinh(float x) { return static_cast<float>(::sinh(static_cast<double>(x))); }
-  LST_HD float facosh(float x) { return static_cast<float>(::acosh(static_cast<double>(x))); }
-  LST_HD float fexp(float x) { return static_cast<float>(::exp(static_cast<double>(x))); }
-  LST_HD float flog(float x) { return static_cast<float>(::log(static_cast<double>(x))); }
-  LST_HD float fatan2(float y, float x) {
+  // One out-of-line copy of each double-precision routine on the device: the
+  // cut algorithms call them from dozens of sites, and an inlined copy per
+  // site multiplies the code the diverging warps of one SM fetch.
+#if defined(__CUDACC__)
+#define LST_HD_MATH __host__ __device__ __noinline__
+#else
+#define LST_HD_MATH inline
+#endif
+  LST_HD_MATH float fsin(float x) { return static_cast<float>(::sin(static_cast<double>(x))); }
+  LST_HD_MATH float fcos(float x) { return static_cast<float>(::cos(static_cast<double>(x))); }
+  LST_HD_MATH float ftan(float x) { return static_cast<float>(::tan(static_cast<double>(x))); }
+  LST_HD_MATH float fasin(float x) { return static_cast<float>(::asin(static_cast<double>(x))); }
+  LST_HD_MATH float facos(float x) { return static_cast<float>(::acos(static_cast<double>(x))); }
+  LST_HD_MATH float fatan(float x) { return static_cast<float>(::atan(static_cast<double>(x))); }
+  LST_HD_MATH float fsinh(float x) { return static_cast<float>(::sinh(static_cast<double>(x))); }
+  LST_HD_MATH float facosh(float x) { return static_cast<float>(::acosh(static_cast<double>(x))); }
+  LST_HD_MATH float fexp(float x) { return static_cast<float>(::exp(static_cast<double>(x))); }
+  LST_HD_MATH float flog(float x) { return static_cast<float>(::log(static_cast<double>(x))); }
+  LST_HD_MATH float fatan2(float y, float x) {
     return static_cast<float>(::atan2(static_cast<double>(y), static_cast<double>(x)));
   }
   // Exact operations.
