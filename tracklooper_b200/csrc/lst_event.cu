@@ -417,13 +417,16 @@ namespace {
         LST_LAUNCH(lst::kT5Walk, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v,
                    useDnn);
         LST_LAUNCH(lst::kT5Emit, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v, useDnn);
-        LST_LAUNCH(lst::kT5DedupAfterBuild, dim3(ceilDiv(nLower * 32, 256), count), 256, d, v);
+        LST_LAUNCH(lst::kT5DedupAfterBuild,
+                   dim3(blocksFor(ev->es->nEligibleMax, count, lst::kT5DedupThreads), count), lst::kT5DedupThreads,
+                   d, v);
         LST_LAUNCH(lst::kT5Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;
       }
       case LST_STAGE_PLS_CLEANING:
         LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
-        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, false);
+        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d, v,
+                   false);
         break;
       case LST_STAGE_PIXEL_QUINTUPLETS:
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
@@ -447,7 +450,7 @@ namespace {
         LST_LAUNCH(lst::kPT3Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 1);
         LST_LAUNCH(lst::kPT3Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
-        LST_LAUNCH(lst::kPT3Dedup, dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPT3Dedup, warpGrid(lst::kMaxPixelTriplets, 8, count), 256, d, v);
         break;
       case LST_STAGE_TRACK_CANDIDATES: {
         const size_t nE = ev->es->nEligibleMax;
@@ -462,7 +465,8 @@ namespace {
         LST_LAUNCH(lst::kT5TCEmit, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kT5TCFinish, one, 32, d, v);
         LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
-        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count), count), kThreads, d, v, true);
+        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d, v,
+                   true);
         LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kTCCleanInfo, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kCrossCleanPLS, dim3(blocksFor(P, count, lst::kCleanTile), count), lst::kCleanTile, d, v);

@@ -1083,37 +1083,85 @@ namespace lst {
     return nMatched;
   }
 
-  // Duplicate removal among the T5s of one module (SDL/Kernels.h:202-249);
-  // one warp per module, only ever setting bit 1.
-  __global__ void kT5DedupAfterBuild(DeviceES es, const EventView* evs) {
+  // Duplicate removal among the T5s of one module (SDL/Kernels.h:202-249).
+  // Every pair (i < j) of a module is independent and only ever sets isDup
+  // bit 1, so the pairs are spread over a block: a chunk of the eligible-module
+  // list is scanned for modules holding two or more T5s, and each such module's
+  // T5s are staged in shared memory (eta, phi, score, hits) and its n x n pair
+  // square is shared out among the block's threads.  The largest modules hold
+  // a few hundred T5s, whose pairs would otherwise run on one warp.
+  constexpr int kT5DedupThreads = 128;
+  constexpr unsigned int kT5DedupStage = 256;
+  __global__ void __launch_bounds__(kT5DedupThreads) kT5DedupAfterBuild(DeviceES es, const EventView* evs) {
+    __shared__ float sEta[kT5DedupStage], sPhi[kT5DedupStage], sScore[kT5DedupStage];
+    __shared__ unsigned int sHits[kT5DedupStage * 10];
+    __shared__ uint16_t sMods[kT5DedupThreads];
     const EventView& ev = evs[blockIdx.y];
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (warp >= es.nLowerModules)
-      return;
-    const unsigned int n = ev.t5.nQuintuplets[warp];
-    if (n < 2)
-      return;
-    const unsigned int base = ev.rg.quintupletModuleIndices[warp];
+    const unsigned int nElig = *ev.rg.nEligibleT5Modules;
     Quintuplets q = ev.t5;
-    for (unsigned int ix1 = laneId(); ix1 < n; ix1 += 32) {
-      unsigned int ix = base + ix1;
-      float eta1 = q.eta[ix], phi1 = q.phi[ix], score1 = q.score_rphisum[ix];
-      for (unsigned int jx1 = ix1 + 1; jx1 < n; jx1++) {
-        unsigned int jx = base + jx1;
-        float eta2 = q.eta[jx], phi2 = q.phi[jx];
-        float dEta = fabs_(eta1 - eta2);
-        float dPhi = wrapDPhi(phi1, phi2);
-        float score2 = q.score_rphisum[jx];
-        if (dEta > 0.1f)
-          continue;
-        if (fabs_(dPhi) > 0.1f)
-          continue;
-        if (sharedHitsT5(q, ix, jx) >= 7) {
-          if (score1 >= score2)
-            q.isDup[ix] = 1;
-          else
-            q.isDup[jx] = 1;
+    for (unsigned int c0 = blockIdx.x * blockDim.x; c0 < nElig; c0 += gridDim.x * blockDim.x) {
+      const unsigned int e = c0 + threadIdx.x;
+      uint16_t lmLoad = 0;
+      unsigned int nLoad = 0;
+      if (e < nElig) {
+        lmLoad = ev.rg.indicesOfEligibleT5Modules[e];
+        nLoad = q.nQuintuplets[lmLoad];
+      }
+      unsigned int nMods;
+      const unsigned int slot = blockExclusiveScan(nLoad >= 2 ? 1u : 0u, nMods);
+      if (nLoad >= 2)
+        sMods[slot] = lmLoad;
+      __syncthreads();
+      for (unsigned int k = 0; k < nMods; ++k) {
+        const uint16_t lm = sMods[k];
+        const unsigned int n = q.nQuintuplets[lm];
+        const unsigned int base = ev.rg.quintupletModuleIndices[lm];
+        const bool staged = n <= kT5DedupStage;
+        if (staged) {
+          for (unsigned int t = threadIdx.x; t < n; t += blockDim.x) {
+            sEta[t] = q.eta[base + t];
+            sPhi[t] = q.phi[base + t];
+            sScore[t] = q.score_rphisum[base + t];
+          }
+          for (unsigned int t = threadIdx.x; t < 10 * n; t += blockDim.x)
+            sHits[t] = q.hitIndices[10 * base + t];
         }
+        __syncthreads();
+        for (unsigned int pr = threadIdx.x; pr < n * n; pr += blockDim.x) {
+          const unsigned int i = pr / n, j = pr - i * n;
+          if (j <= i)
+            continue;
+          const unsigned int ix = base + i, jx = base + j;
+          const float eta1 = staged ? sEta[i] : q.eta[ix], phi1 = staged ? sPhi[i] : q.phi[ix];
+          const float eta2 = staged ? sEta[j] : q.eta[jx], phi2 = staged ? sPhi[j] : q.phi[jx];
+          const float dEta = fabs_(eta1 - eta2);
+          const float dPhi = wrapDPhi(phi1, phi2);
+          if (dEta > 0.1f)
+            continue;
+          if (fabs_(dPhi) > 0.1f)
+            continue;
+          int nMatched = 0;
+          if (staged) {
+            for (int a = 0; a < 10; a++) {
+              const unsigned int h = sHits[10 * i + a];
+              bool matched = false;
+              for (int b = 0; b < 10; b++)
+                matched |= h == sHits[10 * j + b];
+              nMatched += matched ? 1 : 0;
+            }
+          } else {
+            nMatched = sharedHitsT5(q, ix, jx);
+          }
+          if (nMatched >= 7) {
+            const float score1 = staged ? sScore[i] : q.score_rphisum[ix];
+            const float score2 = staged ? sScore[j] : q.score_rphisum[jx];
+            if (score1 >= score2)
+              q.isDup[ix] = 1;
+            else
+              q.isDup[jx] = 1;
+          }
+        }
+        __syncthreads();
       }
     }
   }
@@ -1182,68 +1230,30 @@ namespace lst {
       ev.plsOrder[atomicAdd(&sCursor[plsEtaBin(ev.ls.eta[i])], 1u)] = i;
   }
 
-  // One (ix, jx) pair of the pLS duplicate check (SDL/Kernels.h:384-473).
-  LST_DEV void plsPair(const EventView& ev, unsigned int ix, unsigned int jx, const unsigned int* phits1,
-                       float eta_pix1, float phi_pix1, bool secondpass) {
-    const Segments& s = ev.ls;
-    float eta_pix2 = s.eta[jx];
-    float phi_pix2 = s.phi[jx];
-    if (fabs_(eta_pix2 - eta_pix1) > 0.1f)
-      return;
-    if (secondpass && (!s.isQuad[jx] || (s.isDup[jx] & 1)))
-      return;
-    int8_t quad_diff = s.isQuad[ix] - s.isQuad[jx];
-    float score_diff = s.score[ix] - s.score[jx];
-    unsigned int idxToRemove;
-    if (quad_diff > 0)
-      idxToRemove = jx;
-    else if (quad_diff < 0)
-      idxToRemove = ix;
-    else if (score_diff < 0)
-      idxToRemove = jx;
-    else if (score_diff > 0)
-      idxToRemove = ix;
-    else
-      idxToRemove = ix;
-    int npMatched = 0;
-    for (int i = 0; i < 4; i++) {
-      bool pmatched = false;
-      for (int j = 0; j < 4; j++) {
-        if (phits1[i] == s.pLSHitsIdxs[4 * jx + j]) {
-          pmatched = true;
-          break;
-        }
-      }
-      if (pmatched) {
-        npMatched++;
-        if (secondpass)
-          break;
-      }
-    }
-    bool remove = npMatched >= 3;
-    if (secondpass) {
-      float dEta = fabs_(eta_pix1 - eta_pix2);
-      float dPhi = wrapDPhi(phi_pix1, phi_pix2);
-      float dR2 = dEta * dEta + dPhi * dPhi;
-      if ((npMatched >= 1) || (dR2 < 1e-5f))
-        remove = true;
-    }
-    if (remove) {
-      if (secondpass)
-        ev.plsFlag[idxToRemove] = 1;
-      else
-        s.isDup[idxToRemove] = 1;
-    }
-  }
-
   // pLS duplicate removal (SDL/Kernels.h:384-473).  Pass 1 sets bit 1 of
   // isDup directly; pass 2 marks plsFlag and kMergePLSFlag folds it into bit 2
   // afterwards, so that pass 2 reads the pass-1 bit while other threads mark
-  // removals.  Every pair ix < jx that can pass the |deta| <= 0.1 test is
-  // visited once through the eta bins (neighbouring bins plus the non-finite
-  // bin); the outcome does not depend on the visiting order because marks are
-  // only ever set.
-  __global__ void kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
+  // removals.  The outcome of a pair (ix < jx) depends only on the two pLS, and
+  // marks are only ever set, so any visiting order and any repeat visit give
+  // the reference's result; pairs more than 0.1 apart in eta return at the
+  // reference's first test.
+  //
+  // Each block takes kPLSCleanTile consecutive pLS of the eta-sorted order (one
+  // per thread) and streams, through shared memory, the sorted positions that
+  // can lie within 0.1 in eta of any of them: the bins from kPLSBinReach below
+  // its first pLS's bin to kPLSBinReach above its last one, plus the
+  // non-finite bin, which meets every pLS (a NaN never satisfies the
+  // reference's skip).  A block holding a non-finite pLS streams all of them.
+  constexpr int kPLSCleanTile = 128;
+  struct PLSCleanTile {
+    float eta[kPLSCleanTile], phi[kPLSCleanTile], score[kPLSCleanTile];
+    unsigned int idx[kPLSCleanTile];
+    uint4 hits[kPLSCleanTile];
+    int8_t quad[kPLSCleanTile], dup[kPLSCleanTile];
+  };
+
+  __global__ void __launch_bounds__(kPLSCleanTile) kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
+    __shared__ PLSCleanTile sT;
     const EventView& ev = evs[blockIdx.y];
     unsigned int nPix = ev.ls.nSegments[es.pixelModule];
     if (nPix > kMaxPixelSegments)
@@ -1251,30 +1261,102 @@ namespace lst {
     const Segments& s = ev.ls;
     const unsigned int* order = ev.plsOrder;
     const unsigned int* binStart = ev.plsBinStart;
-    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < nPix; ix += gridDim.x * blockDim.x) {
-      if (secondpass && (!s.isQuad[ix] || (s.isDup[ix] & 1)))
-        continue;
-      unsigned int phits1[4] = {s.pLSHitsIdxs[4 * ix], s.pLSHitsIdxs[4 * ix + 1], s.pLSHitsIdxs[4 * ix + 2],
-                                s.pLSHitsIdxs[4 * ix + 3]};
-      float eta_pix1 = s.eta[ix];
-      float phi_pix1 = s.phi[ix];
-      const int b = plsEtaBin(eta_pix1);
-      if (b == kPLSBins) {
-        for (unsigned int jx = ix + 1; jx < nPix; jx++)
-          plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
-        continue;
+    const unsigned int nFinite = binStart[kPLSBins];
+    for (unsigned int k0 = blockIdx.x * kPLSCleanTile; k0 < nPix; k0 += gridDim.x * kPLSCleanTile) {
+      const unsigned int k = k0 + threadIdx.x;
+      bool active = k < nPix;
+      unsigned int ix = 0;
+      float eta1 = 0.f, phi1 = 0.f, score1 = 0.f;
+      unsigned int h1[4] = {0, 0, 0, 0};
+      int8_t quad1 = 0;
+      if (active) {
+        ix = order[k];
+        eta1 = s.eta[ix];
+        phi1 = s.phi[ix];
+        score1 = s.score[ix];
+        quad1 = s.isQuad[ix];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+          h1[a] = s.pLSHitsIdxs[4 * ix + a];
+        if (secondpass && (!quad1 || (s.isDup[ix] & 1)))
+          active = false;
       }
-      const int b0 = b >= kPLSBinReach ? b - kPLSBinReach : 0;
-      const int b1 = b + kPLSBinReach < kPLSBins ? b + kPLSBinReach : kPLSBins - 1;
-      for (unsigned int k = binStart[b0]; k < binStart[b1 + 1]; ++k) {
-        unsigned int jx = order[k];
-        if (jx > ix)
-          plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
+      // Sorted positions to stream: [lo, hi) then [nFinite, nPix).
+      const unsigned int kLast = min(k0 + kPLSCleanTile, nPix) - 1;
+      unsigned int lo = 0, hi = nPix, lo2 = nPix;
+      if (kLast < nFinite) {
+        const int bFirst = plsEtaBin(s.eta[order[k0]]), bLast = plsEtaBin(s.eta[order[kLast]]);
+        lo = binStart[bFirst >= kPLSBinReach ? bFirst - kPLSBinReach : 0];
+        hi = binStart[(bLast + kPLSBinReach < kPLSBins ? bLast + kPLSBinReach : kPLSBins - 1) + 1];
+        lo2 = nFinite;
       }
-      for (unsigned int k = binStart[kPLSBins]; k < binStart[kPLSBins + 1]; ++k) {
-        unsigned int jx = order[k];
-        if (jx > ix)
-          plsPair(ev, ix, jx, phits1, eta_pix1, phi_pix1, secondpass);
+      const unsigned int span = (hi - lo) + (nPix - lo2);
+      for (unsigned int t0 = 0; t0 < span; t0 += kPLSCleanTile) {
+        __syncthreads();
+        const unsigned int t = t0 + threadIdx.x;
+        if (t < span) {
+          const unsigned int pos = t < hi - lo ? lo + t : lo2 + (t - (hi - lo));
+          const unsigned int jx = order[pos];
+          sT.idx[threadIdx.x] = jx;
+          sT.eta[threadIdx.x] = s.eta[jx];
+          sT.phi[threadIdx.x] = s.phi[jx];
+          sT.score[threadIdx.x] = s.score[jx];
+          sT.quad[threadIdx.x] = s.isQuad[jx];
+          sT.dup[threadIdx.x] = s.isDup[jx];
+          sT.hits[threadIdx.x] = make_uint4(s.pLSHitsIdxs[4 * jx], s.pLSHitsIdxs[4 * jx + 1], s.pLSHitsIdxs[4 * jx + 2],
+                                            s.pLSHitsIdxs[4 * jx + 3]);
+        }
+        __syncthreads();
+        if (!active)
+          continue;
+        const unsigned int nt = min(span - t0, unsigned(kPLSCleanTile));
+        for (unsigned int u = 0; u < nt; ++u) {
+          const unsigned int jx = sT.idx[u];
+          if (jx <= ix)
+            continue;
+          const float eta2 = sT.eta[u];
+          if (fabs_(eta2 - eta1) > 0.1f)
+            continue;
+          if (secondpass && (!sT.quad[u] || (sT.dup[u] & 1)))
+            continue;
+          const int8_t quad_diff = quad1 - sT.quad[u];
+          const float score_diff = score1 - sT.score[u];
+          unsigned int idxToRemove;
+          if (quad_diff > 0)
+            idxToRemove = jx;
+          else if (quad_diff < 0)
+            idxToRemove = ix;
+          else if (score_diff < 0)
+            idxToRemove = jx;
+          else if (score_diff > 0)
+            idxToRemove = ix;
+          else
+            idxToRemove = ix;
+          const uint4 h2 = sT.hits[u];
+          int npMatched = 0;
+          for (int a = 0; a < 4; a++) {
+            const bool pmatched = h1[a] == h2.x || h1[a] == h2.y || h1[a] == h2.z || h1[a] == h2.w;
+            if (pmatched) {
+              npMatched++;
+              if (secondpass)
+                break;
+            }
+          }
+          bool remove = npMatched >= 3;
+          if (secondpass) {
+            const float dEta = fabs_(eta1 - eta2);
+            const float dPhi = wrapDPhi(phi1, sT.phi[u]);
+            const float dR2 = dEta * dEta + dPhi * dPhi;
+            if ((npMatched >= 1) || (dR2 < 1e-5f))
+              remove = true;
+          }
+          if (remove) {
+            if (secondpass)
+              ev.plsFlag[idxToRemove] = 1;
+            else
+              s.isDup[idxToRemove] = 1;
+          }
+        }
       }
     }
   }
@@ -1876,58 +1958,57 @@ namespace lst {
   }
 
   // Shared pixel and outer hits of two pT3s (SDL/Kernels.h:138-200).
-  LST_DEV void sharedHitsPT3(const PixelTriplets& p, unsigned int ix, unsigned int jx, int& npMatched, int& nMatched) {
-    npMatched = 0;
-    for (int i = 0; i < 4; i++) {
-      int a = static_cast<int>(p.hitIndices[10 * ix + i]);
-      bool pm = false;
-      for (int j = 0; j < 4; j++)
-        if (a == static_cast<int>(p.hitIndices[10 * jx + j])) {
-          pm = true;
-          break;
-        }
-      if (pm)
-        npMatched++;
-    }
-    nMatched = 0;
-    for (int i = 0; i < 6; i++) {
-      int a = static_cast<int>(p.hitIndices[10 * ix + 4 + i]);
-      bool tm = false;
-      for (int j = 0; j < 6; j++)
-        if (a == static_cast<int>(p.hitIndices[10 * jx + 4 + j])) {
-          tm = true;
-          break;
-        }
-      if (tm)
-        nMatched++;
-    }
-  }
-
-  // SDL/Kernels.h:325-356
+  // SDL/Kernels.h:325-356.  pT3 ix is removed as soon as one jx meets the
+  // condition (the reference's loop breaks there), so the outcome is the OR of
+  // the condition over jx: one warp per ix, its lanes over jx.
   __global__ void kPT3Dedup(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt3.nPixelTriplets;
     PixelTriplets p = ev.pt3;
-    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < n; ix += gridDim.x * blockDim.x) {
-      for (unsigned int jx = 0; jx < n; jx++) {
-        if (ix == jx)
-          continue;
-        int np, nm;
-        sharedHitsPT3(p, ix, jx, np, nm);
-        if ((np + nm) >= 5) {
-          uint8_t li = p.logicalLayers[5 * ix + 2], lj = p.logicalLayers[5 * jx + 2];
-          if (lj < li) {
-            p.isDup[ix] = 1;
-            break;
-          } else if (li == lj && p.score[ix] > p.score[jx]) {
-            p.isDup[ix] = 1;
-            break;
-          } else if (li == lj && (p.score[ix] == p.score[jx]) && (ix < jx)) {
-            p.isDup[ix] = 1;
-            break;
+    const unsigned int wpb = blockDim.x >> 5;
+    for (unsigned int ix = blockIdx.x * wpb + (threadIdx.x >> 5); ix < n; ix += gridDim.x * wpb) {
+      unsigned int mine[10];
+#pragma unroll
+      for (int i = 0; i < 10; ++i)
+        mine[i] = p.hitIndices[10 * ix + i];
+      const uint8_t li = p.logicalLayers[5 * ix + 2];
+      const float scoreI = p.score[ix];
+      bool dup = false;
+      for (unsigned int j0 = 0; j0 < n && !dup; j0 += 32) {
+        const unsigned int jx = j0 + laneId();
+        bool c = false;
+        if (jx < n && jx != ix) {
+          unsigned int other[10];
+#pragma unroll
+          for (int i = 0; i < 10; ++i)
+            other[i] = p.hitIndices[10 * jx + i];
+          int np = 0, nm = 0;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            bool m = false;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+              m |= mine[a] == other[b];
+            np += m ? 1 : 0;
+          }
+#pragma unroll
+          for (int a = 4; a < 10; ++a) {
+            bool m = false;
+#pragma unroll
+            for (int b = 4; b < 10; ++b)
+              m |= mine[a] == other[b];
+            nm += m ? 1 : 0;
+          }
+          if (np + nm >= 5) {
+            const uint8_t lj = p.logicalLayers[5 * jx + 2];
+            const float scoreJ = p.score[jx];
+            c = lj < li || (li == lj && scoreI > scoreJ) || (li == lj && scoreI == scoreJ && ix < jx);
           }
         }
+        dup = __any_sync(kFullMask, c);
       }
+      if (dup && laneId() == 0)
+        p.isDup[ix] = 1;
     }
   }
 
