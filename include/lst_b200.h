@@ -154,8 +154,10 @@ int lst_event_set_t5_method(lst_event* ev, int method);
 
 /* The quintuplet and pixel stages evaluate their candidates as flat lists and
  * fall back to one warp per module / pLS for events whose candidates overflow
- * the list buffers.  on = 1 makes every event take the fallback (same
- * results; for testing it). */
+ * the list buffers; the duplicate-removal and cross-cleaning kernels fall back
+ * to pair-by-pair tests for events whose objects overflow their shared-memory
+ * staging.  on = 1 makes every event take the fallbacks (same results; for
+ * testing them). */
 int lst_event_set_walk(lst_event* ev, int on);
 
 /* Event::resetEvent (SDL/Event.cc:45): clears slot `slot`'s objects.  Adding

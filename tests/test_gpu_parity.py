@@ -154,8 +154,10 @@ def test_batched_uneven_events_match_reference(ref, es):
 
 
 def test_fallback_walks_match_reference(ref, es):
-    """The warp-per-module / per-pLS walks (taken for overflowing events) give
-    the same objects as the candidate lists."""
+    """The fallbacks taken for overflowing events -- the warp-per-module /
+    per-pLS walks instead of the candidate lists, and the pair-by-pair
+    duplicate-removal and pLS cross-cleaning tests instead of the shared-memory
+    staged ones -- give the reference's objects."""
     inp = gen.generate_event(2, 3)
     ev = lst.Event(es, max_hits=inp.n_hits + 1024)
     ev.event_set.set_walk(True)

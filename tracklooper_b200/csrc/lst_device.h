@@ -121,7 +121,7 @@ namespace lst {
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
     unsigned int maxHits;
-    unsigned int forceWalk;  // take the warp-per-object walks instead of the candidate lists
+    unsigned int forceWalk;  // take the fallback paths (walks, pair-by-pair tests) for testing them
   };
 
 }  // namespace lst

@@ -49,13 +49,14 @@ namespace {
   // launch is rejected.
   // With profiling on, each launch is bracketed by two CUDA events on the
   // same stream (see lst_event_set_profiling).
-#define LST_LAUNCH(kernel, grid, block, ...)                   \
+#define LST_LAUNCH(kernel, grid, block, ...) LST_LAUNCH_SMEM(kernel, grid, block, 0, __VA_ARGS__)
+#define LST_LAUNCH_SMEM(kernel, grid, block, smem, ...)        \
   do {                                                         \
     cudaGetLastError(); /* drop a stale non-sticky error */    \
     cudaEvent_t p0_ = nullptr;                                 \
     if (ev->profiling && (p0_ = profEvent(ev)))                \
       cudaEventRecord(p0_, s);                                 \
-    kernel<<<(grid), (block), 0, s>>>(__VA_ARGS__);            \
+    kernel<<<(grid), (block), (smem), s>>>(__VA_ARGS__);       \
     cudaError_t e_ = cudaGetLastError();                       \
     if (e_ != cudaSuccess)                                     \
       return cudaFail(e_, #kernel);                            \
@@ -437,6 +438,7 @@ namespace {
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 0);
         LST_LAUNCH(lst::kPT5Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
+        LST_LAUNCH_SMEM(lst::kPT5DedupSorted, dim3(1, count), 1024, lst::kPT5DedupSmem, d, v);
         LST_LAUNCH(lst::kPT5Dedup, dim3(blocksFor(lst::kMaxPixelQuintuplets, count, lst::kDedupTile), count),
                    lst::kDedupTile, d, v);
         LST_LAUNCH(lst::kAddPT5TC, one, 1024, d, v);
@@ -469,7 +471,7 @@ namespace {
                    true);
         LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kTCCleanInfo, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, d, v);
-        LST_LAUNCH(lst::kCrossCleanPLS, dim3(blocksFor(P, count, lst::kCleanTile), count), lst::kCleanTile, d, v);
+        LST_LAUNCH_SMEM(lst::kCrossCleanPLS, dim3(lst::kXCleanBlocksPerEvent, count), 1024, lst::kXCleanSmem, d, v);
         LST_LAUNCH(lst::kAddPLSTC, one, 1024, d, v);
         break;
       }
@@ -569,6 +571,7 @@ namespace {
         {"kPT5Emit", (const void*)lst::kPT5Emit},
         {"kPLSScan", (const void*)lst::kPLSScan},
         {"kPT5Dedup", (const void*)lst::kPT5Dedup},
+        {"kPT5DedupSorted", (const void*)lst::kPT5DedupSorted},
         {"kAddPT5TC", (const void*)lst::kAddPT5TC},
         {"kPT3Count", (const void*)lst::kPT3Count},
         {"kPT3Emit", (const void*)lst::kPT3Emit},
@@ -795,6 +798,11 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
                     lst::kMaxPixelQuintuplets,
                     lst::kMaxTrackCandidates};
   LST_CUDA(cudaSetDevice(es->device));
+  // Kernels whose shared memory exceeds the 48 KB default opt in (per device).
+  LST_CUDA(cudaFuncSetAttribute(lst::kCrossCleanPLS, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(lst::kXCleanSmem)));
+  LST_CUDA(cudaFuncSetAttribute(lst::kPT5DedupSorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(lst::kPT5DedupSmem)));
   Carver measure;
   lst::EventView tmp{};
   carveEvent(measure, tmp, ev->sizes);

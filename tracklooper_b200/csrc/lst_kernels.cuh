@@ -1116,7 +1116,7 @@ namespace lst {
         const uint16_t lm = sMods[k];
         const unsigned int n = q.nQuintuplets[lm];
         const unsigned int base = ev.rg.quintupletModuleIndices[lm];
-        const bool staged = n <= kT5DedupStage;
+        const bool staged = n <= kT5DedupStage && !ev.forceWalk;
         if (staged) {
           for (unsigned int t = threadIdx.x; t < n; t += blockDim.x) {
             sEta[t] = q.eta[base + t];
@@ -1521,12 +1521,114 @@ namespace lst {
   // higher index is dropped).  The other candidates' hits are staged in
   // shared memory 128 at a time; the outcome per pT5 is an "any" over the
   // others, so the visiting order does not matter.
+  // pT5 duplicate removal (SDL/Kernels.h:356-382): pT5 ix is removed if some
+  // jx shares at least 7 of its 14 hit slots and has a lower score (ties: the
+  // higher index goes).  The outcome is an OR over jx, and a pair sharing 7
+  // slots shares at least one hit, so only pairs that meet in some hit need the
+  // full test.  kPT5DedupSorted (one block per event) sorts the event's
+  // (hit, pT5) entries in shared memory and tests each entry against the other
+  // pT5s of its hit; an event with more than kPT5DedupMaxN pT5s is left to
+  // kPT5Dedup, which tests every pair in shared-memory tiles.
+  constexpr unsigned int kPT5DedupMaxEntries = 16384;
+  constexpr unsigned int kPT5DedupMaxN = kPT5DedupMaxEntries / 14;
+  constexpr size_t kPT5DedupSmem = kPT5DedupMaxEntries * sizeof(unsigned long long) +
+                                   kPT5DedupMaxN * 14 * sizeof(unsigned int) + kPT5DedupMaxN * sizeof(float) +
+                                   kPT5DedupMaxN;
+
+  __global__ void __launch_bounds__(1024) kPT5DedupSorted(DeviceES es, const EventView* evs) {
+    extern __shared__ __align__(16) unsigned char psm[];
+    unsigned long long* sKey = reinterpret_cast<unsigned long long*>(psm);
+    unsigned int* sHits = reinterpret_cast<unsigned int*>(sKey + kPT5DedupMaxEntries);
+    float* sScore = reinterpret_cast<float*>(sHits + kPT5DedupMaxN * 14);
+    unsigned char* sDup = reinterpret_cast<unsigned char*>(sScore + kPT5DedupMaxN);
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = *ev.pt5.nPixelQuintuplets;
+    if (n < 2 || n > kPT5DedupMaxN || ev.forceWalk)
+      return;
+    PixelQuintuplets p = ev.pt5;
+    const unsigned int E = 14 * n;
+    unsigned int N = 1;
+    while (N < E)
+      N <<= 1;
+    for (unsigned int t = threadIdx.x; t < N; t += blockDim.x) {
+      if (t < E) {
+        const unsigned int h = p.hitIndices[t];
+        sHits[t] = h;
+        sKey[t] = (static_cast<unsigned long long>(h) << 16) | (t / 14);
+      } else {
+        sKey[t] = ~0ull;
+      }
+    }
+    for (unsigned int t = threadIdx.x; t < n; t += blockDim.x) {
+      sScore[t] = p.score[t];
+      sDup[t] = 0;
+    }
+    __syncthreads();
+    // Bitonic sort of sKey[0, N).
+    for (unsigned int k = 2; k <= N; k <<= 1) {
+      for (unsigned int j = k >> 1; j > 0; j >>= 1) {
+        for (unsigned int i = threadIdx.x; i < N; i += blockDim.x) {
+          const unsigned int l = i ^ j;
+          if (l > i) {
+            const unsigned long long a = sKey[i], b = sKey[l];
+            if (((i & k) == 0) == (a > b)) {
+              sKey[i] = b;
+              sKey[l] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (unsigned int e = threadIdx.x; e < E; e += blockDim.x) {
+      const unsigned int a = e / 14;
+      const unsigned long long h = sHits[e];
+      // first entry of this hit
+      unsigned int lo = 0, hi = E;
+      while (lo < hi) {
+        const unsigned int mid = (lo + hi) >> 1;
+        if ((sKey[mid] >> 16) < h)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      const float score1 = sScore[a];
+      for (unsigned int q = lo; q < E && (sKey[q] >> 16) == h; ++q) {
+        if (sDup[a])
+          break;
+        const unsigned int b = static_cast<unsigned int>(sKey[q] & 0xffffu);
+        if (b == a)
+          continue;
+        const float score2 = sScore[b];
+        if (!(score1 > score2 or ((score1 == score2) and (a > b))))
+          continue;
+        const unsigned int* mine = sHits + 14 * a;
+        const unsigned int* other = sHits + 14 * b;
+        int nMatched = 0;
+        for (int i = 0; i < 14; ++i) {
+          bool matched = false;
+          for (int j = 0; j < 14; ++j)
+            matched |= (mine[i] == other[j]);
+          nMatched += matched ? 1 : 0;
+        }
+        if (nMatched >= 7)
+          sDup[a] = 1;
+      }
+    }
+    __syncthreads();
+    for (unsigned int t = threadIdx.x; t < n; t += blockDim.x)
+      if (sDup[t])
+        p.isDup[t] = 1;
+  }
+
   constexpr int kDedupTile = 128;
   __global__ void __launch_bounds__(kDedupTile) kPT5Dedup(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sHits[kDedupTile * 14];
     __shared__ float sScore[kDedupTile];
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt5.nPixelQuintuplets;
+    if (n <= kPT5DedupMaxN && !ev.forceWalk)
+      return;  // kPT5DedupSorted has done this event
     PixelQuintuplets p = ev.pt5;
     for (unsigned int ixBase = blockIdx.x * kDedupTile; ixBase < n; ixBase += gridDim.x * kDedupTile) {
       const unsigned int ix = ixBase + threadIdx.x;
@@ -2316,58 +2418,162 @@ namespace lst {
     }
   }
 
-  // pLS vs existing TCs (SDL/TrackCandidate.h:302-381); the TC records are
-  // staged in shared memory 128 at a time.
-  constexpr int kCleanTile = 128;
-  __global__ void __launch_bounds__(kCleanTile) kCrossCleanPLS(DeviceES es, const EventView* evs) {
-    __shared__ TCCleanInfo sInfo[kCleanTile];
+  // pLS vs existing TCs (SDL/TrackCandidate.h:302-381).  A quadruplet pLS
+  // that is not yet a duplicate becomes one if some TC of type 5 or 7 shares a
+  // pixel hit with it, if some T5 TC (type 4) lies within dR^2 < 1e-3, or if
+  // some type 5 / 7 TC lies within dR^2 < 1e-6; the outcome is an OR over the
+  // TCs, so it is evaluated per pLS without walking every TC:
+  //  - the pixel hits of all type 5 / 7 TCs go into a shared-memory hash set,
+  //    and a pLS shares a hit with one of them iff one of its hits is in it;
+  //  - the TCs are counting-sorted by eta into the pLS-cleaning bins (width
+  //    0.02), and only bins within kXCleanReach of the pLS's bin are read:
+  //    dR^2 < 1e-3 needs |deta| < 0.0317 (two bin widths plus rounding), and a
+  //    non-finite eta or dR^2 never passes the test.
+  // A set with more TCs than kXCleanMaxTC, or more hits than the hash holds,
+  // is checked pair by pair instead.
+  constexpr unsigned int kXCleanHashSlots = 1u << 14;
+  constexpr unsigned int kXCleanMaxTC = 4096;
+  constexpr int kXCleanReach = 3;
+  constexpr int kXCleanBlocksPerEvent = 4;
+  constexpr size_t kXCleanSmem =
+      kXCleanHashSlots * 4 + 2 * (kPLSBins + 2) * 4 + kXCleanMaxTC * (sizeof(float) * 2 + sizeof(int));
+
+  LST_DEV unsigned int xcleanSlot(unsigned int key) { return (key * 2654435761u) >> 18; }
+
+  LST_DEV bool xcleanPairDup(const TCCleanInfo& info, const int* phits1, float eta1, float phi1) {
+    if (info.type == 4) {
+      float dEta = fabs_(eta1 - info.eta);
+      float dPhi = wrapDPhi(phi1, info.phi);
+      return dEta * dEta + dPhi * dPhi < 1e-3f;
+    }
+    if (info.type == 5 || info.type == 7) {
+      if (sharedPixelHits(phits1, info.hits) > 0)
+        return true;
+      float dEta = fabs_(eta1 - info.eta);
+      float dPhi = wrapDPhi(phi1, info.phi);
+      return dEta * dEta + dPhi * dPhi < 0.000001f;
+    }
+    return false;
+  }
+
+  __global__ void __launch_bounds__(1024) kCrossCleanPLS(DeviceES es, const EventView* evs) {
+    extern __shared__ __align__(16) unsigned char xsm[];
+    unsigned int* sHash = reinterpret_cast<unsigned int*>(xsm);
+    unsigned int* sBinStart = sHash + kXCleanHashSlots;
+    unsigned int* sCursor = sBinStart + kPLSBins + 2;
+    float* sEta = reinterpret_cast<float*>(sCursor + kPLSBins + 2);
+    float* sPhi = sEta + kXCleanMaxTC;
+    int* sType = reinterpret_cast<int*>(sPhi + kXCleanMaxTC);
+    __shared__ unsigned int sOverflow;
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nPix = ev.ls.nSegments[es.pixelModule];
     const unsigned int prefix = es.lsOffset[es.nLowerModules];
     const unsigned int nTC = *ev.tc.nTrackCandidates;
+    const TCCleanInfo* infos = ev.tcCleanInfo;
     Segments s = ev.ls;
-    for (unsigned int iBase = blockIdx.x * kCleanTile; iBase < nPix; iBase += gridDim.x * kCleanTile) {
-      const unsigned int i = iBase + threadIdx.x;
-      const bool active = i < nPix && s.isQuad[i] && !s.isDup[i];
-      int phits1[4] = {-1, -1, -1, -1};
-      float eta1 = 0.f, phi1 = 0.f;
-      if (active) {
-        pixelHitsOf(s, ev.md, ev.hits, prefix + i, phits1);
-        eta1 = s.eta[i];
-        phi1 = s.phi[i];
-      }
-      bool dup = false;
-      for (unsigned int tBase = 0; tBase < nTC; tBase += kCleanTile) {
-        const unsigned int tile = (nTC - tBase < kCleanTile) ? nTC - tBase : kCleanTile;
-        __syncthreads();
-        if (threadIdx.x < tile)
-          sInfo[threadIdx.x] = ev.tcCleanInfo[tBase + threadIdx.x];
-        __syncthreads();
-        if (!active || dup)
-          continue;
-        for (unsigned int k = 0; k < tile; ++k) {
-          const TCCleanInfo& info = sInfo[k];
-          if (info.type == 4) {
-            float dEta = fabs_(eta1 - info.eta);
-            float dPhi = wrapDPhi(phi1, info.phi);
-            if (dEta * dEta + dPhi * dPhi < 1e-3f)
-              dup = true;
-          } else if (info.type == 5 || info.type == 7) {
-            if (sharedPixelHits(phits1, info.hits) > 0)
-              dup = true;
-            float dEta = fabs_(eta1 - info.eta);
-            float dPhi = wrapDPhi(phi1, info.phi);
-            if (dEta * dEta + dPhi * dPhi < 0.000001f)
-              dup = true;
+
+    if (threadIdx.x == 0)
+      sOverflow = (nTC > kXCleanMaxTC || ev.forceWalk) ? 1u : 0u;
+    for (unsigned int t = threadIdx.x; t < kXCleanHashSlots; t += blockDim.x)
+      sHash[t] = 0;
+    for (unsigned int t = threadIdx.x; t < kPLSBins + 2; t += blockDim.x)
+      sCursor[t] = 0;
+    __syncthreads();
+    const bool fits = nTC <= kXCleanMaxTC;
+    if (fits) {
+      for (unsigned int t = threadIdx.x; t < nTC; t += blockDim.x) {
+        const TCCleanInfo info = infos[t];
+        if (info.type == 5 || info.type == 7) {
+          for (int a = 0; a < 4; ++a) {
+            if (info.hits[a] == -1)
+              continue;
+            const unsigned int key = static_cast<unsigned int>(info.hits[a]) + 1u;
+            unsigned int slot = xcleanSlot(key), probes = 0;
+            while (true) {
+              const unsigned int old = atomicCAS(&sHash[slot], 0u, key);
+              if (old == 0u || old == key)
+                break;
+              if (++probes == kXCleanHashSlots) {
+                sOverflow = 1;
+                break;
+              }
+              slot = (slot + 1) & (kXCleanHashSlots - 1);
+            }
           }
         }
+        if (info.type == 4 || info.type == 5 || info.type == 7)
+          atomicAdd(&sCursor[plsEtaBin(info.eta)], 1u);
       }
-      if (active && dup)
+    }
+    __syncthreads();
+    const bool fast = sOverflow == 0;
+    if (fast) {
+      unsigned int tot;
+      const unsigned int c = threadIdx.x <= kPLSBins ? sCursor[threadIdx.x] : 0u;
+      const unsigned int ex = blockExclusiveScan(c, tot);
+      if (threadIdx.x <= kPLSBins) {
+        sBinStart[threadIdx.x] = ex;
+        sCursor[threadIdx.x] = ex;
+      }
+      if (threadIdx.x == 0)
+        sBinStart[kPLSBins + 1] = tot;
+      __syncthreads();
+      for (unsigned int t = threadIdx.x; t < nTC; t += blockDim.x) {
+        const TCCleanInfo& info = infos[t];
+        if (info.type == 4 || info.type == 5 || info.type == 7) {
+          const unsigned int pos = atomicAdd(&sCursor[plsEtaBin(info.eta)], 1u);
+          sEta[pos] = info.eta;
+          sPhi[pos] = info.phi;
+          sType[pos] = info.type;
+        }
+      }
+      __syncthreads();
+    }
+
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPix; i += gridDim.x * blockDim.x) {
+      if (!s.isQuad[i] || s.isDup[i])
+        continue;
+      int phits1[4];
+      pixelHitsOf(s, ev.md, ev.hits, prefix + i, phits1);
+      const float eta1 = s.eta[i], phi1 = s.phi[i];
+      bool dup = false;
+      if (fast) {
+        for (int a = 0; a < 4 && !dup; ++a) {
+          if (phits1[a] == -1)
+            continue;
+          const unsigned int key = static_cast<unsigned int>(phits1[a]) + 1u;
+          unsigned int slot = xcleanSlot(key);
+          for (unsigned int probes = 0; probes < kXCleanHashSlots; ++probes) {
+            const unsigned int h = sHash[slot];
+            if (h == key) {
+              dup = true;
+              break;
+            }
+            if (h == 0u)
+              break;
+            slot = (slot + 1) & (kXCleanHashSlots - 1);
+          }
+        }
+        const int b = plsEtaBin(eta1);
+        if (!dup && b < kPLSBins) {
+          const int b0 = b >= kXCleanReach ? b - kXCleanReach : 0;
+          const int b1 = b + kXCleanReach < kPLSBins ? b + kXCleanReach : kPLSBins - 1;
+          for (unsigned int k = sBinStart[b0]; k < sBinStart[b1 + 1] && !dup; ++k) {
+            float dEta = fabs_(eta1 - sEta[k]);
+            float dPhi = wrapDPhi(phi1, sPhi[k]);
+            const float dR2 = dEta * dEta + dPhi * dPhi;
+            dup = sType[k] == 4 ? dR2 < 1e-3f : dR2 < 0.000001f;
+          }
+        }
+      } else {
+        for (unsigned int t = 0; t < nTC && !dup; ++t)
+          dup = xcleanPairDup(infos[t], phits1, eta1, phi1);
+      }
+      if (dup)
         s.isDup[i] = 1;
     }
   }
 
-  // pLS -> TC (SDL/TrackCandidate.h:489-529, quadruplets only); one block per event.
   __global__ void __launch_bounds__(1024) kAddPLSTC(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = ev.ls.nSegments[es.pixelModule];
