@@ -358,6 +358,28 @@ typedef struct lst_kernel_time {
 int lst_event_set_profiling(lst_event* ev, int on);
 int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int* n_kernels);
 
+/* ---------------------------------------------------------- autotuner */
+/* No reference counterpart (the reference launches with fixed work
+ * divisions, SDL/Event.cc).  The kernels that do most of the work take their
+ * launch shape from the event set: warps per block and resident blocks per
+ * SM across the batch (each event gets blocks_per_sm x SMs / events blocks).
+ * Object lists do not depend on the shape. */
+int lst_tune_kernel_count(void);
+const char* lst_tune_kernel_name(int k);
+int lst_event_set_launch_shape(lst_event* ev, int k, int warps_per_block, int blocks_per_sm);
+int lst_event_get_launch_shape(const lst_event* ev, int k, int* warps_per_block, int* blocks_per_sm);
+/* Hash of the loaded geometry (module map, connections, static arenas). */
+uint64_t lst_es_geometry_hash(const lst_es* es);
+/* Times a sweep of launch shapes (1-8 warps per block x 8-64 blocks per SM)
+ * on slots [first, first + count), whose inputs must be resident from the
+ * last upload, keeps the fastest shape per kernel, and checks that every
+ * shape gave the same object counts.  With a cache path the result is stored
+ * there under a key of geometry hash, device name, batch size and library
+ * build, replacing an older entry of that key; lst_autotune_load applies the
+ * stored entry (1 if found, 0 if not). */
+int lst_autotune(lst_event* ev, int first, int count, const char* cache_path);
+int lst_autotune_load(lst_event* ev, int count, const char* cache_path);
+
 /* ---------------------------------------------------------- T5 classifier */
 /* Classifier-stage probe (no reference counterpart; it serves retraining the
  * T5 DNN of SDL/NeuralNetwork.h): after createQuintuplets, every quintuplet

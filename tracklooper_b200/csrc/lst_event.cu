@@ -15,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <sstream>
 #include <string>
 #include <tuple>
 #include <type_traits>
@@ -268,6 +269,28 @@ namespace {
   };
 }  // namespace
 
+namespace {
+  // Kernels whose launch shape the autotuner picks: warps per block and
+  // resident blocks per SM across the batch (the grid holds
+  // blocks_per_sm x SMs / events blocks per event).  Their results do not
+  // depend on the shape: each module / candidate is processed the same way by
+  // whichever warp takes it.
+  enum TunedKernel { kTuMD, kTuMDDerived, kTuLS, kTuT3, kTuT5Eval, kTuPix5, kTuPix3, kTuCount };
+  struct TuneSpec {
+    const char* name;  // as it appears in the launch profile
+    int maxWarps;      // the kernel's launch bounds / per-warp shared memory
+    int defWarps;
+  };
+  const TuneSpec kTuneSpecs[kTuCount] = {{"kCreateMD", 8, 8},   {"kMDDerived", 8, 8},   {"kCreateLS", 4, 4},
+                                         {"kCreateT3", 4, 4},   {"kT5Eval", 4, 4},      {"kPixEval<5>", 4, 4},
+                                         {"kPixEval<3>", 4, 4}};
+  constexpr int kDefaultBlocksPerSM = 16;
+  struct LaunchShape {
+    int warps = 4;
+    int perSM = kDefaultBlocksPerSM;
+  };
+}  // namespace
+
 struct lst_event {
   lst_es* es = nullptr;
   int device = 0;
@@ -282,6 +305,8 @@ struct lst_event {
   std::vector<lst::EventView> hv;
   lst::EventView* dv = nullptr;
   int t5Method = LST_T5_DNN;
+  int nSM = 148;
+  LaunchShape shape[kTuCount];
   // batched-input staging: the last upload's packed events (kind 0: the
   // Event-API layout of lst_batch_upload, 1: CMSSW seeds of
   // lst_batch_upload_seeds) for slots [inboxFirst, inboxFirst + inboxCount)
@@ -381,6 +406,23 @@ namespace {
     return dim3(blocksFor(nObjects * 32, count, 32u * warps), count);
   }
 
+  // Tuned warp-per-object kernel k over nObjects per event.
+  dim3 tunedWarpGrid(const lst_event* ev, int k, size_t nObjects, int count) {
+    const LaunchShape& sh = ev->shape[k];
+    const size_t want = std::max<size_t>(1, ceilDiv(nObjects, static_cast<size_t>(sh.warps)));
+    const size_t cap = std::max<size_t>(1, ceilDiv(static_cast<size_t>(sh.perSM) * ev->nSM,
+                                                   static_cast<size_t>(std::max(count, 1))));
+    return dim3(static_cast<unsigned int>(std::min(want, cap)), count);
+  }
+  // Tuned kernel k striding over a candidate list whose length only the device knows.
+  dim3 tunedFlatGrid(const lst_event* ev, int k, int count) {
+    const LaunchShape& sh = ev->shape[k];
+    const size_t blocks = std::max<size_t>(1, ceilDiv(static_cast<size_t>(sh.perSM) * ev->nSM,
+                                                      static_cast<size_t>(std::max(count, 1))));
+    return dim3(static_cast<unsigned int>(blocks), count);
+  }
+  unsigned int tunedThreads(const lst_event* ev, int k) { return 32u * static_cast<unsigned int>(ev->shape[k].warps); }
+
   int runStage(lst_event* ev, int first, int count, int stage) {
     const lst::DeviceES& d = ev->es->view;
     const lst::EventView* v = ev->dv + first;
@@ -390,18 +432,19 @@ namespace {
     const dim3 one(1, count);
     switch (stage) {
       case LST_STAGE_MINI_DOUBLETS:
-        LST_LAUNCH(lst::kCreateMD, warpGrid(nLower, 8, count), 256, d, v);
+        LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, nLower, count), tunedThreads(ev, kTuMD), d, v);
         LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
-        LST_LAUNCH(lst::kMDDerived, warpGrid(nLower + 1, 8, count), 256, d, v);
+        LST_LAUNCH(lst::kMDDerived, tunedWarpGrid(ev, kTuMDDerived, nLower + 1, count), tunedThreads(ev, kTuMDDerived),
+                   d, v);
         break;
       case LST_STAGE_SEGMENTS:
-        LST_LAUNCH(lst::kCreateLS, warpGrid(nLower, lst::kLSWarps, count), 32 * lst::kLSWarps, d, v);
+        LST_LAUNCH(lst::kCreateLS, tunedWarpGrid(ev, kTuLS, nLower, count), tunedThreads(ev, kTuLS), d, v);
         LST_LAUNCH(lst::kLSRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kLSByMD, warpGrid(nLower, lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
       case LST_STAGE_TRIPLETS:
         LST_LAUNCH(lst::kT3Offsets, one, 1024, d, v);
-        LST_LAUNCH(lst::kCreateT3, warpGrid(nLower, lst::kT3Warps, count), 32 * lst::kT3Warps, d, v);
+        LST_LAUNCH(lst::kCreateT3, tunedWarpGrid(ev, kTuT3, nLower, count), tunedThreads(ev, kTuT3), d, v);
         LST_LAUNCH(lst::kT3Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kT3ByMD, warpGrid(nLower, lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
@@ -412,7 +455,7 @@ namespace {
         LST_LAUNCH(lst::kT5Eligible, one, 1024, d, v);
         LST_LAUNCH(lst::kT5Prefix, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v);
         LST_LAUNCH(lst::kT5ModScan, one, 1024, d, v);
-        LST_LAUNCH(lst::kT5Eval, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v, useDnn);
+        LST_LAUNCH(lst::kT5Eval, tunedFlatGrid(ev, kTuT5Eval, count), tunedThreads(ev, kTuT5Eval), d, v, useDnn);
         if (useDnn)
           LST_LAUNCH(lst::kT5Dnn, dim3(blocksFor(lst::kT5DnnCap, count, 128), count), 128, d, v);
         LST_LAUNCH(lst::kT5Walk, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v,
@@ -433,7 +476,7 @@ namespace {
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kPixPrefix<5>, warpGrid(P, 8, count), 256, d, v);
         LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
-        LST_LAUNCH(lst::kPixEval<5>, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v);
+        LST_LAUNCH(lst::kPixEval<5>, tunedFlatGrid(ev, kTuPix5, count), tunedThreads(ev, kTuPix5), d, v);
         LST_LAUNCH(lst::kPixRankEmit<5>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 0);
@@ -447,7 +490,7 @@ namespace {
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kPixPrefix<3>, warpGrid(P, 8, count), 256, d, v);
         LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
-        LST_LAUNCH(lst::kPixEval<3>, dim3(2 * kResidentBlocks / std::max(count, 1) + 1, count), 128, d, v);
+        LST_LAUNCH(lst::kPixEval<3>, tunedFlatGrid(ev, kTuPix3, count), tunedThreads(ev, kTuPix3), d, v);
         LST_LAUNCH(lst::kPixRankEmit<3>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT3Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 1);
@@ -798,6 +841,9 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
                     lst::kMaxPixelQuintuplets,
                     lst::kMaxTrackCandidates};
   LST_CUDA(cudaSetDevice(es->device));
+  LST_CUDA(cudaDeviceGetAttribute(&ev->nSM, cudaDevAttrMultiProcessorCount, es->device));
+  for (int k = 0; k < kTuCount; ++k)
+    ev->shape[k].warps = kTuneSpecs[k].defWarps;
   // Kernels whose shared memory exceeds the 48 KB default opt in (per device).
   LST_CUDA(cudaFuncSetAttribute(lst::kCrossCleanPLS, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(lst::kXCleanSmem)));
@@ -1591,6 +1637,284 @@ int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int
     out[i] = acc[i];
   ev->profile.clear();
   ev->poolUsed = 0;
+  return 0;
+}
+
+}  // extern "C"
+
+// ================================================================ autotuner
+namespace {
+  // FNV-1a over the arrays that define the geometry and the static arenas.
+  template <typename T>
+  void fnv(uint64_t& h, const std::vector<T>& v) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(v.data());
+    for (size_t i = 0; i < v.size() * sizeof(T); ++i) {
+      h ^= p[i];
+      h *= 1099511628211ull;
+    }
+  }
+  uint64_t geometryHash(const lst_es* es) {
+    uint64_t h = 1469598103934665603ull;
+    const lst::EsHost& g = es->host;
+    fnv(h, g.detIds);
+    fnv(h, g.moduleMap);
+    fnv(h, g.nConnectedModules);
+    fnv(h, g.connectedPixels);
+    fnv(h, g.connectedPixelsIndex);
+    fnv(h, g.mdCap);
+    fnv(h, g.lsCap);
+    fnv(h, g.t3CapIfUsed);
+    fnv(h, g.t5CapIfEligible);
+    return h;
+  }
+
+  void dropGraphs(lst_event* ev) {
+    cudaStreamSynchronize(ev->stream);
+    for (auto& g : ev->graphs)
+      cudaGraphExecDestroy(g.second.exec);
+    ev->graphs.clear();
+  }
+
+  // Cache key: geometry, device, batch size and this build of the kernels
+  // (shapes tuned for one build need not suit another).
+  std::string tuneKey(const lst_event* ev, int count) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, ev->device);
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "g%016llx-d%s-n%d-b%s_%s", static_cast<unsigned long long>(geometryHash(ev->es)),
+                  prop.name, count, __DATE__, __TIME__);
+    std::string key(buf);
+    for (char& c : key)
+      if (c == ' ' || c == '\t')
+        c = '_';
+    return key;
+  }
+
+  std::string shapesLine(const lst_event* ev) {
+    std::string line;
+    for (int k = 0; k < kTuCount; ++k)
+      line += " " + std::string(kTuneSpecs[k].name) + "=" + std::to_string(ev->shape[k].warps) + "x" +
+              std::to_string(ev->shape[k].perSM);
+    return line;
+  }
+
+  // Parses the "name=WxP" fields of a cache line; false if malformed or incomplete.
+  bool parseShapes(const std::string& rest, LaunchShape* out) {
+    std::istringstream is(rest);
+    std::string tok;
+    int found = 0;
+    while (is >> tok) {
+      const size_t eq = tok.find('='), x = tok.rfind('x');
+      if (eq == std::string::npos || x == std::string::npos || x < eq)
+        return false;
+      const std::string name = tok.substr(0, eq);
+      int w = 0, p = 0;
+      try {
+        w = std::stoi(tok.substr(eq + 1, x - eq - 1));
+        p = std::stoi(tok.substr(x + 1));
+      } catch (...) {
+        return false;
+      }
+      for (int k = 0; k < kTuCount; ++k) {
+        if (name == kTuneSpecs[k].name) {
+          if (w < 1 || w > kTuneSpecs[k].maxWarps || p < 1 || p > 64)
+            return false;
+          out[k].warps = w;
+          out[k].perSM = p;
+          ++found;
+        }
+      }
+    }
+    return found == kTuCount;
+  }
+
+  // Per-kernel device time (ms) of the launches profiled since the last clear.
+  int collectProfile(lst_event* ev, std::map<std::string, double>& ms) {
+    LST_CUDA(cudaStreamSynchronize(ev->stream));
+    for (const ProfRecord& r : ev->profile) {
+      float t = 0.f;
+      LST_CUDA(cudaEventElapsedTime(&t, r.start, r.stop));
+      const char* name = r.kernel;
+      if (std::strncmp(name, "lst::", 5) == 0)
+        name += 5;
+      ms[name] += t;
+    }
+    ev->profile.clear();
+    ev->poolUsed = 0;
+    return 0;
+  }
+}  // namespace
+
+extern "C" {
+
+int lst_tune_kernel_count(void) { return kTuCount; }
+
+const char* lst_tune_kernel_name(int k) { return (k >= 0 && k < kTuCount) ? kTuneSpecs[k].name : nullptr; }
+
+int lst_event_set_launch_shape(lst_event* ev, int k, int warps_per_block, int blocks_per_sm) {
+  if (!ev)
+    return setError("null event set");
+  if (k < 0 || k >= kTuCount)
+    return setError("lst_event_set_launch_shape: no tunable kernel " + std::to_string(k));
+  if (warps_per_block < 1 || warps_per_block > kTuneSpecs[k].maxWarps)
+    return setError(std::string("lst_event_set_launch_shape: ") + kTuneSpecs[k].name + " takes 1.." +
+                    std::to_string(kTuneSpecs[k].maxWarps) + " warps per block");
+  if (blocks_per_sm < 1 || blocks_per_sm > 64)
+    return setError("lst_event_set_launch_shape: blocks per SM must be 1..64");
+  if (ev->shape[k].warps != warps_per_block || ev->shape[k].perSM != blocks_per_sm) {
+    dropGraphs(ev);
+    ev->shape[k].warps = warps_per_block;
+    ev->shape[k].perSM = blocks_per_sm;
+  }
+  return 0;
+}
+
+int lst_event_get_launch_shape(const lst_event* ev, int k, int* warps_per_block, int* blocks_per_sm) {
+  if (!ev || !warps_per_block || !blocks_per_sm)
+    return setError("lst_event_get_launch_shape: null argument");
+  if (k < 0 || k >= kTuCount)
+    return setError("lst_event_get_launch_shape: no tunable kernel " + std::to_string(k));
+  *warps_per_block = ev->shape[k].warps;
+  *blocks_per_sm = ev->shape[k].perSM;
+  return 0;
+}
+
+uint64_t lst_es_geometry_hash(const lst_es* es) { return es ? geometryHash(es) : 0; }
+
+int lst_autotune_load(lst_event* ev, int count, const char* cache_path) {
+  if (!ev || !cache_path)
+    return setError("lst_autotune_load: null argument");
+  std::ifstream in(cache_path);
+  if (!in)
+    return 0;
+  const std::string key = tuneKey(ev, count);
+  std::string line, found;
+  while (std::getline(in, line))
+    if (line.compare(0, key.size() + 1, key + " ") == 0)
+      found = line.substr(key.size() + 1);
+  if (found.empty())
+    return 0;
+  LaunchShape shapes[kTuCount];
+  if (!parseShapes(found, shapes))
+    return setError("lst_autotune_load: malformed entry for " + key + " in " + cache_path);
+  for (int k = 0; k < kTuCount; ++k) {
+    int rc = lst_event_set_launch_shape(ev, k, shapes[k].warps, shapes[k].perSM);
+    if (rc)
+      return rc;
+  }
+  return 1;
+}
+
+int lst_autotune(lst_event* ev, int first, int count, const char* cache_path) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (count == 0)
+    return 0;
+  if (!ev->inboxValid || first < ev->inboxFirst || first + count > ev->inboxFirst + ev->inboxCount)
+    return setError("lst_autotune: upload the calibration events into slots [first, first + count) first");
+  const bool wasProfiling = ev->profiling;
+  LaunchShape saved[kTuCount];
+  std::copy(ev->shape, ev->shape + kTuCount, saved);
+  auto restore = [&]() {
+    for (int k = 0; k < kTuCount; ++k)
+      lst_event_set_launch_shape(ev, k, saved[k].warps, saved[k].perSM);
+    ev->profiling = wasProfiling;
+    ev->profile.clear();
+    ev->poolUsed = 0;
+  };
+  std::vector<lst_counts> refCounts(count), counts(count);
+  ev->profiling = false;
+  if ((rc = ingestInbox(ev, first, count)) || (rc = lst_batch_run(ev, first, count, 1, 8)) ||
+      (rc = readCounts(ev, first, count, refCounts.data()))) {
+    restore();
+    return rc;
+  }
+  const int warpOpts[] = {1, 2, 4, 8};
+  const int perSMOpts[] = {8, 16, 32, 64};
+  struct Trial {
+    int w, p;
+  };
+  std::vector<Trial> trials;
+  for (int w : warpOpts)
+    for (int p : perSMOpts)
+      trials.push_back({w, p});
+  std::vector<std::vector<double>> best(kTuCount, std::vector<double>(trials.size(), 1e30));
+  for (int rep = 0; rep < 2; ++rep) {
+    for (size_t t = 0; t < trials.size(); ++t) {
+      for (int k = 0; k < kTuCount; ++k)
+        lst_event_set_launch_shape(ev, k, std::min(trials[t].w, kTuneSpecs[k].maxWarps), trials[t].p);
+      ev->profiling = false;
+      if ((rc = ingestInbox(ev, first, count))) {
+        restore();
+        return rc;
+      }
+      if (cudaStreamSynchronize(ev->stream) != cudaSuccess) {
+        restore();
+        return cudaFail(cudaGetLastError(), "lst_autotune");
+      }
+      ev->profile.clear();
+      ev->poolUsed = 0;
+      ev->profiling = true;
+      rc = lst_batch_run(ev, first, count, 1, 8);
+      std::map<std::string, double> ms;
+      if (!rc)
+        rc = collectProfile(ev, ms);
+      ev->profiling = false;
+      if (!rc)
+        rc = readCounts(ev, first, count, counts.data());
+      if (rc) {
+        restore();
+        return rc;
+      }
+      if (std::memcmp(counts.data(), refCounts.data(), sizeof(lst_counts) * count) != 0) {
+        restore();
+        return setError("lst_autotune: the object counts changed with the launch shape (" +
+                        std::to_string(trials[t].w) + " warps, " + std::to_string(trials[t].p) +
+                        " blocks per SM)");
+      }
+      for (int k = 0; k < kTuCount; ++k) {
+        if (trials[t].w > kTuneSpecs[k].maxWarps)
+          continue;  // this kernel ran the shape of another trial
+        auto it = ms.find(kTuneSpecs[k].name);
+        if (it != ms.end())
+          best[k][t] = std::min(best[k][t], it->second);
+      }
+    }
+  }
+  ev->profiling = wasProfiling;
+  for (int k = 0; k < kTuCount; ++k) {
+    size_t arg = 0;
+    for (size_t t = 1; t < trials.size(); ++t)
+      if (best[k][t] < best[k][arg])
+        arg = t;
+    if (best[k][arg] >= 1e30)  // never timed: keep the previous shape
+      lst_event_set_launch_shape(ev, k, saved[k].warps, saved[k].perSM);
+    else
+      lst_event_set_launch_shape(ev, k, trials[arg].w, trials[arg].p);
+  }
+  if (cache_path && *cache_path) {
+    const std::string key = tuneKey(ev, count);
+    std::vector<std::string> lines;
+    {
+      std::ifstream in(cache_path);
+      std::string line;
+      while (std::getline(in, line))
+        if (!line.empty() && line.compare(0, key.size() + 1, key + " ") != 0)
+          lines.push_back(line);
+    }
+    lines.push_back(key + shapesLine(ev));
+    const std::string tmp = std::string(cache_path) + ".tmp";
+    {
+      std::ofstream out(tmp, std::ios::trunc);
+      if (!out)
+        return setError(std::string("lst_autotune: cannot write ") + tmp);
+      for (const std::string& l : lines)
+        out << l << "\n";
+    }
+    if (std::rename(tmp.c_str(), cache_path) != 0)
+      return setError(std::string("lst_autotune: cannot replace ") + cache_path);
+  }
   return 0;
 }
 

@@ -325,7 +325,23 @@ namespace lst {
     }
   }
 
-  __global__ void __launch_bounds__(256, 2) kCreateMD(DeviceES es, const EventView* evs) {
+  // Register budgets of the cut kernels, as resident blocks per SM.  The cut
+  // kernels wait mostly on dependent loads, so they run faster with more warps
+  // resident even where the tighter budget spills a little; the values are
+  // the fastest of a sweep over 2..12 blocks on B200 (PU200 batches).
+#ifndef LST_LB_MD_B
+#define LST_LB_MD_B 2
+#endif
+#ifndef LST_LB_LST3_B
+#define LST_LB_LST3_B 8
+#endif
+#ifndef LST_LB_EVAL_B
+#define LST_LB_EVAL_B 10
+#endif
+#define LST_LB_MD 256, LST_LB_MD_B
+#define LST_LB_LST3 128, LST_LB_LST3_B
+#define LST_LB_EVAL 128, LST_LB_EVAL_B
+  __global__ void __launch_bounds__(LST_LB_MD) kCreateMD(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const int wpb = blockDim.x >> 5;
     for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < es.nLowerModules; w += gridDim.x * wpb) {
@@ -412,12 +428,13 @@ namespace lst {
     }
   }
 
-  __global__ void kCreateLS(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(LST_LB_LST3) kCreateLS(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kLSWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sOuter[kLSWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
-    for (int w = blockIdx.x * kLSWarps + wib; w < es.nLowerModules; w += gridDim.x * kLSWarps) {
+    const int wpb = blockDim.x >> 5;  // at most kLSWarps
+    for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
       __syncwarp();
       lsModule(es, ev, static_cast<uint16_t>(w), sPre[wib], sOuter[wib]);
     }
@@ -618,11 +635,12 @@ namespace lst {
     }
   }
 
-  __global__ void kCreateT3(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(LST_LB_LST3) kCreateT3(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kT3Warps][kT3MaxInner + 1];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
-    for (int w = blockIdx.x * kT3Warps + wib; w < es.nLowerModules; w += gridDim.x * kT3Warps) {
+    const int wpb = blockDim.x >> 5;  // at most kT3Warps
+    for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
       __syncwarp();
       t3Module(es, ev, static_cast<uint16_t>(w), sPre[wib]);
     }
@@ -825,7 +843,7 @@ namespace lst {
     }
   }
 
-  __global__ void kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
+  __global__ void __launch_bounds__(LST_LB_EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow)
       return;
@@ -1938,7 +1956,7 @@ namespace lst {
   }
 
   template <int K>
-  __global__ void kPixEval(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(LST_LB_EVAL) kPixEval(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int total = ev.sc->pixCandTotal;
     const unsigned int plsBase = es.lsOffset[es.nLowerModules];

@@ -124,6 +124,13 @@ EXPORTS = (
     "lst_batch_upload_seeds",
     "lst_event_prepare_input",
     "lst_run",
+    "lst_tune_kernel_count",
+    "lst_tune_kernel_name",
+    "lst_event_set_launch_shape",
+    "lst_event_get_launch_shape",
+    "lst_es_geometry_hash",
+    "lst_autotune",
+    "lst_autotune_load",
 )
 
 
@@ -310,6 +317,15 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_batch_upload_seeds.argtypes = [vp, i32, i32, vp, sz, vp]
         lib.lst_event_prepare_input.argtypes = [vp, i32, ctypes.POINTER(SeedInputC)]
         lib.lst_run.argtypes = [vp, i32, ctypes.POINTER(SeedInputC), ctypes.POINTER(Output)]
+        lib.lst_tune_kernel_count.argtypes = []
+        lib.lst_tune_kernel_name.argtypes = [i32]
+        lib.lst_tune_kernel_name.restype = ctypes.c_char_p
+        lib.lst_event_set_launch_shape.argtypes = [vp, i32, i32, i32]
+        lib.lst_event_get_launch_shape.argtypes = [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        lib.lst_es_geometry_hash.argtypes = [vp]
+        lib.lst_es_geometry_hash.restype = ctypes.c_uint64
+        lib.lst_autotune.argtypes = [vp, i32, i32, ctypes.c_char_p]
+        lib.lst_autotune_load.argtypes = [vp, i32, ctypes.c_char_p]
         _lib = lib
         return lib
 
@@ -375,6 +391,9 @@ class ES:
     @property
     def handle(self):
         return self._h
+
+    def geometry_hash(self) -> int:
+        return int(library().lst_es_geometry_hash(self._h))
 
     def set_t5dnn_threshold(self, wp: float):
         _check(library().lst_es_set_t5dnn_threshold(self._h, float(wp)), "lst_es_set_t5dnn_threshold")
@@ -555,6 +574,32 @@ class EventSet:
         """lst_event_prepare_input: LST::prepareInput + addHitToEvent + addPixelSegmentToEvent."""
         c, keep = seed_struct(seeds)
         _check(library().lst_event_prepare_input(self._h, slot, ctypes.byref(c)), "lst_event_prepare_input")
+
+    # -- launch shapes and the autotuner
+    def launch_shapes(self) -> dict:
+        """{kernel: (warps per block, blocks per SM)} of the tunable kernels."""
+        lib = library()
+        out = {}
+        for k in range(lib.lst_tune_kernel_count()):
+            w, p = ctypes.c_int(), ctypes.c_int()
+            _check(lib.lst_event_get_launch_shape(self._h, k, ctypes.byref(w), ctypes.byref(p)),
+                   "lst_event_get_launch_shape")
+            out[lib.lst_tune_kernel_name(k).decode()] = (w.value, p.value)
+        return out
+
+    def set_launch_shape(self, kernel: str, warps_per_block: int, blocks_per_sm: int):
+        lib = library()
+        names = [lib.lst_tune_kernel_name(k).decode() for k in range(lib.lst_tune_kernel_count())]
+        _check(lib.lst_event_set_launch_shape(self._h, names.index(kernel), warps_per_block, blocks_per_sm),
+               "lst_event_set_launch_shape")
+
+    def autotune(self, first: int, count: int, cache_path: str | None = None):
+        """lst_autotune on the resident inputs of slots [first, first + count)."""
+        _check(library().lst_autotune(self._h, first, count, cache_path.encode() if cache_path else None),
+               "lst_autotune")
+
+    def autotune_load(self, count: int, cache_path: str) -> bool:
+        return bool(_check(library().lst_autotune_load(self._h, count, cache_path.encode()), "lst_autotune_load"))
 
     def ingest(self, first: int, count: int):
         _check(library().lst_batch_ingest(self._h, first, count), "lst_batch_ingest")
