@@ -233,6 +233,20 @@ def run_ours(args, rank, world, local, events):
         raise RuntimeError(f"events with input errors: {bad[:5]}")
     d2h_bytes = get_output()
 
+    # launch shapes: the cached autotuner entry for this geometry, device,
+    # batch size and build, or a fresh sweep on these (resident) events
+    tune_cache = os.environ.get("LST_TUNE_CACHE") or os.path.join(
+        os.path.expanduser("~"), ".cache", "tracklooper_b200", "autotune.txt")
+    os.makedirs(os.path.dirname(tune_cache), exist_ok=True)
+    t_tune = time.perf_counter()
+    tuned_from = "cache" if eset.autotune_load(B, tune_cache) else "sweep"
+    if tuned_from == "sweep":
+        eset.autotune(0, B, tune_cache)
+    tune_info = {"source": tuned_from, "seconds": round(time.perf_counter() - t_tune, 2),
+                 "shapes": {k: list(v) for k, v in eset.launch_shapes().items()},
+                 "geometry_hash": f"{es.geometry_hash():016x}"}
+    eset.upload_packed(0, blob, offsets)
+
     def batched_step():
         eset.ingest(0, B)
         eset.run_graph(0, B)
@@ -393,6 +407,7 @@ def run_ours(args, rank, world, local, events):
         "kernels": kernel_table,
         "objects_per_event": {k: round(v / B, 1) for k, v in agg.items() if k != "nLower"},
         "device_memory_gb": round(eset.memory_bytes() / 1e9, 2),
+        "autotune": tune_info,
         "l2": f"inputs larger than L2: {in_bytes / 1e6:.0f} MB of packed inputs per step plus the object arenas",
     }
     eset.close()

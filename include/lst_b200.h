@@ -370,7 +370,7 @@ int lst_event_set_launch_shape(lst_event* ev, int k, int warps_per_block, int bl
 int lst_event_get_launch_shape(const lst_event* ev, int k, int* warps_per_block, int* blocks_per_sm);
 /* Hash of the loaded geometry (module map, connections, static arenas). */
 uint64_t lst_es_geometry_hash(const lst_es* es);
-/* Times a sweep of launch shapes (1-8 warps per block x 8-64 blocks per SM)
+/* Times a sweep of launch shapes (1-8 warps per block x 16-128 blocks per SM)
  * on slots [first, first + count), whose inputs must be resident from the
  * last upload, keeps the fastest shape per kernel, and checks that every
  * shape gave the same object counts.  With a cache path the result is stored

@@ -42,7 +42,7 @@ def test_autotune_keeps_outputs_and_limits(es, events, tmp_path):
                   "kPixEval<3>": 4}
         assert set(shapes) == set(limits)
         for k, (w, p) in shapes.items():
-            assert 1 <= w <= limits[k] and 1 <= p <= 64, (k, w, p)
+            assert 1 <= w <= limits[k] and 1 <= p <= 256, (k, w, p)
         for graph in (False, True):
             after = _run(s, events, graph)
             for a, b in zip(before, after):

@@ -60,7 +60,8 @@ namespace lst {
     unsigned int pixPassCount;    // passing candidates found by kPixEval
     unsigned int pixFallback;     // the pixel stage overflowed the staging: walk instead
     unsigned int t5DnnCount;      // candidates buffered for kT5Dnn
-    unsigned int pad[3];
+    unsigned int pixQueueCount;   // candidates passing the pixel pre-selection
+    unsigned int pad[2];
   };
 
   // All device pointers of one event.
@@ -117,6 +118,7 @@ namespace lst {
     unsigned int* pixPassObj;   //   the T5 / T3 index
     unsigned int* pixPassPLS;   //   the pLS index
     float* pixPassV;            //   the selection values (8 per candidate)
+    unsigned int* pixQueue;     // candidates passing the pixel pre-selection (any order)
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)

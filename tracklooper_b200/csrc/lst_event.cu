@@ -476,6 +476,7 @@ namespace {
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kPixPrefix<5>, warpGrid(P, 8, count), 256, d, v);
         LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kPixPre<5>, dim3(blocksFor(size_t(1) << 20, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kPixEval<5>, tunedFlatGrid(ev, kTuPix5, count), tunedThreads(ev, kTuPix5), d, v);
         LST_LAUNCH(lst::kPixRankEmit<5>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
@@ -490,6 +491,7 @@ namespace {
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kPixPrefix<3>, warpGrid(P, 8, count), 256, d, v);
         LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kPixPre<3>, dim3(blocksFor(size_t(1) << 20, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kPixEval<3>, tunedFlatGrid(ev, kTuPix3, count), tunedThreads(ev, kTuPix3), d, v);
         LST_LAUNCH(lst::kPixRankEmit<3>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT3Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
@@ -607,6 +609,8 @@ namespace {
         {"kPixPrefix<3>", (const void*)lst::kPixPrefix<3>},
         {"kPixScan", (const void*)lst::kPixScan},
         {"kPixEval<5>", (const void*)lst::kPixEval<5>},
+        {"kPixPre<5>", (const void*)lst::kPixPre<5>},
+        {"kPixPre<3>", (const void*)lst::kPixPre<3>},
         {"kPixEval<3>", (const void*)lst::kPixEval<3>},
         {"kPixRankEmit<5>", (const void*)lst::kPixRankEmit<5>},
         {"kPixRankEmit<3>", (const void*)lst::kPixRankEmit<3>},
@@ -1717,7 +1721,7 @@ namespace {
       }
       for (int k = 0; k < kTuCount; ++k) {
         if (name == kTuneSpecs[k].name) {
-          if (w < 1 || w > kTuneSpecs[k].maxWarps || p < 1 || p > 64)
+          if (w < 1 || w > kTuneSpecs[k].maxWarps || p < 1 || p > 256)
             return false;
           out[k].warps = w;
           out[k].perSM = p;
@@ -1759,8 +1763,8 @@ int lst_event_set_launch_shape(lst_event* ev, int k, int warps_per_block, int bl
   if (warps_per_block < 1 || warps_per_block > kTuneSpecs[k].maxWarps)
     return setError(std::string("lst_event_set_launch_shape: ") + kTuneSpecs[k].name + " takes 1.." +
                     std::to_string(kTuneSpecs[k].maxWarps) + " warps per block");
-  if (blocks_per_sm < 1 || blocks_per_sm > 64)
-    return setError("lst_event_set_launch_shape: blocks per SM must be 1..64");
+  if (blocks_per_sm < 1 || blocks_per_sm > 256)
+    return setError("lst_event_set_launch_shape: blocks per SM must be 1..256");
   if (ev->shape[k].warps != warps_per_block || ev->shape[k].perSM != blocks_per_sm) {
     dropGraphs(ev);
     ev->shape[k].warps = warps_per_block;
@@ -1831,7 +1835,7 @@ int lst_autotune(lst_event* ev, int first, int count, const char* cache_path) {
     return rc;
   }
   const int warpOpts[] = {1, 2, 4, 8};
-  const int perSMOpts[] = {8, 16, 32, 64};
+  const int perSMOpts[] = {16, 32, 64, 128};
   struct Trial {
     int w, p;
   };

@@ -1860,6 +1860,7 @@ namespace lst {
   // Events with more passing candidates than the staging holds take the
   // per-pLS count/emit walk instead.
   constexpr unsigned int kPixPassCap = 8192;
+  constexpr unsigned int kPixQueueCap = 1u << 18;
   constexpr int kConnStride = kMaxConnectedModules + 1;
 
   template <int K>
@@ -1921,6 +1922,7 @@ namespace lst {
       ev.plsCandOff[n] = carry;
       ev.sc->pixCandTotal = carry;
       ev.sc->pixPassCount = 0;
+      ev.sc->pixQueueCount = 0;
     }
   }
 
@@ -1955,12 +1957,56 @@ namespace lst {
           (f - pre[klo]);
   }
 
+  // Pre-selection of the pT5 / pT3 candidates: the tests that come first in
+  // kPixEval (object not removed or used, the pLS-triplet radius criterion),
+  // which most candidates fail.  The survivors are queued in any order, so
+  // that kPixEval runs its long selection with all lanes of a warp busy; the
+  // outcome of a candidate does not depend on which thread evaluates it, and
+  // the passing ones are ranked by candidate index afterwards.  A full queue
+  // makes kPixEval evaluate every candidate instead.
+  template <int K>
+  __global__ void __launch_bounds__(256) kPixPre(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int total = ev.sc->pixCandTotal;
+    const unsigned int plsBase = es.lsOffset[es.nLowerModules];
+    const unsigned int stride = gridDim.x * blockDim.x;
+    for (unsigned int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+      const unsigned int c = base + laneId();
+      bool pass = false;
+      if (c < total) {
+        unsigned int iPLS, obj;
+        uint16_t mod;
+        pixCandidate<K>(es, ev, c, iPLS, obj, mod);
+        if (K == 5)
+          pass = !ev.t5.isDup[obj] &&
+                 pt3RadiusPass(es.m, ev.rg, ev.ls, ev.t3, plsBase + iPLS, ev.t5.tripletIndices[2 * obj]);
+        else
+          pass = es.m.moduleType[ev.t3.lowerModuleIndices[3 * obj + 1]] != TwoS && !ev.t3.partOfPT5[obj] &&
+                 pt3RadiusPass(es.m, ev.rg, ev.ls, ev.t3, plsBase + iPLS, obj);
+      }
+      const unsigned int mask = __ballot_sync(kFullMask, pass);
+      if (mask == 0u)
+        continue;
+      unsigned int start = 0;
+      if (laneId() == 0)
+        start = atomicAdd(&ev.sc->pixQueueCount, __popc(mask));
+      start = __shfl_sync(kFullMask, start, 0);
+      const unsigned int pos = start + __popc(mask & lanesBelowMask());
+      if (pass && pos < kPixQueueCap)
+        ev.pixQueue[pos] = c;
+    }
+  }
+
   template <int K>
   __global__ void __launch_bounds__(LST_LB_EVAL) kPixEval(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int total = ev.sc->pixCandTotal;
+    const unsigned int queued = ev.sc->pixQueueCount;
+    const bool fromQueue = queued <= kPixQueueCap;
+    const unsigned int n = fromQueue ? queued : total;
     const unsigned int plsBase = es.lsOffset[es.nLowerModules];
-    for (unsigned int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+    for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+      const unsigned int c = fromQueue ? ev.pixQueue[q] : q;
       unsigned int iPLS, obj;
       uint16_t mod;
       pixCandidate<K>(es, ev, c, iPLS, obj, mod);

@@ -530,6 +530,20 @@ namespace lst {
         rPhiChiSquaredInwards;
   };
 
+  // The opening test of pt3Select below, alone: the radius criterion of the
+  // pLS and triplet radii (the cheapest test, and the first one evaluated).
+  LST_HD bool pt3RadiusPass(const Modules& m, const Ranges& rg, const Segments& s, const Triplets& t,
+                            unsigned int plsIndex, unsigned int t3) {
+    uint16_t pixelModule = s.innerLowerModuleIndices[plsIndex];
+    uint16_t lmL = t.lowerModuleIndices[3 * t3], lmM = t.lowerModuleIndices[3 * t3 + 1],
+             lmU = t.lowerModuleIndices[3 * t3 + 2];
+    unsigned int pls = plsIndex - rg.segmentModuleIndices[pixelModule];
+    const float pixelRadius = s.ptIn[pls] * kR1GeVf;
+    const float pixelRadiusError = s.ptErr[pls] * kR1GeVf;
+    int kind = (m.subdets[lmL] == Endcap) ? 3 : (m.subdets[lmM] == Endcap) ? 2 : (m.subdets[lmU] == Endcap) ? 1 : 0;
+    return pt3RadiusCriterion(kind, pixelRadius, pixelRadiusError, t.circleRadius[t3]);
+  }
+
   // pLS x T3 selection (SDL/PixelTriplet.h:826-1023).
   LST_HD bool pt3Select(const Modules& m,
                         const Ranges& rg,
