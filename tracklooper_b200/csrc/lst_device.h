@@ -61,7 +61,8 @@ namespace lst {
     unsigned int pixFallback;     // the pixel stage overflowed the staging: walk instead
     unsigned int t5DnnCount;      // candidates buffered for kT5Dnn
     unsigned int pixQueueCount;   // candidates passing the pixel pre-selection
-    unsigned int pad[2];
+    unsigned int t5QueueCount;    // candidates passing the quintuplet pre-selection
+    unsigned int pad[1];
   };
 
   // All device pointers of one event.
@@ -118,7 +119,7 @@ namespace lst {
     unsigned int* pixPassObj;   //   the T5 / T3 index
     unsigned int* pixPassPLS;   //   the pLS index
     float* pixPassV;            //   the selection values (8 per candidate)
-    unsigned int* pixQueue;     // candidates passing the pixel pre-selection (any order)
+    unsigned int* candQueue;    // candidates passing a pre-selection (T5, then pT5 / pT3), any order
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
     unsigned int* plsOrder;     // pLS indices sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)

@@ -455,6 +455,7 @@ namespace {
         LST_LAUNCH(lst::kT5Eligible, one, 1024, d, v);
         LST_LAUNCH(lst::kT5Prefix, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v);
         LST_LAUNCH(lst::kT5ModScan, one, 1024, d, v);
+        LST_LAUNCH(lst::kT5Pre, dim3(blocksFor(size_t(1) << 20, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kT5Eval, tunedFlatGrid(ev, kTuT5Eval, count), tunedThreads(ev, kTuT5Eval), d, v, useDnn);
         if (useDnn)
           LST_LAUNCH(lst::kT5Dnn, dim3(blocksFor(lst::kT5DnnCap, count, 128), count), 128, d, v);
@@ -610,6 +611,7 @@ namespace {
         {"kPixScan", (const void*)lst::kPixScan},
         {"kPixEval<5>", (const void*)lst::kPixEval<5>},
         {"kPixPre<5>", (const void*)lst::kPixPre<5>},
+        {"kT5Pre", (const void*)lst::kT5Pre},
         {"kPixPre<3>", (const void*)lst::kPixPre<3>},
         {"kPixEval<3>", (const void*)lst::kPixEval<3>},
         {"kPixRankEmit<5>", (const void*)lst::kPixRankEmit<5>},

@@ -247,7 +247,7 @@
   X(pixPassObj, unsigned int, lst::kPixPassCap)       \
   X(pixPassPLS, unsigned int, lst::kPixPassCap)       \
   X(pixPassV, float, 8 * lst::kPixPassCap)            \
-  X(pixQueue, unsigned int, lst::kPixQueueCap)        \
+  X(candQueue, unsigned int, lst::kCandQueueCap)        \
   X(tcCleanInfo, lst::TCCleanInfo, TC)                \
   X(plsOrder, unsigned int, P)                        \
   X(plsBinStart, unsigned int, lst::kPLSBins + 2)

@@ -759,6 +759,7 @@ namespace lst {
   // ranks, caps and stored values are those of the walk.  Events with more
   // candidates than the flag buffer holds take the walk instead.
   constexpr unsigned int kT5CandCap = 1u << 21;  // candidates per event
+  constexpr unsigned int kCandQueueCap = 1u << 18;  // pre-selected candidates per event (T5, pT5, pT3)
   constexpr unsigned int kT5PassCap = 1u << 16;  // passing candidates per event whose values are kept
   constexpr unsigned int kT5DnnCap = 1u << 14;   // candidates per event classified in kT5Dnn
 
@@ -840,6 +841,67 @@ namespace lst {
       ev.sc->t5CandOverflow = (carry > kT5CandCap || ev.forceWalk) ? 1u : 0u;
       ev.sc->t5PassCount = 0;
       ev.sc->t5DnnCount = 0;
+      ev.sc->t5QueueCount = 0;
+    }
+  }
+
+  // (inner T3, outer T3, lower modules) of quintuplet candidate c.
+  __device__ __forceinline__ void t5Decode(const EventView& ev, unsigned int c, unsigned int& innerT3,
+                                           unsigned int& outerT3, uint16_t* lm) {
+    const int nE = *ev.rg.nEligibleT5Modules;
+    const unsigned int* off = ev.t5ModOff;
+    int lo = 0, hi = nE;  // largest w with off[w] <= c
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (off[mid] <= c)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
+    t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
+    lm[0] = lm1;
+    lm[1] = ev.t3.lowerModuleIndices[3 * innerT3 + 1];
+    lm[2] = ev.t3.lowerModuleIndices[3 * innerT3 + 2];
+    lm[3] = ev.t3.lowerModuleIndices[3 * outerT3 + 1];
+    lm[4] = ev.t3.lowerModuleIndices[3 * outerT3 + 2];
+  }
+
+  // Pre-selection of the quintuplet candidates: the shared-MD and radius tests
+  // that open the selection, which most candidates fail.  A failing candidate
+  // gets its flag here; the survivors are queued in any order for kT5Eval,
+  // which then runs the long tests with all lanes of a warp busy (a
+  // candidate's outcome does not depend on the thread that evaluates it).
+  // A full queue makes kT5Eval evaluate every candidate.
+  __global__ void __launch_bounds__(256) kT5Pre(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    if (ev.sc->t5CandOverflow)
+      return;
+    const unsigned int total = ev.sc->t5CandTotal;
+    const unsigned int stride = gridDim.x * blockDim.x;
+    for (unsigned int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+      const unsigned int c = base + laneId();
+      bool pass = false;
+      if (c < total) {
+        unsigned int innerT3, outerT3;
+        uint16_t lm[5];
+        t5Decode(ev, c, innerT3, outerT3, lm);
+        T5Values v;
+        T5Stage st;
+        pass = t5RadiusStage(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st);
+        if (!pass)
+          ev.t5CandFlag[c] = 0;
+      }
+      const unsigned int mask = __ballot_sync(kFullMask, pass);
+      if (mask == 0u)
+        continue;
+      unsigned int start = 0;
+      if (laneId() == 0)
+        start = atomicAdd(&ev.sc->t5QueueCount, __popc(mask));
+      start = __shfl_sync(kFullMask, start, 0);
+      const unsigned int pos = start + __popc(mask & lanesBelowMask());
+      if (pass && pos < kCandQueueCap)
+        ev.candQueue[pos] = c;
     }
   }
 
@@ -848,26 +910,15 @@ namespace lst {
     if (ev.sc->t5CandOverflow)
       return;
     const unsigned int total = ev.sc->t5CandTotal;
-    const int nE = *ev.rg.nEligibleT5Modules;
-    const unsigned int* off = ev.t5ModOff;
+    const unsigned int queued = ev.sc->t5QueueCount;
+    const bool fromQueue = queued <= kCandQueueCap;
+    const unsigned int n = fromQueue ? queued : total;
     ConstDnn dnn;
-    for (unsigned int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
-      int lo = 0, hi = nE;  // largest w with off[w] <= c
-      while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (off[mid] <= c)
-          lo = mid;
-        else
-          hi = mid;
-      }
-      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
+    for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+      const unsigned int c = fromQueue ? ev.candQueue[q] : q;
       unsigned int innerT3, outerT3;
-      t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
-      uint16_t lm[5] = {lm1,
-                        ev.t3.lowerModuleIndices[3 * innerT3 + 1],
-                        ev.t3.lowerModuleIndices[3 * innerT3 + 2],
-                        ev.t3.lowerModuleIndices[3 * outerT3 + 1],
-                        ev.t3.lowerModuleIndices[3 * outerT3 + 2]};
+      uint16_t lm[5];
+      t5Decode(ev, c, innerT3, outerT3, lm);
       T5Values v;
       unsigned int flag = 0;
       T5Stage st;
@@ -1860,7 +1911,6 @@ namespace lst {
   // Events with more passing candidates than the staging holds take the
   // per-pLS count/emit walk instead.
   constexpr unsigned int kPixPassCap = 8192;
-  constexpr unsigned int kPixQueueCap = 1u << 18;
   constexpr int kConnStride = kMaxConnectedModules + 1;
 
   template <int K>
@@ -1992,8 +2042,8 @@ namespace lst {
         start = atomicAdd(&ev.sc->pixQueueCount, __popc(mask));
       start = __shfl_sync(kFullMask, start, 0);
       const unsigned int pos = start + __popc(mask & lanesBelowMask());
-      if (pass && pos < kPixQueueCap)
-        ev.pixQueue[pos] = c;
+      if (pass && pos < kCandQueueCap)
+        ev.candQueue[pos] = c;
     }
   }
 
@@ -2002,11 +2052,11 @@ namespace lst {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int total = ev.sc->pixCandTotal;
     const unsigned int queued = ev.sc->pixQueueCount;
-    const bool fromQueue = queued <= kPixQueueCap;
+    const bool fromQueue = queued <= kCandQueueCap;
     const unsigned int n = fromQueue ? queued : total;
     const unsigned int plsBase = es.lsOffset[es.nLowerModules];
     for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-      const unsigned int c = fromQueue ? ev.pixQueue[q] : q;
+      const unsigned int c = fromQueue ? ev.candQueue[q] : q;
       unsigned int iPLS, obj;
       uint16_t mod;
       pixCandidate<K>(es, ev, c, iPLS, obj, mod);

@@ -1241,15 +1241,18 @@ namespace lst {
   };
 
   // Every test before the classifier decision, and the circle regression.
-  LST_HD bool t5SelectPre(const Modules& m,
-                          const MiniDoublets& md,
-                          const Segments& s,
-                          const Triplets& t,
-                          const uint16_t* lm,
-                          unsigned int innerT3,
-                          unsigned int outerT3,
-                          T5Values& v,
-                          T5Stage& st) {
+  // The shared-MD test and the radius tests that open t5SelectPre (the
+  // cheapest tests, which most candidates fail); fills the hit coordinates,
+  // MD indices and radii the later tests use.
+  LST_HD bool t5RadiusStage(const Modules& m,
+                            const MiniDoublets& md,
+                            const Segments& s,
+                            const Triplets& t,
+                            const uint16_t* lm,
+                            unsigned int innerT3,
+                            unsigned int outerT3,
+                            T5Values& v,
+                            T5Stage& st) {
     unsigned int seg1 = t.segmentIndices[2 * innerT3];
     unsigned int seg2 = t.segmentIndices[2 * innerT3 + 1];
     unsigned int seg3 = t.segmentIndices[2 * outerT3];
@@ -1320,10 +1323,28 @@ namespace lst {
         radiusSpread(px[0], py[0], np[0], px[1], py[1], np[1], px[2], py[2], np[2], innerRadiusMin2S, innerRadiusMax2S);
       radiusSpread(px[1], py[1], np[1], px[2], py[2], np[2], px[3], py[3], np[3], bridgeRadiusMin2S, bridgeRadiusMax2S);
     }
-    if (!matchRadii(
-            kind, v.innerRadius, v.bridgeRadius, innerRadiusMin2S, innerRadiusMax2S, bridgeRadiusMin2S, bridgeRadiusMax2S))
-      return false;
+    return matchRadii(
+        kind, v.innerRadius, v.bridgeRadius, innerRadiusMin2S, innerRadiusMax2S, bridgeRadiusMin2S, bridgeRadiusMax2S);
+  }
 
+  LST_HD bool t5SelectPre(const Modules& m,
+                          const MiniDoublets& md,
+                          const Segments& s,
+                          const Triplets& t,
+                          const uint16_t* lm,
+                          unsigned int innerT3,
+                          unsigned int outerT3,
+                          T5Values& v,
+                          T5Stage& st) {
+    if (!t5RadiusStage(m, md, s, t, lm, innerT3, outerT3, v, st))
+      return false;
+    const unsigned int* mdIdx = st.mdIdx;
+    const float* xs = st.xs;
+    const float* ys = st.ys;
+    const unsigned int seg1 = t.segmentIndices[2 * innerT3];
+    const unsigned int seg3 = t.segmentIndices[2 * outerT3];
+    const unsigned int seg4 = t.segmentIndices[2 * outerT3 + 1];
+    float g, f;
     T4Input q1{lm[0], lm[1], lm[2], lm[3], seg1, seg3, mdIdx[0], mdIdx[1], mdIdx[2], mdIdx[3]};
     if (!t4Select(m, md, s, q1))
       return false;
