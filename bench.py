@@ -120,12 +120,17 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi takes a moment to start: begin the timed region at its first sample
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.lines.clear()
 
     def _read(self):
         for line in self.proc.stdout:
@@ -416,8 +421,10 @@ def run_ours(args, rank, world, local, events):
 
 
 # ----------------------------------------------------------- reference CPU
-def run_reference_cpu(events, threads: int, min_events: int, budget_s: float = 20.0):
-    """Reference CPU backend, one event per thread at a time; returns (events/s, events, threads, seconds)."""
+def run_reference_cpu(events, threads: int, min_events: int, budget_s: float = 0.0):
+    """Reference CPU backend, one event per thread at a time, over at least
+    min_events events and (when budget_s > 0) for at least budget_s seconds,
+    cycling through the events; returns (events/s, events, threads, seconds)."""
     from oracle import reflib
 
     variant = "fast"
@@ -436,7 +443,7 @@ def run_reference_cpu(events, threads: int, min_events: int, budget_s: float = 2
         while True:
             with lock:
                 i = next_i[0]
-                if i >= n:
+                if i >= n and time.perf_counter() - t0 >= budget_s:
                     return
                 next_i[0] += 1
             w.run_event(events[i % len(events)])
@@ -473,7 +480,7 @@ def cpu_threads(ncpu: int) -> int:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=64)
@@ -527,9 +534,10 @@ def main():
     if rank == 0 and world == 1:
         try:
             threads = cpu_threads(ncpu)
-            r, ne, th, dt = run_reference_cpu(events, threads, args.cpu_events or 2 * threads)
+            r, ne, th, dt = run_reference_cpu(events, threads, args.cpu_events or 2 * threads, budget_s=12.0)
             cpu = {"value": r, "unit": "events/s", "cores": th, "kind": "reference",
-                   "sample": f"{ne} events of this batch, one event per thread, {dt:.1f} s wall, liblstref_fast.so"}
+                   "sample": f"{ne} events of this batch (cycled), one event per thread, {dt:.1f} s wall, "
+                             f"liblstref_fast.so"}
         except Exception as e:  # the CPU baseline is reported, not required
             cpu = {"value": None, "unit": "events/s", "cores": ncpu, "kind": "reference", "sample": f"failed: {e}"}
 
