@@ -119,6 +119,10 @@ namespace lst {
     unsigned int* pixPassObj;   //   the T5 / T3 index
     unsigned int* pixPassPLS;   //   the pLS index
     float* pixPassV;            //   the selection values (8 per candidate)
+    float* hitMiniSlope;        // per hit: the slope term of the mini-doublet dphi threshold
+    float* hitShiftXa;          // per hit moved by the strip shift: its moved point and z
+    float* hitShiftYa;
+    float* hitShiftZn;
     unsigned int* candQueue;    // candidates passing a pre-selection (T5, then pT5 / pT3), any order
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
     unsigned int* plsOrder;     // pLS indices sorted by eta bin

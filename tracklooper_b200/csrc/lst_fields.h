@@ -248,6 +248,10 @@
   X(pixPassPLS, unsigned int, lst::kPixPassCap)       \
   X(pixPassV, float, 8 * lst::kPixPassCap)            \
   X(candQueue, unsigned int, lst::kCandQueueCap)        \
+  X(hitMiniSlope, float, H)                           \
+  X(hitShiftXa, float, H)                             \
+  X(hitShiftYa, float, H)                             \
+  X(hitShiftZn, float, H)                             \
   X(tcCleanInfo, lst::TCCleanInfo, TC)                \
   X(plsOrder, unsigned int, P)                        \
   X(plsBinStart, unsigned int, lst::kPLSBins + 2)

@@ -196,6 +196,22 @@ namespace lst {
       }
       uint16_t mi = m.mapIdx[found];
       h.moduleIndices[ihit] = mi;
+      // Per-hit parts of the mini-doublet cuts of the module pair this hit
+      // belongs to (lower module lm): the dphi-threshold slope, and the strip
+      // shift of the hit it moves (tilted barrel and endcap modules).
+      ev.hitMiniSlope[ihit] = mdMiniSlope(rt);
+      if (mi != es.pixelModule) {
+        const bool isLowerHit = m.isLower[mi];
+        const uint16_t lm = isLowerHit ? mi : m.partnerModuleIndices[mi];
+        const bool shifted = m.subdets[lm] == Endcap || (m.subdets[lm] == Barrel && m.sides[lm] != Center);
+        if (shifted && shiftMovesLower(m, lm) == isLowerHit) {
+          float xa, ya, zn;
+          shiftStripPrep(m, lm, x, y, z, rt, xa, ya, zn);
+          ev.hitShiftXa[ihit] = xa;
+          ev.hitShiftYa[ihit] = ya;
+          ev.hitShiftZn[ihit] = zn;
+        }
+      }
       if (m.subdets[mi] == Endcap && m.moduleType[mi] == TwoS) {
         int f = sortedFind(m.geoMapDetId, detId, m.nEndCapMap);
         if (f < 0) {
@@ -284,6 +300,7 @@ namespace lst {
     const int cap = es.mdCap[lm];
     const unsigned int base = es.mdOffset[lm];
     MiniDoublets md = ev.md;
+    const MDHitPre pre{ev.hitMiniSlope, ev.hitShiftXa, ev.hitShiftYa, ev.hitShiftZn};
     unsigned int count = 0;
     for (int start = 0; start < limit; start += 32) {
       int hitIndex = start + int(laneId());
@@ -308,6 +325,9 @@ namespace lst {
                         h.rts[upperIdx],
                         h.phis[lowerIdx],
                         h.phis[upperIdx],
+                        pre,
+                        lowerIdx,
+                        upperIdx,
                         v);
         }
       }

@@ -69,9 +69,12 @@ namespace lst {
   }
 
   // dPhi acceptance of a mini-doublet (SDL/MiniDoublet.h:340-402).
-  LST_HD float mdDPhiThreshold(const Modules& m, float rt, uint16_t mi, float dPhi = 0, float dz = 0) {
+  // The slope term of mdDPhiThreshold, a function of the hit's rt alone
+  // (computed once per hit by kHitPrep).
+  LST_HD float mdMiniSlope(float rt) { return fasin(fmin_(rt * k2Rinv1GeVf / kPtCut, kSinAlphaMax)); }
+
+  LST_HD float mdDPhiThresholdFromSlope(const Modules& m, float miniSlope, uint16_t mi, float dPhi = 0, float dz = 0) {
     unsigned int iL = m.layers[mi] - 1;
-    const float miniSlope = fasin(fmin_(rt * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
     const bool barrel = m.subdets[mi] == Barrel;
     const float rLayNominal = barrel ? miniRminMeanBarrel(iL) : miniRminMeanEndcap(iL);
     const float miniPVoff = 0.1f / rLayNominal;
@@ -97,49 +100,28 @@ namespace lst {
     return miniSlope + fsqrt(miniMuls * miniMuls + miniPVoff * miniPVoff + miniLum * miniLum);
   }
 
+  LST_HD float mdDPhiThreshold(const Modules& m, float rt, uint16_t mi, float dPhi = 0, float dz = 0) {
+    return mdDPhiThresholdFromSlope(m, mdMiniSlope(rt), mi, dPhi, dz);
+  }
+
   // Moves the strip hit along the strip so that it lines up with the
   // interaction point and the pixel hit (SDL/MiniDoublet.h:404-568).
-  LST_HD void shiftStripHit(const Modules& m,
-                            uint16_t lm,
-                            float xLower,
-                            float yLower,
-                            float zLower,
-                            float rtLower,
-                            float xUpper,
-                            float yUpper,
-                            float zUpper,
-                            float rtUpper,
-                            float& xn,
-                            float& yn,
-                            float& zn) {
-    float xp, yp, zp, rtp, xo, yo;
+  // shiftStripHit (SDL/MiniDoublet.h:110-191) moves one hit of the pair (p)
+  // along the strip direction onto the other sensor's plane and projects it
+  // next to the other hit (o).  Which hit is p depends only on the lower
+  // module lm: true = the lower hit.
+  LST_HD bool shiftMovesLower(const Modules& m, uint16_t lm) {
+    if (m.moduleType[lm] == PS)
+      return m.subdets[lm] == Barrel ? m.moduleLayerType[lm] != Pixel : m.moduleLayerType[lm] == Pixel;
+    return true;
+  }
+
+  // The part of shiftStripHit that depends on p alone: the moved point before
+  // the projection (xa, ya) and the moved z (computed once per hit by kHitPrep).
+  LST_HD void shiftStripPrep(const Modules& m, uint16_t lm, float xp, float yp, float zp, float rtp, float& xa, float& ya,
+                             float& zn) {
     const float slope = m.dxdys[lm];
     const float drdz_ = m.drdzs[lm];
-    const bool barrel = m.subdets[lm] == Barrel;
-    if (m.moduleType[lm] == PS) {
-      if (barrel ? m.moduleLayerType[lm] != Pixel : m.moduleLayerType[lm] == Pixel) {
-        xo = xUpper;
-        yo = yUpper;
-        xp = xLower;
-        yp = yLower;
-        zp = zLower;
-        rtp = rtLower;
-      } else {
-        xo = xLower;
-        yo = yLower;
-        xp = xUpper;
-        yp = yUpper;
-        zp = zUpper;
-        rtp = rtUpper;
-      }
-    } else {
-      xo = xUpper;
-      yo = yUpper;
-      xp = xLower;
-      yp = yLower;
-      zp = zLower;
-      rtp = rtLower;
-    }
     const bool isEndcap = m.subdets[lm] == Endcap;
     float angleA = fabs_(fatan(rtp / zp));
     float angleB = isEndcap ? float(M_PI) / 2.f : fatan(drdz_);
@@ -159,8 +141,21 @@ namespace lst {
       angleM = 2.f * float(M_PI) - absArctanSlope;
     float drprime_x = drprime * fsin(angleM);
     float drprime_y = drprime * fcos(angleM);
-    float xa = xp + drprime_x;
-    float ya = yp + drprime_y;
+    xa = xp + drprime_x;
+    ya = yp + drprime_y;
+    float absdzprime = fabs_(moduleSeparation / fsin(angleA + angleB) * fcos(angleA));
+    float abszn;
+    if (m.moduleLayerType[lm] == Pixel)
+      abszn = fabs_(zp) + absdzprime;
+    else
+      abszn = fabs_(zp) - absdzprime;
+    zn = abszn * ((zp > 0) ? 1 : -1);
+  }
+
+  // The projection next to the other hit (xo, yo) that completes shiftStripHit.
+  LST_HD void shiftStripFinish(const Modules& m, uint16_t lm, float xa, float ya, float xo, float yo, float& xn,
+                               float& yn) {
+    const float slope = m.dxdys[lm];
     if (slope == kInf) {
       xn = xa;
       yn = yo;
@@ -171,13 +166,35 @@ namespace lst {
       xn = (slope * xa + (1.f / slope) * xo - ya + yo) / (slope + (1.f / slope));
       yn = (xn - xa) * slope + ya;
     }
-    float absdzprime = fabs_(moduleSeparation / fsin(angleA + angleB) * fcos(angleA));
-    float abszn;
-    if (m.moduleLayerType[lm] == Pixel)
-      abszn = fabs_(zp) + absdzprime;
-    else
-      abszn = fabs_(zp) - absdzprime;
-    zn = abszn * ((zp > 0) ? 1 : -1);
+  }
+
+  // Per-hit values of the mini-doublet cuts computed once per hit: the slope
+  // term of the dphi threshold and, for the hit that shiftStripHit moves, its
+  // moved point (xa, ya) and z.  Arrays indexed by hit.
+  struct MDHitPre {
+    const float* miniSlope;
+    const float* shiftXa;
+    const float* shiftYa;
+    const float* shiftZn;
+  };
+
+  LST_HD void shiftStripHit(const Modules& m,
+                            uint16_t lm,
+                            const MDHitPre& pre,
+                            unsigned int lowerIdx,
+                            unsigned int upperIdx,
+                            float xLower,
+                            float yLower,
+                            float xUpper,
+                            float yUpper,
+                            float& xn,
+                            float& yn,
+                            float& zn) {
+    const bool fromLower = shiftMovesLower(m, lm);
+    const unsigned int p = fromLower ? lowerIdx : upperIdx;
+    const float xo = fromLower ? xUpper : xLower, yo = fromLower ? yUpper : yLower;
+    zn = pre.shiftZn[p];
+    shiftStripFinish(m, lm, pre.shiftXa[p], pre.shiftYa[p], xo, yo, xn, yn);
   }
 
   // The derived per-MD values of MiniDoublets (slope, tanSlope, slope3).
@@ -206,6 +223,9 @@ namespace lst {
                        float rtUpper,
                        float phiLower,
                        float phiUpper,
+                       const MDHitPre& pre,
+                       unsigned int lowerIdx,
+                       unsigned int upperIdx,
                        MDValues& v) {
     v.dz = zLower - zUpper;
     const float dzCut = m.moduleType[lm] == PS ? 2.f : 10.f;
@@ -215,13 +235,13 @@ namespace lst {
       return false;
 
     const bool lowerIsPixel = m.moduleLayerType[lm] == Pixel;
-    float miniCut = lowerIsPixel ? mdDPhiThreshold(m, rtLower, lm) : mdDPhiThreshold(m, rtUpper, lm);
+    float miniCut = mdDPhiThresholdFromSlope(m, pre.miniSlope[lowerIsPixel ? lowerIdx : upperIdx], lm);
 
     float shiftedRt = 0;
     const bool tilted = m.sides[lm] != Center;
     if (tilted) {
       float xn, yn, zn;
-      shiftStripHit(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, xn, yn, zn);
+      shiftStripHit(m, lm, pre, lowerIdx, upperIdx, xLower, yLower, xUpper, yUpper, xn, yn, zn);
       v.shiftedX = xn;
       v.shiftedY = yn;
       shiftedRt = fsqrt(xn * xn + yn * yn);
@@ -275,6 +295,9 @@ namespace lst {
                        float rtUpper,
                        float phiLower,
                        float phiUpper,
+                       const MDHitPre& pre,
+                       unsigned int lowerIdx,
+                       unsigned int upperIdx,
                        MDValues& v) {
     float dz = zLower - zUpper;
     const float dzCut = 1.f;
@@ -286,7 +309,7 @@ namespace lst {
       return false;
 
     float xn, yn, zn;
-    shiftStripHit(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, xn, yn, zn);
+    shiftStripHit(m, lm, pre, lowerIdx, upperIdx, xLower, yLower, xUpper, yUpper, xn, yn, zn);
     const bool isPS = m.moduleType[lm] == PS;
     const bool lowerIsPixel = m.moduleLayerType[lm] == Pixel;
     v.shiftedX = xn;
@@ -308,8 +331,7 @@ namespace lst {
     if (isPS)
       dz = lowerIsPixel ? zLower - zn : zUpper - zn;
 
-    float miniCut = lowerIsPixel ? mdDPhiThreshold(m, rtLower, lm, v.dphi, dz)
-                                 : mdDPhiThreshold(m, rtUpper, lm, v.dphi, dz);
+    float miniCut = mdDPhiThresholdFromSlope(m, pre.miniSlope[lowerIsPixel ? lowerIdx : upperIdx], lm, v.dphi, dz);
     if (!(fabs_(v.dphi) < miniCut))
       return false;
 
@@ -334,10 +356,15 @@ namespace lst {
                        float rtUpper,
                        float phiLower,
                        float phiUpper,
+                       const MDHitPre& pre,
+                       unsigned int lowerIdx,
+                       unsigned int upperIdx,
                        MDValues& v) {
     if (m.subdets[lm] == Barrel)
-      return mdBarrel(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, phiLower, phiUpper, v);
-    return mdEndcap(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, phiLower, phiUpper, v);
+      return mdBarrel(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, phiLower, phiUpper, pre,
+                      lowerIdx, upperIdx, v);
+    return mdEndcap(m, lm, xLower, yLower, zLower, rtLower, xUpper, yUpper, zUpper, rtUpper, phiLower, phiUpper, pre,
+                    lowerIdx, upperIdx, v);
   }
 
   // Writes a mini-doublet record (SDL/MiniDoublet.h:193-266).  On PS modules
