@@ -267,6 +267,13 @@ namespace lst {
     float* slope;
     float* tanSlope;
     float* slope3;
+    // The anchor hit's x, y, z, rt in one 16-byte record: the segment, triplet
+    // and pixel kernels gather them together for mini-doublets chosen by index.
+    struct MDPos* anchorPos;
+  };
+
+  struct alignas(16) MDPos {
+    float x, y, z, rt;
   };
 
   struct Segments {

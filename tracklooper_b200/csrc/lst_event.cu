@@ -100,6 +100,7 @@ namespace {
     v.md.slope = c.take<float>(MD);
     v.md.tanSlope = c.take<float>(MD);
     v.md.slope3 = c.take<float>(MD);
+    v.md.anchorPos = c.take<lst::MDPos>(MD);
     v.sc = c.take<lst::EventScalars>(1);
   }
 

@@ -85,9 +85,9 @@ namespace lst {
                        LSValues& v) {
     float sdMuls = (m.subdets[innerLM] == Barrel) ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / kPtCut
                                                   : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / kPtCut;
-    float xIn = md.anchorX[innerMD], yIn = md.anchorY[innerMD], zIn = md.anchorZ[innerMD], rtIn = md.anchorRt[innerMD];
-    float xOut = md.anchorX[outerMD], yOut = md.anchorY[outerMD], zOut = md.anchorZ[outerMD],
-          rtOut = md.anchorRt[outerMD];
+    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
+    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
+    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
 
     float sdSlope = md.slope[outerMD];
     float sdPVoff = 0.1f / rtOut;
@@ -128,9 +128,9 @@ namespace lst {
                        unsigned int innerMD,
                        unsigned int outerMD,
                        LSValues& v) {
-    float xIn = md.anchorX[innerMD], yIn = md.anchorY[innerMD], zIn = md.anchorZ[innerMD], rtIn = md.anchorRt[innerMD];
-    float xOut = md.anchorX[outerMD], yOut = md.anchorY[outerMD], zOut = md.anchorZ[outerMD],
-          rtOut = md.anchorRt[outerMD];
+    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
+    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
+    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
     bool outerLayerEndcapTwoS = (m.subdets[outerLM] == Endcap) && (m.moduleType[outerLM] == TwoS);
     float sdSlope = md.slope[outerMD];
     float disks2SMinRadius = 60.f;

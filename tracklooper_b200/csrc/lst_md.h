@@ -402,6 +402,7 @@ namespace lst {
     md.anchorY[idx] = h.ys[anchor];
     md.anchorZ[idx] = h.zs[anchor];
     md.anchorRt[idx] = h.rts[anchor];
+    md.anchorPos[idx] = MDPos{h.xs[anchor], h.ys[anchor], h.zs[anchor], h.rts[anchor]};
     md.anchorPhi[idx] = h.phis[anchor];
     md.anchorEta[idx] = h.etas[anchor];
     float hex = h.highEdgeXs[anchor], hey = h.highEdgeYs[anchor];

@@ -28,10 +28,10 @@ namespace lst {
                      unsigned int md3,
                      unsigned int md4) {
     bool isPS_OutLo = (m.moduleType[lmOI] == PS);
-    float rt_InLo = md.anchorRt[md1], rt_InUp = md.anchorRt[md2], rt_OutLo = md.anchorRt[md3], rt_OutUp = md.anchorRt[md4];
-    float z_InUp = md.anchorZ[md2], z_OutLo = md.anchorZ[md3];
-    float x_InLo = md.anchorX[md1], x_InUp = md.anchorX[md2], x_OutLo = md.anchorX[md3], x_OutUp = md.anchorX[md4];
-    float y_InLo = md.anchorY[md1], y_InUp = md.anchorY[md2], y_OutLo = md.anchorY[md3], y_OutUp = md.anchorY[md4];
+    float rt_InLo = md.anchorPos[md1].rt, rt_InUp = md.anchorPos[md2].rt, rt_OutLo = md.anchorPos[md3].rt, rt_OutUp = md.anchorPos[md4].rt;
+    float z_InUp = md.anchorPos[md2].z, z_OutLo = md.anchorPos[md3].z;
+    float x_InLo = md.anchorPos[md1].x, x_InUp = md.anchorPos[md2].x, x_OutLo = md.anchorPos[md3].x, x_OutUp = md.anchorPos[md4].x;
+    float y_InLo = md.anchorPos[md1].y, y_InUp = md.anchorPos[md2].y, y_OutLo = md.anchorPos[md3].y, y_OutUp = md.anchorPos[md4].y;
     float rt_InOut = rt_InUp;
     // deltaPhi of two anchor hits, from their stored phi (hits.phis is phi()
     // of the same coordinates, so the value is identical)
@@ -174,13 +174,13 @@ namespace lst {
                      unsigned int md3,
                      unsigned int md4) {
     bool isPS_OutLo = (m.moduleType[lmOI] == PS);
-    float z_InUp = md.anchorZ[md2];
-    float z_OutLo = md.anchorZ[md3];
+    float z_InUp = md.anchorPos[md2].z;
+    float z_OutLo = md.anchorPos[md3].z;
     if (!(z_InUp * z_OutLo > 0))
       return false;
-    float rt_InLo = md.anchorRt[md1], rt_InUp = md.anchorRt[md2], rt_OutLo = md.anchorRt[md3], rt_OutUp = md.anchorRt[md4];
-    float x_InLo = md.anchorX[md1], x_InUp = md.anchorX[md2], x_OutLo = md.anchorX[md3], x_OutUp = md.anchorX[md4];
-    float y_InLo = md.anchorY[md1], y_InUp = md.anchorY[md2], y_OutLo = md.anchorY[md3], y_OutUp = md.anchorY[md4];
+    float rt_InLo = md.anchorPos[md1].rt, rt_InUp = md.anchorPos[md2].rt, rt_OutLo = md.anchorPos[md3].rt, rt_OutUp = md.anchorPos[md4].rt;
+    float x_InLo = md.anchorPos[md1].x, x_InUp = md.anchorPos[md2].x, x_OutLo = md.anchorPos[md3].x, x_OutUp = md.anchorPos[md4].x;
+    float y_InLo = md.anchorPos[md1].y, y_InUp = md.anchorPos[md2].y, y_OutLo = md.anchorPos[md3].y, y_OutUp = md.anchorPos[md4].y;
     unsigned int pls = innerSeg - rg.segmentModuleIndices[pixelModule];
     float ptIn = s.ptIn[pls];
     float px = s.px[pls], py = s.py[pls], pz = s.pz[pls];
@@ -581,19 +581,19 @@ namespace lst {
     unsigned int pixelOuterMD = s.mdIndices[2 * plsIndex + 1];
     unsigned int innerSeg = t.segmentIndices[2 * t3], outerSeg = t.segmentIndices[2 * t3 + 1];
     unsigned int md1 = s.mdIndices[2 * innerSeg], md2 = s.mdIndices[2 * innerSeg + 1], md3 = s.mdIndices[2 * outerSeg + 1];
-    float xs[3] = {md.anchorX[md1], md.anchorX[md2], md.anchorX[md3]};
-    float ys[3] = {md.anchorY[md1], md.anchorY[md2], md.anchorY[md3]};
+    float xs[3] = {md.anchorPos[md1].x, md.anchorPos[md2].x, md.anchorPos[md3].x};
+    float ys[3] = {md.anchorPos[md1].y, md.anchorPos[md2].y, md.anchorPos[md3].y};
     float g = t.circleCenterX[t3];
     float f = t.circleCenterY[t3];
 
     uint16_t lm3[3] = {lmL, lmM, lmU};
     if (runChiSquaredCuts and pixelSegmentPt < 5.0f) {
-      float rts[3] = {md.anchorRt[md1], md.anchorRt[md2], md.anchorRt[md3]};
-      float zs[3] = {md.anchorZ[md1], md.anchorZ[md2], md.anchorZ[md3]};
-      float rtPix[2] = {md.anchorRt[pixelInnerMD], md.anchorRt[pixelOuterMD]};
-      float xPix[2] = {md.anchorX[pixelInnerMD], md.anchorX[pixelOuterMD]};
-      float yPix[2] = {md.anchorY[pixelInnerMD], md.anchorY[pixelOuterMD]};
-      float zPix[2] = {md.anchorZ[pixelInnerMD], md.anchorZ[pixelOuterMD]};
+      float rts[3] = {md.anchorPos[md1].rt, md.anchorPos[md2].rt, md.anchorPos[md3].rt};
+      float zs[3] = {md.anchorPos[md1].z, md.anchorPos[md2].z, md.anchorPos[md3].z};
+      float rtPix[2] = {md.anchorPos[pixelInnerMD].rt, md.anchorPos[pixelOuterMD].rt};
+      float xPix[2] = {md.anchorPos[pixelInnerMD].x, md.anchorPos[pixelOuterMD].x};
+      float yPix[2] = {md.anchorPos[pixelInnerMD].y, md.anchorPos[pixelOuterMD].y};
+      float zPix[2] = {md.anchorPos[pixelInnerMD].z, md.anchorPos[pixelOuterMD].z};
       v.rzChiSquared = pt3RZChi2(m, lm3, rtPix, xPix, yPix, zPix, rts, zs, s.px[pls], s.py[pls], s.pz[pls], s.charge[pls]);
       if (!pt3PassRZ(m, lmL, lmM, lmU, v.rzChiSquared))
         return false;
@@ -609,8 +609,8 @@ namespace lst {
       if (!pt3PassRPhi(m, lmL, lmM, lmU, v.rPhiChiSquared))
         return false;
     }
-    float xPix[2] = {md.anchorX[pixelInnerMD], md.anchorX[pixelOuterMD]};
-    float yPix[2] = {md.anchorY[pixelInnerMD], md.anchorY[pixelOuterMD]};
+    float xPix[2] = {md.anchorPos[pixelInnerMD].x, md.anchorPos[pixelOuterMD].x};
+    float yPix[2] = {md.anchorPos[pixelInnerMD].y, md.anchorPos[pixelOuterMD].y};
     v.rPhiChiSquaredInwards = pixelInwardsChi2(g, f, v.tripletRadius, xPix, yPix);
     if (runChiSquaredCuts and pixelSegmentPt < 5.0f) {
       if (!pt3PassRPhiInwards(m, lmL, lmM, lmU, v.rPhiChiSquaredInwards))
@@ -905,14 +905,14 @@ namespace lst {
     uint16_t lm[5];
     for (int i = 0; i < 5; ++i)
       lm[i] = q.lowerModuleIndices[5 * t5 + i];
-    float zPix[2] = {md.anchorZ[pixelInnerMD], md.anchorZ[pixelOuterMD]};
-    float rtPix[2] = {md.anchorRt[pixelInnerMD], md.anchorRt[pixelOuterMD]};
+    float zPix[2] = {md.anchorPos[pixelInnerMD].z, md.anchorPos[pixelOuterMD].z};
+    float rtPix[2] = {md.anchorPos[pixelInnerMD].rt, md.anchorPos[pixelOuterMD].rt};
     float zs[5], rts[5], xs[5], ys[5];
     for (int i = 0; i < 5; ++i) {
-      zs[i] = md.anchorZ[mdi[i]];
-      rts[i] = md.anchorRt[mdi[i]];
-      xs[i] = md.anchorX[mdi[i]];
-      ys[i] = md.anchorY[mdi[i]];
+      zs[i] = md.anchorPos[mdi[i]].z;
+      rts[i] = md.anchorPos[mdi[i]].rt;
+      xs[i] = md.anchorPos[mdi[i]].x;
+      ys[i] = md.anchorPos[mdi[i]].y;
     }
     v.rzChiSquared = 0;
     v.centerX = s.circleCenterX[pls];
@@ -934,8 +934,8 @@ namespace lst {
       if (!pt5PassRPhi(m, lm, v.rPhiChiSquared))
         return false;
     }
-    float xPix[2] = {md.anchorX[pixelInnerMD], md.anchorX[pixelOuterMD]};
-    float yPix[2] = {md.anchorY[pixelInnerMD], md.anchorY[pixelOuterMD]};
+    float xPix[2] = {md.anchorPos[pixelInnerMD].x, md.anchorPos[pixelOuterMD].x};
+    float yPix[2] = {md.anchorPos[pixelInnerMD].y, md.anchorPos[pixelOuterMD].y};
     v.rPhiChiSquaredInwards = pixelInwardsChi2(T5CenterX, T5CenterY, v.quintupletRadius, xPix, yPix);
     if (q.regressionRadius[t5] < 5.0f * kR1GeVf) {
       if (!pt5PassRPhiInwards(m, lm, v.rPhiChiSquaredInwards))

@@ -16,8 +16,8 @@ namespace lst {
                        unsigned int md1,
                        unsigned int md2,
                        unsigned int md3) {
-    const float r1 = md.anchorRt[md1], r2 = md.anchorRt[md2], r3 = md.anchorRt[md3];
-    const float z1 = md.anchorZ[md1], z2 = md.anchorZ[md2], z3 = md.anchorZ[md3];
+    const float r1 = md.anchorPos[md1].rt, r2 = md.anchorPos[md2].rt, r3 = md.anchorPos[md3].rt;
+    const float z1 = md.anchorPos[md1].z, z2 = md.anchorPos[md2].z, z3 = md.anchorPos[md3].z;
     const int layer1 = m.sdlLayers[lm1], layer2 = m.sdlLayers[lm2], layer3 = m.sdlLayers[lm3];
     const float residual = z2 - ((z3 - z1) / (r3 - r1) * (r2 - r1) + z1);
     const float ar = fabs_(residual);
@@ -53,8 +53,8 @@ namespace lst {
   }
 
   LST_HD float segmentDr(const MiniDoublets& md, unsigned int a, unsigned int b) {
-    return fsqrt((md.anchorX[b] - md.anchorX[a]) * (md.anchorX[b] - md.anchorX[a]) +
-                 (md.anchorY[b] - md.anchorY[a]) * (md.anchorY[b] - md.anchorY[a]));
+    return fsqrt((md.anchorPos[b].x - md.anchorPos[a].x) * (md.anchorPos[b].x - md.anchorPos[a].x) +
+                 (md.anchorPos[b].y - md.anchorPos[a].y) * (md.anchorPos[b].y - md.anchorPos[a].y));
   }
 
   // Barrel-barrel-barrel pointing and first beta cut (SDL/Triplet.h:301-402).
@@ -70,8 +70,8 @@ namespace lst {
                             float& betaIn) {
     bool isPSIn = (m.moduleType[lm1] == PS);
     bool isPSOut = (m.moduleType[lm3] == PS);
-    float rtIn = md.anchorRt[md1], rtMid = md.anchorRt[md2], rtOut = md.anchorRt[md3];
-    float zIn = md.anchorZ[md1], zMid = md.anchorZ[md2], zOut = md.anchorZ[md3];
+    float rtIn = md.anchorPos[md1].rt, rtMid = md.anchorPos[md2].rt, rtOut = md.anchorPos[md3].rt;
+    float zIn = md.anchorPos[md1].z, zMid = md.anchorPos[md2].z, zOut = md.anchorPos[md3].z;
     float alpha1GeVOut = md.slope[md3];
     float rtRatio_OutIn = rtOut / rtIn;
     float dzDrtScale = md.tanSlope[md3] / alpha1GeVOut;
@@ -102,8 +102,8 @@ namespace lst {
     bool pass = ((zOut >= zLoPointed) && (zOut <= zHiPointed));
 
     float alpha_InLo = s.dPhiChanges[innerSeg];
-    float tl_axis_x = md.anchorX[md3] - md.anchorX[md1];
-    float tl_axis_y = md.anchorY[md3] - md.anchorY[md1];
+    float tl_axis_x = md.anchorPos[md3].x - md.anchorPos[md1].x;
+    float tl_axis_y = md.anchorPos[md3].y - md.anchorPos[md1].y;
     betaIn = alpha_InLo - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
     float drt_tl_axis = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
     const float rt_InSeg = segmentDr(md, md1, md2);
@@ -124,8 +124,8 @@ namespace lst {
                             float& betaIn) {
     bool isPSIn = (m.moduleType[lm1] == PS);
     bool isPSOut = (m.moduleType[lm3] == PS);
-    float rtIn = md.anchorRt[md1], rtMid = md.anchorRt[md2], rtOut = md.anchorRt[md3];
-    float zIn = md.anchorZ[md1], zMid = md.anchorZ[md2], zOut = md.anchorZ[md3];
+    float rtIn = md.anchorPos[md1].rt, rtMid = md.anchorPos[md2].rt, rtOut = md.anchorPos[md3].rt;
+    float zIn = md.anchorPos[md1].z, zMid = md.anchorPos[md2].z, zOut = md.anchorPos[md3].z;
     float alpha1GeV_OutLo = md.slope[md3];
     float dzDrtScale = md.tanSlope[md3] / alpha1GeV_OutLo;
     float zpitchIn = (isPSIn ? kPixelPSZpitch : kStrip2SZpitch);
@@ -165,11 +165,11 @@ namespace lst {
     drtErr = fsqrt(drtErr);
     bool pass = (kZ >= 0) && (rtOut >= rtLo) && (rtOut <= rtHi);
 
-    float rt_InLo = md.anchorRt[md1];
-    float rt_InOut = md.anchorRt[md2];
+    float rt_InLo = md.anchorPos[md1].rt;
+    float rt_InOut = md.anchorPos[md2].rt;
     float sdIn_alpha = s.dPhiChanges[innerSeg];
-    float tl_axis_x = md.anchorX[md3] - md.anchorX[md1];
-    float tl_axis_y = md.anchorY[md3] - md.anchorY[md1];
+    float tl_axis_x = md.anchorPos[md3].x - md.anchorPos[md1].x;
+    float tl_axis_y = md.anchorPos[md3].y - md.anchorPos[md1].y;
     betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
     float betaInRHmin = betaIn;
     float betaInRHmax = betaIn;
@@ -196,8 +196,8 @@ namespace lst {
                             unsigned int md3,
                             unsigned int innerSeg,
                             float& betaIn) {
-    float rtIn = md.anchorRt[md1], rtMid = md.anchorRt[md2], rtOut = md.anchorRt[md3];
-    float zIn = md.anchorZ[md1], zMid = md.anchorZ[md2], zOut = md.anchorZ[md3];
+    float rtIn = md.anchorPos[md1].rt, rtMid = md.anchorPos[md2].rt, rtOut = md.anchorPos[md3].rt;
+    float zIn = md.anchorPos[md1].z, zMid = md.anchorPos[md2].z, zOut = md.anchorPos[md3].z;
     float alpha1GeV_Out = md.slope[md3];
     float dzDrtScale = md.tanSlope[md3] / alpha1GeV_Out;
     if (!(zIn * zOut > 0))
@@ -234,11 +234,11 @@ namespace lst {
     if (isInSgInnerMDPS and isInSgOuterMDPS)
       pass = ((kZ >= 0) && (rtOut >= rtLo_point) && (rtOut <= rtHi_point));
 
-    float rt_InLo = md.anchorRt[md1];
-    float rt_InOut = md.anchorRt[md2];
+    float rt_InLo = md.anchorPos[md1].rt;
+    float rt_InOut = md.anchorPos[md2].rt;
     float sdIn_alpha = s.dPhiChanges[innerSeg];
-    float tl_axis_x = md.anchorX[md3] - md.anchorX[md1];
-    float tl_axis_y = md.anchorY[md3] - md.anchorY[md1];
+    float tl_axis_x = md.anchorPos[md3].x - md.anchorPos[md1].x;
+    float tl_axis_y = md.anchorPos[md3].y - md.anchorPos[md1].y;
     betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
     float sdIn_alphaRHmin = s.dPhiChangeMins[innerSeg];
     float sdIn_alphaRHmax = s.dPhiChangeMaxs[innerSeg];
@@ -309,12 +309,12 @@ namespace lst {
       pass = false;
     if (!pass)
       return false;
-    v.circleRadius = circleFrom3(md.anchorX[md1],
-                                 md.anchorY[md1],
-                                 md.anchorX[md2],
-                                 md.anchorY[md2],
-                                 md.anchorX[md3],
-                                 md.anchorY[md3],
+    v.circleRadius = circleFrom3(md.anchorPos[md1].x,
+                                 md.anchorPos[md1].y,
+                                 md.anchorPos[md2].x,
+                                 md.anchorPos[md2].y,
+                                 md.anchorPos[md3].x,
+                                 md.anchorPos[md3].y,
                                  v.circleCenterX,
                                  v.circleCenterY);
     return true;

@@ -87,8 +87,8 @@ namespace lst {
   LST_HD_BIG bool t4BBBB(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
     bool isPS_InLo = (m.moduleType[q.lmII] == PS);
     bool isPS_OutLo = (m.moduleType[q.lmOI] == PS);
-    float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
-    float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
+    float rt_InLo = md.anchorPos[q.md1].rt, rt_InOut = md.anchorPos[q.md2].rt, rt_OutLo = md.anchorPos[q.md3].rt;
+    float z_InLo = md.anchorPos[q.md1].z, z_InOut = md.anchorPos[q.md2].z, z_OutLo = md.anchorPos[q.md3].z;
     float alpha1GeV_OutLo = md.slope[q.md3];
     float rtRatio_OutLoInLo = rt_OutLo / rt_InLo;
     float dzDrtScale = md.tanSlope[q.md3] / alpha1GeV_OutLo;
@@ -124,10 +124,10 @@ namespace lst {
     float deltaPhiPos = phiMpiPi(md.anchorPhi[q.md4] - md.anchorPhi[q.md2]);
     if (!(fabs_(deltaPhiPos) <= sdlCut))
       return false;
-    float midPointX = 0.5f * (md.anchorX[q.md1] + md.anchorX[q.md3]);
-    float midPointY = 0.5f * (md.anchorY[q.md1] + md.anchorY[q.md3]);
-    float diffX = md.anchorX[q.md3] - md.anchorX[q.md1];
-    float diffY = md.anchorY[q.md3] - md.anchorY[q.md1];
+    float midPointX = 0.5f * (md.anchorPos[q.md1].x + md.anchorPos[q.md3].x);
+    float midPointY = 0.5f * (md.anchorPos[q.md1].y + md.anchorPos[q.md3].y);
+    float diffX = md.anchorPos[q.md3].x - md.anchorPos[q.md1].x;
+    float diffY = md.anchorPos[q.md3].y - md.anchorPos[q.md1].y;
     float dPhi = deltaPhi(midPointX, midPointY, diffX, diffY);
     if (!(fabs_(dPhi) <= sdlCut))
       return false;
@@ -135,10 +135,10 @@ namespace lst {
     float alpha_InLo = s.dPhiChanges[q.innerSeg];
     float alpha_OutLo = s.dPhiChanges[q.outerSeg];
     bool isEC_lastLayer = m.subdets[q.lmOO] == Endcap and m.moduleType[q.lmOO] == TwoS;
-    float alpha_OutUp = phiMpiPi(phiOf(md.anchorX[q.md4] - md.anchorX[q.md3], md.anchorY[q.md4] - md.anchorY[q.md3]) -
+    float alpha_OutUp = phiMpiPi(phiOf(md.anchorPos[q.md4].x - md.anchorPos[q.md3].x, md.anchorPos[q.md4].y - md.anchorPos[q.md3].y) -
                                  md.anchorPhi[q.md4]);
-    float tl_axis_x = md.anchorX[q.md4] - md.anchorX[q.md1];
-    float tl_axis_y = md.anchorY[q.md4] - md.anchorY[q.md1];
+    float tl_axis_x = md.anchorPos[q.md4].x - md.anchorPos[q.md1].x;
+    float tl_axis_y = md.anchorPos[q.md4].y - md.anchorPos[q.md1].y;
     float betaIn = alpha_InLo - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[q.md1]);
     float betaInRHmin = betaIn;
     float betaInRHmax = betaIn;
@@ -147,15 +147,15 @@ namespace lst {
     float betaOutRHmax = betaOut;
     if (isEC_lastLayer) {
       float alpha_OutUp_highEdge =
-          phiMpiPi(phiOf(md.anchorHighEdgeX[q.md4] - md.anchorX[q.md3], md.anchorHighEdgeY[q.md4] - md.anchorY[q.md3]) -
+          phiMpiPi(phiOf(md.anchorHighEdgeX[q.md4] - md.anchorPos[q.md3].x, md.anchorHighEdgeY[q.md4] - md.anchorPos[q.md3].y) -
                    md.anchorHighEdgePhi[q.md4]);
       float alpha_OutUp_lowEdge =
-          phiMpiPi(phiOf(md.anchorLowEdgeX[q.md4] - md.anchorX[q.md3], md.anchorLowEdgeY[q.md4] - md.anchorY[q.md3]) -
+          phiMpiPi(phiOf(md.anchorLowEdgeX[q.md4] - md.anchorPos[q.md3].x, md.anchorLowEdgeY[q.md4] - md.anchorPos[q.md3].y) -
                    md.anchorLowEdgePhi[q.md4]);
-      float tl_axis_highEdge_x = md.anchorHighEdgeX[q.md4] - md.anchorX[q.md1];
-      float tl_axis_highEdge_y = md.anchorHighEdgeY[q.md4] - md.anchorY[q.md1];
-      float tl_axis_lowEdge_x = md.anchorLowEdgeX[q.md4] - md.anchorX[q.md1];
-      float tl_axis_lowEdge_y = md.anchorLowEdgeY[q.md4] - md.anchorY[q.md1];
+      float tl_axis_highEdge_x = md.anchorHighEdgeX[q.md4] - md.anchorPos[q.md1].x;
+      float tl_axis_highEdge_y = md.anchorHighEdgeY[q.md4] - md.anchorPos[q.md1].y;
+      float tl_axis_lowEdge_x = md.anchorLowEdgeX[q.md4] - md.anchorPos[q.md1].x;
+      float tl_axis_lowEdge_y = md.anchorLowEdgeY[q.md4] - md.anchorPos[q.md1].y;
       betaOutRHmin = -alpha_OutUp_highEdge +
                      phiMpiPi(phiOf(tl_axis_highEdge_x, tl_axis_highEdge_y) - md.anchorHighEdgePhi[q.md4]);
       betaOutRHmax =
@@ -175,7 +175,7 @@ namespace lst {
     int lIn = 5;
     int lOut = isEC_lastLayer ? 11 : 5;
     float sdOut_dr = segmentDr(md, q.md3, q.md4);
-    float sdOut_d = md.anchorRt[q.md4] - md.anchorRt[q.md3];
+    float sdOut_d = md.anchorPos[q.md4].rt - md.anchorPos[q.md3].rt;
     deltaBetaIterations(betaIn, betaOut, betaAv, pt_beta, rt_InSeg, sdOut_dr, drt_tl_axis, lIn);
 
     const float betaInMMSF =
@@ -218,8 +218,8 @@ namespace lst {
   LST_HD_BIG bool t4BBEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
     bool isPS_InLo = (m.moduleType[q.lmII] == PS);
     bool isPS_OutLo = (m.moduleType[q.lmOI] == PS);
-    float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
-    float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
+    float rt_InLo = md.anchorPos[q.md1].rt, rt_InOut = md.anchorPos[q.md2].rt, rt_OutLo = md.anchorPos[q.md3].rt;
+    float z_InLo = md.anchorPos[q.md1].z, z_InOut = md.anchorPos[q.md2].z, z_OutLo = md.anchorPos[q.md3].z;
     float alpha1GeV_OutLo = md.slope[q.md3];
     float dzDrtScale = md.tanSlope[q.md3] / alpha1GeV_OutLo;
     float zpitch_InLo = (isPS_InLo ? kPixelPSZpitch : kStrip2SZpitch);
@@ -266,10 +266,10 @@ namespace lst {
     float deltaPhiPos = phiMpiPi(md.anchorPhi[q.md4] - md.anchorPhi[q.md2]);
     if (!(fabs_(deltaPhiPos) <= sdlCut))
       return false;
-    float midPointX = 0.5f * (md.anchorX[q.md1] + md.anchorX[q.md3]);
-    float midPointY = 0.5f * (md.anchorY[q.md1] + md.anchorY[q.md3]);
-    float diffX = md.anchorX[q.md3] - md.anchorX[q.md1];
-    float diffY = md.anchorY[q.md3] - md.anchorY[q.md1];
+    float midPointX = 0.5f * (md.anchorPos[q.md1].x + md.anchorPos[q.md3].x);
+    float midPointY = 0.5f * (md.anchorPos[q.md1].y + md.anchorPos[q.md3].y);
+    float diffX = md.anchorPos[q.md3].x - md.anchorPos[q.md1].x;
+    float diffY = md.anchorPos[q.md3].y - md.anchorPos[q.md1].y;
     float dPhi = deltaPhi(midPointX, midPointY, diffX, diffY);
     if (!(fabs_(dPhi) <= sdlCut))
       return false;
@@ -278,12 +278,12 @@ namespace lst {
     float sdIn_alpha_min = s.dPhiChangeMins[q.innerSeg];
     float sdIn_alpha_max = s.dPhiChangeMaxs[q.innerSeg];
     float sdOut_alpha = sdIn_alpha;
-    float sdOut_alphaOut = phiMpiPi(phiOf(md.anchorX[q.md4] - md.anchorX[q.md3], md.anchorY[q.md4] - md.anchorY[q.md3]) -
+    float sdOut_alphaOut = phiMpiPi(phiOf(md.anchorPos[q.md4].x - md.anchorPos[q.md3].x, md.anchorPos[q.md4].y - md.anchorPos[q.md3].y) -
                                     md.anchorPhi[q.md4]);
     float sdOut_alphaOut_min = phiMpiPi(s.dPhiChangeMins[q.outerSeg] - s.dPhiMins[q.outerSeg]);
     float sdOut_alphaOut_max = phiMpiPi(s.dPhiChangeMaxs[q.outerSeg] - s.dPhiMaxs[q.outerSeg]);
-    float tl_axis_x = md.anchorX[q.md4] - md.anchorX[q.md1];
-    float tl_axis_y = md.anchorY[q.md4] - md.anchorY[q.md1];
+    float tl_axis_x = md.anchorPos[q.md4].x - md.anchorPos[q.md1].x;
+    float tl_axis_y = md.anchorPos[q.md4].y - md.anchorPos[q.md1].y;
     float betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[q.md1]);
     float betaInRHmin = betaIn;
     float betaInRHmax = betaIn;
@@ -322,7 +322,7 @@ namespace lst {
     float lIn = 5;
     float lOut = 11;
     float sdOut_dr = segmentDr(md, q.md3, q.md4);
-    float sdOut_d = md.anchorRt[q.md4] - md.anchorRt[q.md3];
+    float sdOut_d = md.anchorPos[q.md4].rt - md.anchorPos[q.md3].rt;
     deltaBetaIterations(betaIn, betaOut, betaAv, pt_beta, sdIn_dr, sdOut_dr, dr, lIn);
 
     const float betaInMMSF =
@@ -362,8 +362,8 @@ namespace lst {
 
   // Endcap-endcap-endcap-endcap (SDL/Quintuplet.h:2031-2297).
   LST_HD_BIG bool t4EEEE(const Modules& m, const MiniDoublets& md, const Segments& s, const T4Input& q) {
-    float rt_InLo = md.anchorRt[q.md1], rt_InOut = md.anchorRt[q.md2], rt_OutLo = md.anchorRt[q.md3];
-    float z_InLo = md.anchorZ[q.md1], z_InOut = md.anchorZ[q.md2], z_OutLo = md.anchorZ[q.md3];
+    float rt_InLo = md.anchorPos[q.md1].rt, rt_InOut = md.anchorPos[q.md2].rt, rt_OutLo = md.anchorPos[q.md3].rt;
+    float z_InLo = md.anchorPos[q.md1].z, z_InOut = md.anchorPos[q.md2].z, z_OutLo = md.anchorPos[q.md3].z;
     float alpha1GeV_OutLo = md.slope[q.md3];
     float dzDrtScale = md.tanSlope[q.md3] / alpha1GeV_OutLo;
     if (!((z_InLo * z_OutLo) > 0))
@@ -407,10 +407,10 @@ namespace lst {
     float deltaPhiPos = phiMpiPi(md.anchorPhi[q.md4] - md.anchorPhi[q.md2]);
     if (!(fabs_(deltaPhiPos) <= sdlCut))
       return false;
-    float midPointX = 0.5f * (md.anchorX[q.md1] + md.anchorX[q.md3]);
-    float midPointY = 0.5f * (md.anchorY[q.md1] + md.anchorY[q.md3]);
-    float diffX = md.anchorX[q.md3] - md.anchorX[q.md1];
-    float diffY = md.anchorY[q.md3] - md.anchorY[q.md1];
+    float midPointX = 0.5f * (md.anchorPos[q.md1].x + md.anchorPos[q.md3].x);
+    float midPointY = 0.5f * (md.anchorPos[q.md1].y + md.anchorPos[q.md3].y);
+    float diffX = md.anchorPos[q.md3].x - md.anchorPos[q.md1].x;
+    float diffY = md.anchorPos[q.md3].y - md.anchorPos[q.md1].y;
     float dPhi = deltaPhi(midPointX, midPointY, diffX, diffY);
     if (!((fabs_(dPhi) <= sdlCut)))
       return false;
@@ -424,8 +424,8 @@ namespace lst {
     float sdOut_alphaOutRHmin = phiMpiPi(sdOut_dPhiChange_min - sdOut_dPhiPos);
     float sdOut_alphaOutRHmax = phiMpiPi(sdOut_dPhiChange_max - sdOut_dPhiPos);
     float sdOut_alphaOut = phiMpiPi(sdOut_dPhiChange - sdOut_dPhiPos);
-    float tl_axis_x = md.anchorX[q.md4] - md.anchorX[q.md1];
-    float tl_axis_y = md.anchorY[q.md4] - md.anchorY[q.md1];
+    float tl_axis_x = md.anchorPos[q.md4].x - md.anchorPos[q.md1].x;
+    float tl_axis_y = md.anchorPos[q.md4].y - md.anchorPos[q.md1].y;
     float betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[q.md1]);
     float sdIn_alphaRHmin = s.dPhiChangeMins[q.innerSeg];
     float sdIn_alphaRHmax = s.dPhiChangeMaxs[q.innerSeg];
@@ -459,7 +459,7 @@ namespace lst {
     int lIn = 11;
     int lOut = 13;
     float sdOut_dr = segmentDr(md, q.md3, q.md4);
-    float sdOut_d = md.anchorRt[q.md4] - md.anchorRt[q.md3];
+    float sdOut_d = md.anchorPos[q.md4].rt - md.anchorPos[q.md3].rt;
     deltaBetaIterations(betaIn, betaOut, betaAv, pt_beta, sdIn_dr, sdOut_dr, dr, lIn);
 
     const float betaInMMSF =
@@ -602,31 +602,31 @@ namespace lst {
                        float g,
                        float f,
                        bool& tightCutFlag) {
-    const float rt1 = md.anchorRt[mdIdx[0]] / 100, rt2 = md.anchorRt[mdIdx[1]] / 100, rt3 = md.anchorRt[mdIdx[2]] / 100,
-                rt4 = md.anchorRt[mdIdx[3]] / 100, rt5 = md.anchorRt[mdIdx[4]] / 100;
-    const float z1 = md.anchorZ[mdIdx[0]] / 100, z2 = md.anchorZ[mdIdx[1]] / 100, z3 = md.anchorZ[mdIdx[2]] / 100,
-                z4 = md.anchorZ[mdIdx[3]] / 100, z5 = md.anchorZ[mdIdx[4]] / 100;
+    const float rt1 = md.anchorPos[mdIdx[0]].rt / 100, rt2 = md.anchorPos[mdIdx[1]].rt / 100, rt3 = md.anchorPos[mdIdx[2]].rt / 100,
+                rt4 = md.anchorPos[mdIdx[3]].rt / 100, rt5 = md.anchorPos[mdIdx[4]].rt / 100;
+    const float z1 = md.anchorPos[mdIdx[0]].z / 100, z2 = md.anchorPos[mdIdx[1]].z / 100, z3 = md.anchorPos[mdIdx[2]].z / 100,
+                z4 = md.anchorPos[mdIdx[3]].z / 100, z5 = md.anchorPos[mdIdx[4]].z / 100;
     const int layer1 = m.sdlLayers[lm[0]], layer2 = m.sdlLayers[lm[1]], layer3 = m.sdlLayers[lm[2]],
               layer4 = m.sdlLayers[lm[3]], layer5 = m.sdlLayers[lm[4]];
     const int moduleType1 = m.moduleType[lm[0]], moduleType2 = m.moduleType[lm[1]], moduleType3 = m.moduleType[lm[2]],
               moduleType4 = m.moduleType[lm[3]], moduleType5 = m.moduleType[lm[4]];
-    const float x1 = md.anchorX[mdIdx[0]] / 100, x2 = md.anchorX[mdIdx[1]] / 100, x3 = md.anchorX[mdIdx[2]] / 100,
-                x4 = md.anchorX[mdIdx[3]] / 100;
-    const float y1 = md.anchorY[mdIdx[0]] / 100, y2 = md.anchorY[mdIdx[1]] / 100, y3 = md.anchorY[mdIdx[2]] / 100,
-                y4 = md.anchorY[mdIdx[3]] / 100;
+    const float x1 = md.anchorPos[mdIdx[0]].x / 100, x2 = md.anchorPos[mdIdx[1]].x / 100, x3 = md.anchorPos[mdIdx[2]].x / 100,
+                x4 = md.anchorPos[mdIdx[3]].x / 100;
+    const float y1 = md.anchorPos[mdIdx[0]].y / 100, y2 = md.anchorPos[mdIdx[1]].y / 100, y3 = md.anchorPos[mdIdx[2]].y / 100,
+                y4 = md.anchorPos[mdIdx[3]].y / 100;
 
     float residual = 0;
     float error = 0;
     float x_center = g / 100, y_center = f / 100;
-    float x_init = md.anchorX[mdIdx[2]] / 100;
-    float y_init = md.anchorY[mdIdx[2]] / 100;
-    float z_init = md.anchorZ[mdIdx[2]] / 100;
-    float rt_init = md.anchorRt[mdIdx[2]] / 100;
+    float x_init = md.anchorPos[mdIdx[2]].x / 100;
+    float y_init = md.anchorPos[mdIdx[2]].y / 100;
+    float z_init = md.anchorPos[mdIdx[2]].z / 100;
+    float rt_init = md.anchorPos[mdIdx[2]].rt / 100;
     if (moduleType3 == 1) {
-      x_init = md.anchorX[mdIdx[1]] / 100;
-      y_init = md.anchorY[mdIdx[1]] / 100;
-      z_init = md.anchorZ[mdIdx[1]] / 100;
-      rt_init = md.anchorRt[mdIdx[1]] / 100;
+      x_init = md.anchorPos[mdIdx[1]].x / 100;
+      y_init = md.anchorPos[mdIdx[1]].y / 100;
+      z_init = md.anchorPos[mdIdx[1]].z / 100;
+      rt_init = md.anchorPos[mdIdx[1]].rt / 100;
     }
 
     int charge = 0;
@@ -1163,7 +1163,7 @@ namespace lst {
       unsigned int mi = mdIdx[slot];
       x[k + 0] = md.anchorEta[mi];
       x[k + 1] = md.anchorPhi[mi];
-      x[k + 2] = md.anchorZ[mi];
+      x[k + 2] = md.anchorPos[mi].z;
       x[k + 3] = fsqrt(xVec[slot] * xVec[slot] + yVec[slot] * yVec[slot]);
       x[k + 4] = float(m.layers[lm[slot]] + 6 * is_endcap[slot]);
     };
@@ -1271,8 +1271,8 @@ namespace lst {
     float* xs = st.xs;
     float* ys = st.ys;
     for (int i = 0; i < 5; ++i) {
-      xs[i] = md.anchorX[mdIdx[i]];
-      ys[i] = md.anchorY[mdIdx[i]];
+      xs[i] = md.anchorPos[mdIdx[i]].x;
+      ys[i] = md.anchorPos[mdIdx[i]].y;
     }
     float g, f;
     v.outerRadius = t.circleRadius[outerT3];
