@@ -62,7 +62,9 @@ namespace lst {
     unsigned int t5DnnCount;      // candidates buffered for kT5Dnn
     unsigned int pixQueueCount;   // candidates passing the pixel pre-selection
     unsigned int t5QueueCount;    // candidates passing the quintuplet pre-selection
-    unsigned int pad[1];
+    unsigned int pixQueueBack;    // pixel candidates queued from the back (endcap tracklet algorithm)
+    unsigned int t5QueueBack;     // quintuplet candidates queued from the back (modules not all barrel)
+    unsigned int pad[3];
   };
 
   // All device pointers of one event.

@@ -862,6 +862,7 @@ namespace lst {
       ev.sc->t5PassCount = 0;
       ev.sc->t5DnnCount = 0;
       ev.sc->t5QueueCount = 0;
+      ev.sc->t5QueueBack = 0;
     }
   }
 
@@ -892,7 +893,9 @@ namespace lst {
   // gets its flag here; the survivors are queued in any order for kT5Eval,
   // which then runs the long tests with all lanes of a warp busy (a
   // candidate's outcome does not depend on the thread that evaluates it).
-  // A full queue makes kT5Eval evaluate every candidate.
+  // Candidates on all-barrel module patterns fill the queue from the front,
+  // the others from the back, so that a warp mostly runs one set of the
+  // tracklet algorithms.  A full queue makes kT5Eval evaluate every candidate.
   __global__ void __launch_bounds__(256) kT5Pre(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow)
@@ -901,7 +904,7 @@ namespace lst {
     const unsigned int stride = gridDim.x * blockDim.x;
     for (unsigned int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
       const unsigned int c = base + laneId();
-      bool pass = false;
+      bool pass = false, mixed = false;
       if (c < total) {
         unsigned int innerT3, outerT3;
         uint16_t lm[5];
@@ -911,17 +914,28 @@ namespace lst {
         pass = t5RadiusStage(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st);
         if (!pass)
           ev.t5CandFlag[c] = 0;
+        else
+          mixed = st.kind > 0;
       }
-      const unsigned int mask = __ballot_sync(kFullMask, pass);
-      if (mask == 0u)
+      const unsigned int maskF = __ballot_sync(kFullMask, pass && !mixed);
+      const unsigned int maskB = __ballot_sync(kFullMask, pass && mixed);
+      if ((maskF | maskB) == 0u)
         continue;
-      unsigned int start = 0;
-      if (laneId() == 0)
-        start = atomicAdd(&ev.sc->t5QueueCount, __popc(mask));
-      start = __shfl_sync(kFullMask, start, 0);
-      const unsigned int pos = start + __popc(mask & lanesBelowMask());
-      if (pass && pos < kCandQueueCap)
-        ev.candQueue[pos] = c;
+      unsigned int startF = 0, startB = 0;
+      if (laneId() == 0) {
+        if (maskF)
+          startF = atomicAdd(&ev.sc->t5QueueCount, __popc(maskF));
+        if (maskB)
+          startB = atomicAdd(&ev.sc->t5QueueBack, __popc(maskB));
+      }
+      startF = __shfl_sync(kFullMask, startF, 0);
+      startB = __shfl_sync(kFullMask, startB, 0);
+      if (pass) {
+        const unsigned int k = mixed ? startB + __popc(maskB & lanesBelowMask())
+                                     : startF + __popc(maskF & lanesBelowMask());
+        if (k < kCandQueueCap)
+          ev.candQueue[mixed ? kCandQueueCap - 1 - k : k] = c;
+      }
     }
   }
 
@@ -930,12 +944,12 @@ namespace lst {
     if (ev.sc->t5CandOverflow)
       return;
     const unsigned int total = ev.sc->t5CandTotal;
-    const unsigned int queued = ev.sc->t5QueueCount;
-    const bool fromQueue = queued <= kCandQueueCap;
-    const unsigned int n = fromQueue ? queued : total;
+    const unsigned int front = ev.sc->t5QueueCount, back = ev.sc->t5QueueBack;
+    const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
+    const unsigned int n = fromQueue ? front + back : total;
     ConstDnn dnn;
     for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-      const unsigned int c = fromQueue ? ev.candQueue[q] : q;
+      const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
       unsigned int innerT3, outerT3;
       uint16_t lm[5];
       t5Decode(ev, c, innerT3, outerT3, lm);
@@ -1993,6 +2007,7 @@ namespace lst {
       ev.sc->pixCandTotal = carry;
       ev.sc->pixPassCount = 0;
       ev.sc->pixQueueCount = 0;
+      ev.sc->pixQueueBack = 0;
     }
   }
 
@@ -2032,8 +2047,10 @@ namespace lst {
   // which most candidates fail.  The survivors are queued in any order, so
   // that kPixEval runs its long selection with all lanes of a warp busy; the
   // outcome of a candidate does not depend on which thread evaluates it, and
-  // the passing ones are ranked by candidate index afterwards.  A full queue
-  // makes kPixEval evaluate every candidate instead.
+  // the passing ones are ranked by candidate index afterwards.  Candidates
+  // whose first pixel tracklet takes the barrel algorithm fill the queue from
+  // the front, the endcap ones from the back, so that a warp mostly runs one
+  // of the two.  A full queue makes kPixEval evaluate every candidate instead.
   template <int K>
   __global__ void __launch_bounds__(256) kPixPre(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
@@ -2042,28 +2059,38 @@ namespace lst {
     const unsigned int stride = gridDim.x * blockDim.x;
     for (unsigned int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
       const unsigned int c = base + laneId();
-      bool pass = false;
+      bool pass = false, endcap = false;
       if (c < total) {
         unsigned int iPLS, obj;
         uint16_t mod;
         pixCandidate<K>(es, ev, c, iPLS, obj, mod);
+        const unsigned int t3 = K == 5 ? ev.t5.tripletIndices[2 * obj] : obj;
         if (K == 5)
-          pass = !ev.t5.isDup[obj] &&
-                 pt3RadiusPass(es.m, ev.rg, ev.ls, ev.t3, plsBase + iPLS, ev.t5.tripletIndices[2 * obj]);
+          pass = !ev.t5.isDup[obj] && pt3RadiusPass(es.m, ev.rg, ev.ls, ev.t3, plsBase + iPLS, t3);
         else
           pass = es.m.moduleType[ev.t3.lowerModuleIndices[3 * obj + 1]] != TwoS && !ev.t3.partOfPT5[obj] &&
                  pt3RadiusPass(es.m, ev.rg, ev.ls, ev.t3, plsBase + iPLS, obj);
+        endcap = es.m.subdets[ev.t3.lowerModuleIndices[3 * t3]] == Endcap;
       }
-      const unsigned int mask = __ballot_sync(kFullMask, pass);
-      if (mask == 0u)
+      const unsigned int maskF = __ballot_sync(kFullMask, pass && !endcap);
+      const unsigned int maskB = __ballot_sync(kFullMask, pass && endcap);
+      if ((maskF | maskB) == 0u)
         continue;
-      unsigned int start = 0;
-      if (laneId() == 0)
-        start = atomicAdd(&ev.sc->pixQueueCount, __popc(mask));
-      start = __shfl_sync(kFullMask, start, 0);
-      const unsigned int pos = start + __popc(mask & lanesBelowMask());
-      if (pass && pos < kCandQueueCap)
-        ev.candQueue[pos] = c;
+      unsigned int startF = 0, startB = 0;
+      if (laneId() == 0) {
+        if (maskF)
+          startF = atomicAdd(&ev.sc->pixQueueCount, __popc(maskF));
+        if (maskB)
+          startB = atomicAdd(&ev.sc->pixQueueBack, __popc(maskB));
+      }
+      startF = __shfl_sync(kFullMask, startF, 0);
+      startB = __shfl_sync(kFullMask, startB, 0);
+      if (pass) {
+        const unsigned int k = endcap ? startB + __popc(maskB & lanesBelowMask())
+                                      : startF + __popc(maskF & lanesBelowMask());
+        if (k < kCandQueueCap)
+          ev.candQueue[endcap ? kCandQueueCap - 1 - k : k] = c;
+      }
     }
   }
 
@@ -2071,12 +2098,12 @@ namespace lst {
   __global__ void __launch_bounds__(LST_LB_EVAL) kPixEval(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int total = ev.sc->pixCandTotal;
-    const unsigned int queued = ev.sc->pixQueueCount;
-    const bool fromQueue = queued <= kCandQueueCap;
-    const unsigned int n = fromQueue ? queued : total;
+    const unsigned int front = ev.sc->pixQueueCount, back = ev.sc->pixQueueBack;
+    const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
+    const unsigned int n = fromQueue ? front + back : total;
     const unsigned int plsBase = es.lsOffset[es.nLowerModules];
     for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-      const unsigned int c = fromQueue ? ev.candQueue[q] : q;
+      const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
       unsigned int iPLS, obj;
       uint16_t mod;
       pixCandidate<K>(es, ev, c, iPLS, obj, mod);

@@ -1238,6 +1238,7 @@ namespace lst {
     unsigned int mdIdx[5];
     float xs[5], ys[5];
     bool tight;  // the rz fit's tight flag
+    int kind;    // barrel/endcap pattern of the five modules (0: all barrel ... 7)
   };
 
   // Every test before the classifier decision, and the circle regression.
@@ -1301,6 +1302,7 @@ namespace lst {
       kind = 6;
     else
       kind = 7;
+    st.kind = kind;
     // Radius spreads over the strip ends of 2S endcap hits; only the tests of
     // kinds >= 2 read them (the reference's third, outer spread is unused).
     float innerRadiusMin2S = 0.f, innerRadiusMax2S = 0.f, bridgeRadiusMin2S = 0.f, bridgeRadiusMax2S = 0.f;
