@@ -39,7 +39,7 @@ def test_autotune_keeps_outputs_and_limits(es, events, tmp_path):
         s.autotune(0, len(events), cache)
         shapes = s.launch_shapes()
         limits = {"kCreateMD": 8, "kMDDerived": 8, "kCreateLS": 4, "kCreateT3": 4, "kT5Eval": 4, "kPixEval<5>": 4,
-                  "kPixEval<3>": 4}
+                  "kPixEval<3>": 4, "kPixMid<5>": 4, "kPixMid<3>": 4}
         assert set(shapes) == set(limits)
         for k, (w, p) in shapes.items():
             assert 1 <= w <= limits[k] and 1 <= p <= 256, (k, w, p)

@@ -64,7 +64,8 @@ namespace lst {
     unsigned int t5QueueCount;    // candidates passing the quintuplet pre-selection
     unsigned int pixQueueBack;    // pixel candidates queued from the back (endcap tracklet algorithm)
     unsigned int t5QueueBack;     // quintuplet candidates queued from the back (modules not all barrel)
-    unsigned int pad[3];
+    unsigned int pixQueue2Count;  // pixel candidates passing the first pixel tracklet as well
+    unsigned int pad[2];
   };
 
   // All device pointers of one event.

@@ -276,7 +276,7 @@ namespace {
   // blocks_per_sm x SMs / events blocks per event).  Their results do not
   // depend on the shape: each module / candidate is processed the same way by
   // whichever warp takes it.
-  enum TunedKernel { kTuMD, kTuMDDerived, kTuLS, kTuT3, kTuT5Eval, kTuPix5, kTuPix3, kTuCount };
+  enum TunedKernel { kTuMD, kTuMDDerived, kTuLS, kTuT3, kTuT5Eval, kTuPix5, kTuPix3, kTuMid5, kTuMid3, kTuCount };
   struct TuneSpec {
     const char* name;  // as it appears in the launch profile
     int maxWarps;      // the kernel's launch bounds / per-warp shared memory
@@ -284,7 +284,7 @@ namespace {
   };
   const TuneSpec kTuneSpecs[kTuCount] = {{"kCreateMD", 8, 8},   {"kMDDerived", 8, 8},   {"kCreateLS", 4, 4},
                                          {"kCreateT3", 4, 4},   {"kT5Eval", 4, 4},      {"kPixEval<5>", 4, 4},
-                                         {"kPixEval<3>", 4, 4}};
+                                         {"kPixEval<3>", 4, 4}, {"kPixMid<5>", 4, 4},    {"kPixMid<3>", 4, 4}};
   constexpr int kDefaultBlocksPerSM = 16;
   struct LaunchShape {
     int warps = 4;
@@ -479,6 +479,7 @@ namespace {
         LST_LAUNCH(lst::kPixPrefix<5>, warpGrid(P, 8, count), 256, d, v);
         LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
         LST_LAUNCH(lst::kPixPre<5>, dim3(blocksFor(size_t(1) << 20, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPixMid<5>, tunedFlatGrid(ev, kTuMid5, count), tunedThreads(ev, kTuMid5), d, v);
         LST_LAUNCH(lst::kPixEval<5>, tunedFlatGrid(ev, kTuPix5, count), tunedThreads(ev, kTuPix5), d, v);
         LST_LAUNCH(lst::kPixRankEmit<5>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
@@ -494,6 +495,7 @@ namespace {
         LST_LAUNCH(lst::kPixPrefix<3>, warpGrid(P, 8, count), 256, d, v);
         LST_LAUNCH(lst::kPixScan, one, 1024, d, v);
         LST_LAUNCH(lst::kPixPre<3>, dim3(blocksFor(size_t(1) << 20, count), count), kThreads, d, v);
+        LST_LAUNCH(lst::kPixMid<3>, tunedFlatGrid(ev, kTuMid3, count), tunedThreads(ev, kTuMid3), d, v);
         LST_LAUNCH(lst::kPixEval<3>, tunedFlatGrid(ev, kTuPix3, count), tunedThreads(ev, kTuPix3), d, v);
         LST_LAUNCH(lst::kPixRankEmit<3>, one, 1024, d, v);
         LST_LAUNCH(lst::kPT3Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
@@ -613,6 +615,8 @@ namespace {
         {"kPixEval<5>", (const void*)lst::kPixEval<5>},
         {"kPixPre<5>", (const void*)lst::kPixPre<5>},
         {"kT5Pre", (const void*)lst::kT5Pre},
+        {"kPixMid<5>", (const void*)lst::kPixMid<5>},
+        {"kPixMid<3>", (const void*)lst::kPixMid<3>},
         {"kPixPre<3>", (const void*)lst::kPixPre<3>},
         {"kPixEval<3>", (const void*)lst::kPixEval<3>},
         {"kPixRankEmit<5>", (const void*)lst::kPixRankEmit<5>},

@@ -2008,6 +2008,7 @@ namespace lst {
       ev.sc->pixPassCount = 0;
       ev.sc->pixQueueCount = 0;
       ev.sc->pixQueueBack = 0;
+      ev.sc->pixQueue2Count = 0;
     }
   }
 
@@ -2094,16 +2095,59 @@ namespace lst {
     }
   }
 
+  // Second pre-selection stage: the first pixel tracklet algorithm (of the
+  // pLS with the triplet's, or the quintuplet's inner triplet's, inner
+  // segment), the long test that few queued candidates pass.  Its survivors
+  // are queued again, between the two ends of the first queue; without room
+  // there, kPixEval takes the first queue instead.
+  template <int K>
+  __global__ void __launch_bounds__(LST_LB_EVAL) kPixMid(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int front = ev.sc->pixQueueCount, back = ev.sc->pixQueueBack;
+    if (!(front <= kCandQueueCap && back <= kCandQueueCap - front))
+      return;
+    const unsigned int n = front + back, room = kCandQueueCap - n;
+    const unsigned int plsBase = es.lsOffset[es.nLowerModules];
+    const unsigned int stride = gridDim.x * blockDim.x;
+    for (unsigned int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+      const unsigned int q = base + laneId();
+      bool pass = false;
+      unsigned int c = 0;
+      if (q < n) {
+        c = ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)];
+        unsigned int iPLS, obj;
+        uint16_t mod;
+        pixCandidate<K>(es, ev, c, iPLS, obj, mod);
+        const unsigned int t3 = K == 5 ? ev.t5.tripletIndices[2 * obj] : obj;
+        pass = pt3FirstTracklet(es.m, ev.rg, ev.md, ev.ls, ev.t3, plsBase + iPLS, t3);
+      }
+      const unsigned int mask = __ballot_sync(kFullMask, pass);
+      if (mask == 0u)
+        continue;
+      unsigned int start = 0;
+      if (laneId() == 0)
+        start = atomicAdd(&ev.sc->pixQueue2Count, __popc(mask));
+      start = __shfl_sync(kFullMask, start, 0);
+      const unsigned int k = start + __popc(mask & lanesBelowMask());
+      if (pass && k < room)
+        ev.candQueue[front + k] = c;
+    }
+  }
+
   template <int K>
   __global__ void __launch_bounds__(LST_LB_EVAL) kPixEval(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int total = ev.sc->pixCandTotal;
     const unsigned int front = ev.sc->pixQueueCount, back = ev.sc->pixQueueBack;
     const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
-    const unsigned int n = fromQueue ? front + back : total;
+    const unsigned int n2 = ev.sc->pixQueue2Count;
+    const bool fromQueue2 = fromQueue && n2 <= kCandQueueCap - front - back;
+    const unsigned int n = fromQueue2 ? n2 : (fromQueue ? front + back : total);
     const unsigned int plsBase = es.lsOffset[es.nLowerModules];
     for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-      const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
+      const unsigned int c = fromQueue2  ? ev.candQueue[front + q]
+                             : fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)]
+                                         : q;
       unsigned int iPLS, obj;
       uint16_t mod;
       pixCandidate<K>(es, ev, c, iPLS, obj, mod);

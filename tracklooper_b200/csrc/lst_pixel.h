@@ -544,6 +544,15 @@ namespace lst {
     return pt3RadiusCriterion(kind, pixelRadius, pixelRadiusError, t.circleRadius[t3]);
   }
 
+  // The second test of pt3Select below, alone: the pixel tracklet algorithm
+  // of the pLS with the triplet's inner segment.
+  LST_HD bool pt3FirstTracklet(const Modules& m, const Ranges& rg, const MiniDoublets& md, const Segments& s,
+                               const Triplets& t, unsigned int plsIndex, unsigned int t3) {
+    const uint16_t pixelModule = s.innerLowerModuleIndices[plsIndex];
+    return ptPixelTracklet(m, rg, md, s, pixelModule, t.lowerModuleIndices[3 * t3], t.lowerModuleIndices[3 * t3 + 1],
+                           plsIndex, t.segmentIndices[2 * t3]);
+  }
+
   // pLS x T3 selection (SDL/PixelTriplet.h:826-1023).
   LST_HD bool pt3Select(const Modules& m,
                         const Ranges& rg,
