@@ -237,6 +237,20 @@ int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, siz
  * host-to-device copy), for re-running events whose inputs are already
  * resident on the device.  The slots must lie inside the last upload. */
 int lst_batch_ingest(lst_event* ev, int first, int count);
+/* Input staging that overlaps the next batch's host-to-device copy with the
+ * current batch's stages (no reference counterpart).  lst_batch_stage starts
+ * the copy of packed events (the lst_batch_upload layout, or with
+ * seed_layout = 1 the lst_batch_upload_seeds one) into one of two device
+ * staging buffers on the set's own copy stream and returns at once; blobs
+ * must be pinned host memory (pageable memory is copied synchronously) and
+ * must stay unchanged until the copy has run.  lst_batch_ingest_staged makes
+ * the set's stream wait for that copy and ingests the staged events into
+ * their slots, as lst_batch_upload does after its copy.  One batch can be
+ * staged at a time; staging the next one while the current one runs its
+ * stages (and before reading its output) hides the copy. */
+int lst_batch_stage(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                    const uint64_t* blob_offsets, int seed_layout);
+int lst_batch_ingest_staged(lst_event* ev);
 /* Runs stages [first_stage, last_stage] for slots [first, first + count). */
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage);
 /* As lst_batch_run, replayed from a CUDA graph: the first call for a given

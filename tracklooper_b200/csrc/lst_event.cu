@@ -311,10 +311,27 @@ struct lst_event {
   // batched-input staging: the last upload's packed events (kind 0: the
   // Event-API layout of lst_batch_upload, 1: CMSSW seeds of
   // lst_batch_upload_seeds) for slots [inboxFirst, inboxFirst + inboxCount)
-  unsigned char* inbox = nullptr;
+  unsigned char* inbox = nullptr;          // current input source of ingestInbox
+  unsigned long long* dOffsets = nullptr;  //   and its per-slot blob offsets
+  unsigned char* ownInbox = nullptr;       // the buffer of lst_batch_upload*
   size_t inboxBytes = 0;
+  unsigned long long* ownOffsets = nullptr;
   size_t inboxUsed = 0;
-  unsigned long long* dOffsets = nullptr;
+  // double-buffered staging of lst_batch_stage on its own copy stream
+  struct StageBuf {
+    unsigned char* ptr = nullptr;
+    size_t bytes = 0;
+    unsigned long long* offsets = nullptr;
+    cudaEvent_t ready = nullptr;  // the copy into it has finished
+    cudaEvent_t freed = nullptr;  // the last ingest that read it has finished
+  } stage[2];
+  int stageNext = 0;
+  cudaStream_t copyStream = nullptr;
+  struct {
+    bool pending = false;
+    int first = 0, count = 0, kind = 0, buf = 0;
+    size_t total = 0;
+  } staged;
   bool inboxValid = false;
   int inboxKind = 0;
   int inboxFirst = 0, inboxCount = 0;
@@ -888,7 +905,8 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
   }
   LST_CUDA(cudaMalloc(&ev->dv, sizeof(lst::EventView) * n_slots));
   LST_CUDA(cudaMemcpy(ev->dv, ev->hv.data(), sizeof(lst::EventView) * n_slots, cudaMemcpyHostToDevice));
-  LST_CUDA(cudaMalloc(&ev->dOffsets, sizeof(unsigned long long) * n_slots));
+  LST_CUDA(cudaMalloc(&ev->ownOffsets, sizeof(unsigned long long) * n_slots));
+  ev->dOffsets = ev->ownOffsets;
   LST_CUDA(cudaMallocHost(&ev->hCounts, sizeof(lst_counts) * n_slots));
   LST_CUDA(cudaMalloc(&ev->dOutOffsets, sizeof(unsigned long long) * 2 * (n_slots + 1)));
   LST_CUDA(cudaMallocHost(&ev->hOutOffsets, sizeof(unsigned long long) * 2 * (n_slots + 1)));
@@ -908,10 +926,22 @@ void lst_event_destroy(lst_event* ev) {
   cudaStreamSynchronize(ev->stream);
   cudaFree(ev->arena);
   cudaFree(ev->dv);
-  cudaFree(ev->dOffsets);
+  cudaFree(ev->ownOffsets);
   cudaFree(ev->dCounts);
-  if (ev->inbox)
-    cudaFree(ev->inbox);
+  if (ev->ownInbox)
+    cudaFree(ev->ownInbox);
+  for (auto& b : ev->stage) {
+    if (b.ptr)
+      cudaFree(b.ptr);
+    if (b.offsets)
+      cudaFree(b.offsets);
+    if (b.ready)
+      cudaEventDestroy(b.ready);
+    if (b.freed)
+      cudaEventDestroy(b.freed);
+  }
+  if (ev->copyStream)
+    cudaStreamDestroy(ev->copyStream);
   cudaFreeHost(ev->hCounts);
   cudaFree(ev->dOutOffsets);
   cudaFreeHost(ev->hOutOffsets);
@@ -931,7 +961,7 @@ void lst_event_destroy(lst_event* ev) {
 int lst_event_memory(const lst_event* ev, size_t* bytes) {
   if (!ev || !bytes)
     return setError("lst_event_memory: null argument");
-  *bytes = ev->totalBytes + ev->inboxBytes;
+  *bytes = ev->totalBytes + ev->inboxBytes + ev->stage[0].bytes + ev->stage[1].bytes;
   return 0;
 }
 
@@ -1164,17 +1194,19 @@ namespace {
     }
     if (total_bytes > ev->inboxBytes) {
     LST_CUDA(cudaStreamSynchronize(ev->stream));
-    if (ev->inbox)
-      LST_CUDA(cudaFree(ev->inbox));
-    ev->inbox = nullptr;
+    if (ev->ownInbox)
+      LST_CUDA(cudaFree(ev->ownInbox));
+    ev->ownInbox = nullptr;
     ev->inboxBytes = 0;
     size_t want = (total_bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
-    LST_CUDA(cudaMalloc(&ev->inbox, want));
+    LST_CUDA(cudaMalloc(&ev->ownInbox, want));
     ev->inboxBytes = want;
   }
   cudaStream_t s = ev->stream;
-  LST_CUDA(cudaMemcpyAsync(ev->inbox, blobs, total_bytes, cudaMemcpyDefault, s));
-  LST_CUDA(cudaMemcpyAsync(ev->dOffsets + first, blob_offsets, sizeof(uint64_t) * count, cudaMemcpyDefault, s));
+  LST_CUDA(cudaMemcpyAsync(ev->ownInbox, blobs, total_bytes, cudaMemcpyDefault, s));
+  LST_CUDA(cudaMemcpyAsync(ev->ownOffsets + first, blob_offsets, sizeof(uint64_t) * count, cudaMemcpyDefault, s));
+  ev->inbox = ev->ownInbox;
+  ev->dOffsets = ev->ownOffsets;
   ev->inboxValid = true;
   ev->inboxUsed = total_bytes;
   ev->inboxKind = kind;
@@ -1194,6 +1226,78 @@ int lst_batch_upload_seeds(lst_event* ev, int first, int count, const void* blob
   return uploadInbox(ev, first, count, blobs, total_bytes, blob_offsets, 1, "lst_batch_upload_seeds");
 }
 
+int lst_batch_stage(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
+                    const uint64_t* blob_offsets, int seed_layout) {
+  int rc = checkSlots(ev, first, count);
+  if (rc)
+    return rc;
+  if (count == 0)
+    return setError("lst_batch_stage: no slots");
+  if (!blobs || !blob_offsets)
+    return setError("lst_batch_stage: null argument");
+  for (int i = 0; i < count; ++i)
+    if (blob_offsets[i] % 16 != 0 || blob_offsets[i] + 16 > total_bytes)
+      return setError("lst_batch_stage: blob offset misaligned or outside the buffer");
+  if (ev->staged.pending)
+    return setError("lst_batch_stage: a staged batch has not been ingested yet");
+  if (!ev->copyStream)
+    LST_CUDA(cudaStreamCreateWithFlags(&ev->copyStream, cudaStreamNonBlocking));
+  lst_event::StageBuf& b = ev->stage[ev->stageNext];
+  if (!b.ready) {
+    LST_CUDA(cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming));
+    LST_CUDA(cudaEventCreateWithFlags(&b.freed, cudaEventDisableTiming));
+    LST_CUDA(cudaMalloc(&b.offsets, sizeof(unsigned long long) * ev->nSlots));
+  }
+  if (total_bytes > b.bytes) {
+    // the buffer may still be read by an ingest or written by a copy
+    LST_CUDA(cudaStreamSynchronize(ev->stream));
+    LST_CUDA(cudaStreamSynchronize(ev->copyStream));
+    if (b.ptr)
+      LST_CUDA(cudaFree(b.ptr));
+    b.ptr = nullptr;
+    b.bytes = 0;
+    const size_t want = (total_bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
+    LST_CUDA(cudaMalloc(&b.ptr, want));
+    b.bytes = want;
+    LST_CUDA(cudaEventRecord(b.freed, ev->stream));
+  }
+  LST_CUDA(cudaStreamWaitEvent(ev->copyStream, b.freed, 0));
+  LST_CUDA(cudaMemcpyAsync(b.ptr, blobs, total_bytes, cudaMemcpyDefault, ev->copyStream));
+  LST_CUDA(cudaMemcpyAsync(b.offsets + first, blob_offsets, sizeof(uint64_t) * count, cudaMemcpyDefault,
+                           ev->copyStream));
+  LST_CUDA(cudaEventRecord(b.ready, ev->copyStream));
+  ev->staged.pending = true;
+  ev->staged.first = first;
+  ev->staged.count = count;
+  ev->staged.kind = seed_layout ? 1 : 0;
+  ev->staged.buf = ev->stageNext;
+  ev->staged.total = total_bytes;
+  ev->stageNext ^= 1;
+  return 0;
+}
+
+int lst_batch_ingest_staged(lst_event* ev) {
+  if (!ev)
+    return setError("null event set");
+  if (!ev->staged.pending)
+    return setError("lst_batch_ingest_staged: nothing staged");
+  lst_event::StageBuf& b = ev->stage[ev->staged.buf];
+  LST_CUDA(cudaStreamWaitEvent(ev->stream, b.ready, 0));
+  ev->inbox = b.ptr;
+  ev->dOffsets = b.offsets;
+  ev->inboxValid = true;
+  ev->inboxUsed = ev->staged.total;
+  ev->inboxKind = ev->staged.kind;
+  ev->inboxFirst = ev->staged.first;
+  ev->inboxCount = ev->staged.count;
+  ev->staged.pending = false;
+  int rc = ingestInbox(ev, ev->staged.first, ev->staged.count);
+  if (rc)
+    return rc;
+  LST_CUDA(cudaEventRecord(b.freed, ev->stream));
+  return 0;
+}
+
 int lst_batch_ingest(lst_event* ev, int first, int count) {
   int rc = checkSlots(ev, first, count);
   if (rc)
@@ -1202,7 +1306,15 @@ int lst_batch_ingest(lst_event* ev, int first, int count) {
     return setError("lst_batch_ingest: no packed inputs uploaded");
   if (count > 0 && (first < ev->inboxFirst || first + count > ev->inboxFirst + ev->inboxCount))
     return setError("lst_batch_ingest: slots outside the range of the last upload");
-  return count == 0 ? 0 : ingestInbox(ev, first, count);
+  if (count == 0)
+    return 0;
+  rc = ingestInbox(ev, first, count);
+  if (rc)
+    return rc;
+  for (auto& b : ev->stage)  // a staging buffer being re-read must not be refilled before this ingest ends
+    if (b.ptr && ev->inbox == b.ptr)
+      LST_CUDA(cudaEventRecord(b.freed, ev->stream));
+  return 0;
 }
 
 size_t lst_seed_packed_size(uint32_t n_ph2, uint32_t n_seeds, uint32_t n_seed_hits) {

@@ -131,6 +131,8 @@ EXPORTS = (
     "lst_es_geometry_hash",
     "lst_autotune",
     "lst_autotune_load",
+    "lst_batch_stage",
+    "lst_batch_ingest_staged",
 )
 
 
@@ -326,6 +328,8 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_es_geometry_hash.restype = ctypes.c_uint64
         lib.lst_autotune.argtypes = [vp, i32, i32, ctypes.c_char_p]
         lib.lst_autotune_load.argtypes = [vp, i32, ctypes.c_char_p]
+        lib.lst_batch_stage.argtypes = [vp, i32, i32, vp, sz, vp, i32]
+        lib.lst_batch_ingest_staged.argtypes = [vp]
         _lib = lib
         return lib
 
@@ -600,6 +604,16 @@ class EventSet:
 
     def autotune_load(self, count: int, cache_path: str) -> bool:
         return bool(_check(library().lst_autotune_load(self._h, count, cache_path.encode()), "lst_autotune_load"))
+
+    def stage(self, first: int, blobs: np.ndarray, offsets: np.ndarray, seed_layout: bool = False):
+        """lst_batch_stage: start copying packed events (pinned buffer) on the copy stream."""
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        self._staged_offsets = offsets  # the offsets are read when the call returns; keep them alive anyway
+        _check(library().lst_batch_stage(self._h, first, offsets.size, blobs.ctypes.data, blobs.nbytes,
+                                         offsets.ctypes.data, int(bool(seed_layout))), "lst_batch_stage")
+
+    def ingest_staged(self):
+        _check(library().lst_batch_ingest_staged(self._h), "lst_batch_ingest_staged")
 
     def ingest(self, first: int, count: int):
         _check(library().lst_batch_ingest(self._h, first, count), "lst_batch_ingest")
