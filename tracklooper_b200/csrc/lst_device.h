@@ -65,7 +65,8 @@ namespace lst {
     unsigned int pixQueueBack;    // pixel candidates queued from the back (endcap tracklet algorithm)
     unsigned int t5QueueBack;     // quintuplet candidates queued from the back (modules not all barrel)
     unsigned int pixQueue2Count;  // pixel candidates passing the first pixel tracklet as well
-    unsigned int pad[2];
+    unsigned int t5SortCount;     // quintuplets binned by eta for the cross-module cleaning
+    unsigned int pad[1];
   };
 
   // All device pointers of one event.
@@ -126,6 +127,9 @@ namespace lst {
     float* hitShiftXa;          // per hit moved by the strip shift: its moved point and z
     float* hitShiftYa;
     float* hitShiftZn;
+    unsigned int* t5Order;      // quintuplets sorted by eta bin (their index)
+    uint16_t* t5OrderPos;       //   and their module's position in the eligible-module list
+    unsigned int* t5BinStart;   // start of each eta bin in t5Order (bins + 2 entries)
     unsigned int* candQueue;    // candidates passing a pre-selection (T5, then pT5 / pT3), any order
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
     unsigned int* plsOrder;     // pLS indices sorted by eta bin

@@ -525,6 +525,8 @@ namespace {
         const dim3 eligGrid(ceilDiv(std::max<size_t>(nE, 1) * 32, 256), count);
         LST_LAUNCH(lst::kCrossCleanPT3, dim3(blocksFor(lst::kMaxPixelTriplets, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kAddPT3TC, one, 1024, d, v);
+        LST_LAUNCH(lst::kT5Bin, one, 1024, d, v);
+        LST_LAUNCH(lst::kT5DedupBinned, dim3(blocksFor(4096, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kT5DedupBeforeTC, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kMergeT5Flag, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kCrossCleanT5, eligGrid, 256, d, v);
@@ -650,6 +652,8 @@ namespace {
         {"kCrossCleanPT3", (const void*)lst::kCrossCleanPT3},
         {"kAddPT3TC", (const void*)lst::kAddPT3TC},
         {"kT5DedupBeforeTC", (const void*)lst::kT5DedupBeforeTC},
+        {"kT5Bin", (const void*)lst::kT5Bin},
+        {"kT5DedupBinned", (const void*)lst::kT5DedupBinned},
         {"kMergeT5Flag", (const void*)lst::kMergeT5Flag},
         {"kCrossCleanT5", (const void*)lst::kCrossCleanT5},
         {"kT5TCCount", (const void*)lst::kT5TCCount},

@@ -249,6 +249,9 @@
   X(pixPassV, float, 8 * lst::kPixPassCap)            \
   X(candQueue, unsigned int, lst::kCandQueueCap)        \
   X(hitMiniSlope, float, H)                           \
+  X(t5Order, unsigned int, lst::kT5SortCap)           \
+  X(t5OrderPos, uint16_t, lst::kT5SortCap)            \
+  X(t5BinStart, unsigned int, lst::kPLSBins + 2)      \
   X(hitShiftXa, float, H)                             \
   X(hitShiftYa, float, H)                             \
   X(hitShiftZn, float, H)                             \

@@ -780,6 +780,7 @@ namespace lst {
   // candidates than the flag buffer holds take the walk instead.
   constexpr unsigned int kT5CandCap = 1u << 21;  // candidates per event
   constexpr unsigned int kCandQueueCap = 1u << 18;  // pre-selected candidates per event (T5, pT5, pT3)
+  constexpr unsigned int kT5SortCap = 1u << 15;     // quintuplets per event sorted by eta for the TC cleaning
   constexpr unsigned int kT5PassCap = 1u << 16;  // passing candidates per event whose values are kept
   constexpr unsigned int kT5DnnCap = 1u << 14;   // candidates per event classified in kT5Dnn
 
@@ -2378,8 +2379,121 @@ namespace lst {
 
   // Cross-module T5 duplicate removal before TC building
   // (SDL/Kernels.h:251-323); one warp per eligible module, marks t5Flag.
+  // Cross-module T5 cleaning (SDL/Kernels.h:251-323).  The reference visits
+  // the ordered pairs (ix in module A, jx in module B) with A's position in
+  // the eligible-module list not after B's and ix != jx; a pair whose
+  // |deta| > 0.1 is skipped at the first test, and marks are only ever set.  kT5Bin counting-sorts the event's
+  // quintuplets into the pLS-cleaning eta bins (one block per event), and
+  // kT5DedupBinned gives each quintuplet a thread that visits the same ordered
+  // pairs among the bins within reach (and the non-finite bin, which meets
+  // every quintuplet, as does a quintuplet of non-finite eta).  Events with
+  // more quintuplets than kT5SortCap keep the module-pair walk.
+  __global__ void __launch_bounds__(1024) kT5Bin(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sCount[kPLSBins + 1];
+    const EventView& ev = evs[blockIdx.y];
+    const int nE = *ev.rg.nEligibleT5Modules;
+    const Quintuplets& q = ev.t5;
+    for (int b = threadIdx.x; b <= kPLSBins; b += blockDim.x)
+      sCount[b] = 0;
+    __syncthreads();
+    unsigned int mine = 0;
+    for (int e = threadIdx.x; e < nE; e += blockDim.x) {
+      const uint16_t lm = ev.rg.indicesOfEligibleT5Modules[e];
+      const unsigned int n = q.nQuintuplets[lm], base = ev.rg.quintupletModuleIndices[lm];
+      for (unsigned int j = 0; j < n; ++j)
+        atomicAdd(&sCount[plsEtaBin(q.eta[base + j])], 1u);
+      mine += n;
+    }
+    unsigned int total;
+    blockExclusiveScan(mine, total);
+    const unsigned int c = threadIdx.x <= kPLSBins ? sCount[threadIdx.x] : 0u;
+    unsigned int tot;
+    const unsigned int ex = blockExclusiveScan(c, tot);
+    if (threadIdx.x <= kPLSBins) {
+      sCount[threadIdx.x] = ex;
+      ev.t5BinStart[threadIdx.x] = ex;
+    }
+    if (threadIdx.x == 0) {
+      ev.t5BinStart[kPLSBins + 1] = tot;
+      ev.sc->t5SortCount = total;
+    }
+    __syncthreads();
+    if (total > kT5SortCap)
+      return;
+    for (int e = threadIdx.x; e < nE; e += blockDim.x) {
+      const uint16_t lm = ev.rg.indicesOfEligibleT5Modules[e];
+      const unsigned int n = q.nQuintuplets[lm], base = ev.rg.quintupletModuleIndices[lm];
+      for (unsigned int j = 0; j < n; ++j) {
+        const unsigned int pos = atomicAdd(&sCount[plsEtaBin(q.eta[base + j])], 1u);
+        ev.t5Order[pos] = base + j;
+        ev.t5OrderPos[pos] = static_cast<uint16_t>(e);
+      }
+    }
+  }
+
+  // The reference's test of one ordered pair (ix, jx), marking the loser.
+  LST_DEV void t5CrossPair(const EventView& ev, unsigned int ix, unsigned int jx, float eta1, float phi1,
+                           float score1) {
+    const Quintuplets& q = ev.t5;
+    if (q.partOfPT5[jx] || (q.isDup[jx] & 1))
+      return;
+    float eta2 = q.eta[jx], phi2 = q.phi[jx], score2 = q.score_rphisum[jx];
+    float dEta = fabs_(eta1 - eta2);
+    float dPhi = wrapDPhi(phi1, phi2);
+    if (dEta > 0.1f)
+      return;
+    if (fabs_(dPhi) > 0.1f)
+      return;
+    float dR2 = dEta * dEta + dPhi * dPhi;
+    int nMatched = sharedHitsT5(q, ix, jx);
+    if (dR2 < 0.001f || nMatched >= 5) {
+      if (score1 > score2)
+        ev.t5Flag[ix] = 1;
+      else if (score1 < score2)
+        ev.t5Flag[jx] = 1;
+      else
+        ev.t5Flag[ix < jx ? ix : jx] = 1;
+    }
+  }
+
+  __global__ void kT5DedupBinned(DeviceES es, const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = ev.sc->t5SortCount;
+    if (n > kT5SortCap || ev.forceWalk)
+      return;
+    const Quintuplets& q = ev.t5;
+    const unsigned int* binStart = ev.t5BinStart;
+    const unsigned int nFinite = binStart[kPLSBins];
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+      const unsigned int ix = ev.t5Order[k];
+      if (q.partOfPT5[ix] || (q.isDup[ix] & 1))
+        continue;
+      const unsigned int posI = ev.t5OrderPos[k];
+      const float eta1 = q.eta[ix], phi1 = q.phi[ix], score1 = q.score_rphisum[ix];
+      const int b = plsEtaBin(eta1);
+      unsigned int lo = 0, hi = n, lo2 = n;  // positions [lo, hi) then [lo2, n)
+      if (b < kPLSBins) {
+        lo = binStart[b >= kPLSBinReach ? b - kPLSBinReach : 0];
+        hi = binStart[(b + kPLSBinReach < kPLSBins ? b + kPLSBinReach : kPLSBins - 1) + 1];
+        lo2 = nFinite;
+      }
+      for (int part = 0; part < 2; ++part) {
+        const unsigned int p0 = part == 0 ? lo : lo2, p1 = part == 0 ? hi : n;
+        for (unsigned int p = p0; p < p1; ++p) {
+          const unsigned int jx = ev.t5Order[p];
+          const unsigned int posJ = ev.t5OrderPos[p];
+          if (jx == ix || posJ < posI)
+            continue;
+          t5CrossPair(ev, ix, jx, eta1, phi1, score1);
+        }
+      }
+    }
+  }
+
   __global__ void kT5DedupBeforeTC(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
+    if (ev.sc->t5SortCount <= kT5SortCap && !ev.forceWalk)
+      return;  // kT5DedupBinned has done this event
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nE = *ev.rg.nEligibleT5Modules;
     if (warp >= nE)
