@@ -112,6 +112,7 @@ namespace lst {
     unsigned int* t5ModOff;     // per eligible module: first candidate of the event
     unsigned int* t5CandFlag;   // per candidate: 0 = fails, else 1 + slot of its values in t5PassValues
     T5Values* t5PassValues;     // selection values of passing candidates
+    unsigned int* t5PassC;      //   and their candidate index
     float* t5DnnFeat;           // candidates at the classifier: features (38 each)
     unsigned int* t5DnnCand;    //   candidate index
     T5Values* t5DnnVals;        //   selection values so far

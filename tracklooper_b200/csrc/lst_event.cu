@@ -479,6 +479,7 @@ namespace {
           LST_LAUNCH(lst::kT5Dnn, dim3(blocksFor(lst::kT5DnnCap, count, 128), count), 128, d, v);
         LST_LAUNCH(lst::kT5Walk, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v,
                    useDnn);
+        LST_LAUNCH_SMEM(lst::kT5RankEmit, dim3(1, count), 1024, lst::kT5RankSmem, d, v);
         LST_LAUNCH(lst::kT5Emit, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v, useDnn);
         LST_LAUNCH(lst::kT5DedupAfterBuild,
                    dim3(blocksFor(ev->es->nEligibleMax, count, lst::kT5DedupThreads), count), lst::kT5DedupThreads,
@@ -619,6 +620,7 @@ namespace {
         {"kT5ModScan", (const void*)lst::kT5ModScan},
         {"kT5Eval", (const void*)lst::kT5Eval},
         {"kT5Emit", (const void*)lst::kT5Emit},
+        {"kT5RankEmit", (const void*)lst::kT5RankEmit},
         {"kT5Walk", (const void*)lst::kT5Walk},
         {"kT5Dnn", (const void*)lst::kT5Dnn},
         {"kT5Probe", (const void*)lst::kT5Probe},
@@ -881,6 +883,8 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
                                 static_cast<int>(lst::kXCleanSmem)));
   LST_CUDA(cudaFuncSetAttribute(lst::kPT5DedupSorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(lst::kPT5DedupSmem)));
+  LST_CUDA(cudaFuncSetAttribute(lst::kT5RankEmit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(lst::kT5RankSmem)));
   Carver measure;
   lst::EventView tmp{};
   carveEvent(measure, tmp, ev->sizes);

@@ -236,6 +236,7 @@
   X(t5ModOff, unsigned int, L + 1)                    \
   X(t5CandFlag, unsigned int, lst::kT5CandCap)        \
   X(t5PassValues, lst::T5Values, lst::kT5PassCap)     \
+  X(t5PassC, unsigned int, lst::kT5PassCap)           \
   X(t5DnnFeat, float, 38 * lst::kT5DnnCap)            \
   X(t5DnnCand, unsigned int, lst::kT5DnnCap)          \
   X(t5DnnVals, lst::T5Values, lst::kT5DnnCap)         \

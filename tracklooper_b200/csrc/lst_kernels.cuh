@@ -981,6 +981,7 @@ namespace lst {
         const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
         if (slot < kT5PassCap) {
           ev.t5PassValues[slot] = v;
+          ev.t5PassC[slot] = c;
           flag = slot + 1;
         } else {
           flag = kT5PassCap + 1;
@@ -1041,6 +1042,7 @@ namespace lst {
       const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
       if (slot < kT5PassCap) {
         ev.t5PassValues[slot] = v;
+        ev.t5PassC[slot] = c;
         ev.t5CandFlag[c] = slot + 1;
       } else {
         ev.t5CandFlag[c] = kT5PassCap + 1;
@@ -1063,9 +1065,100 @@ namespace lst {
     }
   }
 
+  // The passing quintuplet candidates stored in candidate order, one block per
+  // event: their (candidate index, value slot) keys are bitonic-sorted in
+  // shared memory, so that a candidate's position among the passing ones of
+  // its module -- the reference's occupancy rank -- comes from two binary
+  // searches.  Events with more passing candidates than kT5RankCap leave the
+  // storing to kT5Emit's per-module walk.
+  constexpr unsigned int kT5RankCap = 8192;
+  constexpr size_t kT5RankSmem = kT5RankCap * sizeof(unsigned long long);
+  __global__ void __launch_bounds__(1024) kT5RankEmit(DeviceES es, const EventView* evs) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    unsigned long long* sKey = reinterpret_cast<unsigned long long*>(rsm);
+    const EventView& ev = evs[blockIdx.y];
+    const unsigned int n = ev.sc->t5PassCount;
+    if (ev.sc->t5CandOverflow || n > kT5RankCap || ev.forceWalk)
+      return;
+    unsigned int N = 1;
+    while (N < n)
+      N <<= 1;
+    for (unsigned int t = threadIdx.x; t < N; t += blockDim.x)
+      sKey[t] = t < n ? (static_cast<unsigned long long>(ev.t5PassC[t]) << 32) | t : ~0ull;
+    __syncthreads();
+    for (unsigned int k = 2; k <= N; k <<= 1) {
+      for (unsigned int j = k >> 1; j > 0; j >>= 1) {
+        for (unsigned int i = threadIdx.x; i < N; i += blockDim.x) {
+          const unsigned int l = i ^ j;
+          if (l > i) {
+            const unsigned long long a = sKey[i], b = sKey[l];
+            if (((i & k) == 0) == (a > b)) {
+              sKey[i] = b;
+              sKey[l] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    const int nE = *ev.rg.nEligibleT5Modules;
+    const unsigned int* off = ev.t5ModOff;
+    // first sorted position whose candidate index is at least c
+    auto lowerBound = [&](unsigned int c) {
+      unsigned int lo = 0, hi = n;
+      while (lo < hi) {
+        const unsigned int mid = (lo + hi) >> 1;
+        if (static_cast<unsigned int>(sKey[mid] >> 32) < c)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      return lo;
+    };
+    Triplets t3 = ev.t3;
+    Quintuplets t5 = ev.t5;
+    for (unsigned int p = threadIdx.x; p < n; p += blockDim.x) {
+      const unsigned int c = static_cast<unsigned int>(sKey[p] >> 32);
+      const unsigned int slot = static_cast<unsigned int>(sKey[p] & 0xffffffffu);
+      int lo = 0, hi = nE;  // module position w: largest with off[w] <= c
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= c)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
+      const int layer = es.m.layers[lm1];
+      if (layer != 1 && layer != 2)
+        continue;
+      const unsigned int r = p - lowerBound(off[lo]);
+      if (int(r) >= ev.rg.quintupletModuleOccupancy[lm1])
+        continue;
+      unsigned int innerT3, outerT3;
+      t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
+      uint16_t lm[5] = {lm1, t3.lowerModuleIndices[3 * innerT3 + 1], t3.lowerModuleIndices[3 * innerT3 + 2],
+                        t3.lowerModuleIndices[3 * outerT3 + 1], t3.lowerModuleIndices[3 * outerT3 + 2]};
+      storeT5(ev.md, ev.ls, t3, t5, innerT3, outerT3, lm, layer, ev.t5PassValues[slot],
+              ev.rg.quintupletModuleIndices[lm1] + r);
+    }
+    for (int w = threadIdx.x; w < nE; w += blockDim.x) {
+      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[w];
+      const int layer = es.m.layers[lm1];
+      if (layer != 1 && layer != 2)
+        continue;
+      const unsigned int count = lowerBound(off[w] + ev.t5ModCand[w]) - lowerBound(off[w]);
+      const int cap = ev.rg.quintupletModuleOccupancy[lm1];
+      t5.nQuintuplets[lm1] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
+      t5.totOccupancyQuintuplets[lm1] = count;
+      if (int(count) > cap)
+        atomicOr(&ev.sc->status, kStatusCapOverflow);
+    }
+  }
+
   __global__ void kT5Emit(DeviceES es, const EventView* evs, bool useDnn) {
     const EventView& ev = evs[blockIdx.y];
-    if (ev.sc->t5CandOverflow)
+    if (ev.sc->t5CandOverflow || (ev.sc->t5PassCount <= kT5RankCap && !ev.forceWalk))
       return;
     const int wpb = blockDim.x >> 5;
     const int nE = *ev.rg.nEligibleT5Modules;
