@@ -94,6 +94,25 @@ namespace lst {
 
   }  // namespace
 
+  // detId -> module index hash of EsHost::detHashKey / detHashVal.
+  void buildDetHash(EsHost& es) {
+    unsigned int bits = 4;
+    while ((1u << bits) < 2u * es.mapdetId.size())
+      ++bits;
+    es.detHashBits = bits;
+    const unsigned int size = 1u << bits, mask = size - 1;
+    es.detHashKey.assign(size, 0u);
+    es.detHashVal.assign(size, uint16_t(0xffff));
+    for (size_t i = 0; i < es.mapdetId.size(); ++i) {
+      const unsigned int key = es.mapdetId[i];
+      unsigned int slot = (key * 2654435761u) >> (32 - bits);
+      while (es.detHashVal[slot] != 0xffff && es.detHashKey[slot] != key)
+        slot = (slot + 1) & mask;
+      es.detHashKey[slot] = key;
+      es.detHashVal[slot] = es.mapIdx[i];
+    }
+  }
+
   std::string loadEsHost(const std::string& dir, EsHost& es) {
     std::vector<CentroidRec> cents;
     if (!readRecords(dir + "/sensor_centroids.bin", cents) || cents.empty())
@@ -367,6 +386,7 @@ namespace lst {
     es.nTotalSegments = static_cast<unsigned int>(lsTotal) + kMaxPixelSegments;
     es.maxTriplets = t3Total;
     es.maxQuintuplets = t5Total;
+    buildDetHash(es);
     return std::string();
   }
 

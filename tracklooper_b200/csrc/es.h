@@ -42,6 +42,13 @@ namespace lst {
     std::vector<int> lsOffset, lsCap;    // nLowerModules + 1
     std::vector<int> t3CapIfUsed;        // nLowerModules: cap when the module has segments
     std::vector<int> t5CapIfEligible;    // nLowerModules: cap when eligible (-1: never eligible)
+    // detId -> module index as an open-addressing hash table (linear probing,
+    // slot = detId * 2654435761 >> (32 - bits)); value 0xffff marks an empty
+    // slot.  Same answers as a binary search of mapdetId, in one or two probes.
+    std::vector<unsigned int> detHashKey;
+    std::vector<uint16_t> detHashVal;
+    unsigned int detHashBits = 0;
+
     unsigned int nTotalMDs = 0;          // arena size incl. pixel MDs
     unsigned int nTotalSegments = 0;     // arena size incl. pixel segments
     unsigned int maxTriplets = 0;        // upper bound of the triplet arena

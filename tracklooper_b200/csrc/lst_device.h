@@ -29,6 +29,9 @@ namespace lst {
     unsigned int nTotalSegments;
     unsigned int maxTriplets;
     unsigned int maxQuintuplets;
+    const unsigned int* detHashKey;
+    const uint16_t* detHashVal;
+    unsigned int detHashBits;
     uint16_t nModules;
     uint16_t nLowerModules;
     uint16_t pixelModule;

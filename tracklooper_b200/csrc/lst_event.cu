@@ -220,6 +220,9 @@ namespace {
     d.lsCap = upload(c, h.lsCap, copies, sizes);
     d.t3CapIfUsed = upload(c, h.t3CapIfUsed, copies, sizes);
     d.t5CapIfEligible = upload(c, h.t5CapIfEligible, copies, sizes);
+    d.detHashKey = upload(c, h.detHashKey, copies, sizes);
+    d.detHashVal = upload(c, h.detHashVal, copies, sizes);
+    d.detHashBits = h.detHashBits;
     // The positive- and negative-z pixel maps follow the inclusive one in
     // connectedPixels (SDL/Event.cc:1049-1052).
     const size_t last = lst::kSizeSuperbins - 1;

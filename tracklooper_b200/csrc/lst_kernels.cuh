@@ -184,8 +184,22 @@ namespace lst {
       h.phis[ihit] = phiOf(x, y);
       h.etas[ihit] = ((z > 0) - (z < 0)) * facosh(fsqrt(x * x + y * y + z * z) / rt);
       float hex = 0.f, hey = 0.f, lex = 0.f, ley = 0.f;
-      int found = sortedFind(m.mapdetId, detId, es.nModules);
-      if (found < 0) {
+      int mIdx = -1;  // module of detId: the ES hash (linear probing)
+      {
+        const unsigned int mask = (1u << es.detHashBits) - 1;
+        unsigned int slot = (detId * 2654435761u) >> (32 - es.detHashBits);
+        for (unsigned int probe = 0; probe <= mask; ++probe) {
+          const uint16_t val = es.detHashVal[slot];
+          if (val == 0xffff)
+            break;
+          if (es.detHashKey[slot] == detId) {
+            mIdx = val;
+            break;
+          }
+          slot = (slot + 1) & mask;
+        }
+      }
+      if (mIdx < 0) {
         atomicOr(&ev.sc->status, kStatusUnknownDetId);
         h.moduleIndices[ihit] = 0xffff;
         h.highEdgeXs[ihit] = hex;
@@ -194,7 +208,7 @@ namespace lst {
         h.lowEdgeYs[ihit] = ley;
         continue;
       }
-      uint16_t mi = m.mapIdx[found];
+      uint16_t mi = static_cast<uint16_t>(mIdx);
       h.moduleIndices[ihit] = mi;
       // Per-hit parts of the mini-doublet cuts of the module pair this hit
       // belongs to (lower module lm): the dphi-threshold slope, and the strip
