@@ -485,7 +485,9 @@ namespace {
         LST_LAUNCH_SMEM(lst::kT5RankEmit, dim3(1, count), 1024, lst::kT5RankSmem, d, v);
         LST_LAUNCH(lst::kT5Emit, warpGrid(ev->es->nEligibleMax, 8, count), 256, d, v, useDnn);
         LST_LAUNCH(lst::kT5DedupAfterBuild,
-                   dim3(blocksFor(ev->es->nEligibleMax, count, lst::kT5DedupThreads), count), lst::kT5DedupThreads,
+                   dim3(blocksFor(size_t(ev->es->nEligibleMax) * lst::kT5DedupThreads / 32, count, lst::kT5DedupThreads),
+                        count),
+                   lst::kT5DedupThreads,
                    d, v);
         LST_LAUNCH(lst::kT5Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         break;

@@ -386,16 +386,22 @@ namespace lst {
 
   // Derived per-MD values for every stored MD (lower modules and the pixel
   // module); one warp per module.
+  // The pixel module's mini-doublets (two per pLS, thousands per event) are
+  // shared out over all of the event's threads rather than one warp.
   __global__ void kMDDerived(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const int wpb = blockDim.x >> 5;
     MiniDoublets md = ev.md;
-    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w <= es.nLowerModules; w += gridDim.x * wpb) {
+    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < es.nLowerModules; w += gridDim.x * wpb) {
       const unsigned int n = md.nMDs[w];
       const unsigned int base = es.mdOffset[w];
       for (unsigned int k = laneId(); k < n; k += 32)
         storeMDDerived(md, base + k);
     }
+    const unsigned int nPix = md.nMDs[es.nLowerModules];
+    const unsigned int pixBase = es.mdOffset[es.nLowerModules];
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < nPix; k += gridDim.x * blockDim.x)
+      storeMDDerived(md, pixBase + k);
   }
 
   // SDL/MiniDoublet.h:1084-1104
@@ -1296,8 +1302,8 @@ namespace lst {
 
   // Duplicate removal among the T5s of one module (SDL/Kernels.h:202-249).
   // Every pair (i < j) of a module is independent and only ever sets isDup
-  // bit 1, so the pairs are spread over a block: a chunk of the eligible-module
-  // list is scanned for modules holding two or more T5s, and each such module's
+  // bit 1, so the pairs are spread over a block: a chunk of 32 entries of the
+  // eligible-module list is scanned for modules holding two or more T5s, and each such module's
   // T5s are staged in shared memory (eta, phi, score, hits) and its n x n pair
   // square is shared out among the block's threads.  The largest modules hold
   // a few hundred T5s, whose pairs would otherwise run on one warp.
@@ -1306,23 +1312,30 @@ namespace lst {
   __global__ void __launch_bounds__(kT5DedupThreads) kT5DedupAfterBuild(DeviceES es, const EventView* evs) {
     __shared__ float sEta[kT5DedupStage], sPhi[kT5DedupStage], sScore[kT5DedupStage];
     __shared__ unsigned int sHits[kT5DedupStage * 10];
-    __shared__ uint16_t sMods[kT5DedupThreads];
+    __shared__ uint16_t sMods[32];
+    __shared__ unsigned int sNMods;
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nElig = *ev.rg.nEligibleT5Modules;
     Quintuplets q = ev.t5;
-    for (unsigned int c0 = blockIdx.x * blockDim.x; c0 < nElig; c0 += gridDim.x * blockDim.x) {
-      const unsigned int e = c0 + threadIdx.x;
-      uint16_t lmLoad = 0;
-      unsigned int nLoad = 0;
-      if (e < nElig) {
-        lmLoad = ev.rg.indicesOfEligibleT5Modules[e];
-        nLoad = q.nQuintuplets[lmLoad];
+    // chunks of 32 eligible modules: the first warp picks those with two or more T5s
+    for (unsigned int c0 = blockIdx.x * 32; c0 < nElig; c0 += gridDim.x * 32) {
+      if (threadIdx.x < 32) {
+        const unsigned int e = c0 + threadIdx.x;
+        uint16_t lmLoad = 0;
+        unsigned int nLoad = 0;
+        if (e < nElig) {
+          lmLoad = ev.rg.indicesOfEligibleT5Modules[e];
+          nLoad = q.nQuintuplets[lmLoad];
+        }
+        unsigned int tot;
+        const unsigned int slot = warpRank(nLoad >= 2, tot);
+        if (nLoad >= 2)
+          sMods[slot] = lmLoad;
+        if (threadIdx.x == 0)
+          sNMods = tot;
       }
-      unsigned int nMods;
-      const unsigned int slot = blockExclusiveScan(nLoad >= 2 ? 1u : 0u, nMods);
-      if (nLoad >= 2)
-        sMods[slot] = lmLoad;
       __syncthreads();
+      const unsigned int nMods = sNMods;
       for (unsigned int k = 0; k < nMods; ++k) {
         const uint16_t lm = sMods[k];
         const unsigned int n = q.nQuintuplets[lm];
@@ -1374,6 +1387,7 @@ namespace lst {
         }
         __syncthreads();
       }
+      __syncthreads();  // sMods / sNMods are rewritten for the next chunk
     }
   }
 
