@@ -7,6 +7,7 @@
 namespace lst {
 
   struct TCCleanInfo;
+  struct PLSRec;
 
   // Event setup resident on the device (read-only during an event).
   struct DeviceES {
@@ -136,8 +137,8 @@ namespace lst {
     unsigned int* t5BinStart;   // start of each eta bin in t5Order (bins + 2 entries)
     unsigned int* candQueue;    // candidates passing a pre-selection (T5, then pT5 / pT3), any order
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
-    unsigned int* plsOrder;     // pLS indices sorted by eta bin
-    unsigned int* plsBinStart;  // start of each eta bin in plsOrder (bins + 2 entries)
+    struct PLSRec* plsRec;      // pLS records sorted by eta bin
+    unsigned int* plsBinStart;  // start of each eta bin in plsRec (bins + 2 entries)
     unsigned int maxHits;
     unsigned int forceWalk;  // take the fallback paths (walks, pair-by-pair tests) for testing them
   };

@@ -257,5 +257,5 @@
   X(hitShiftYa, float, H)                             \
   X(hitShiftZn, float, H)                             \
   X(tcCleanInfo, lst::TCCleanInfo, TC)                \
-  X(plsOrder, unsigned int, P)                        \
+  X(plsRec, lst::PLSRec, P)                           \
   X(plsBinStart, unsigned int, lst::kPLSBins + 2)

@@ -1427,19 +1427,36 @@ namespace lst {
     return static_cast<int>(t);
   }
 
-  // Counting sort of the pLS by eta bin; one block per event.
+  // One pLS as the cleaning passes read it, stored in eta-bin order so that a
+  // tile of candidates is one coalesced read: eta, phi, score, the pLS index
+  // with its isQuad byte and bit 0 of its isDup packed above it, and its four
+  // pixel hits.
+  struct __align__(16) PLSRec {
+    float eta, phi, score;
+    unsigned int key;  // index | uint8(isQuad) << 16 | (isDup & 1) << 24
+    uint4 hits;
+  };
+  static_assert(kMaxPixelSegments <= 0xffff, "pLS index must fit the record key's low 16 bits");
+  LST_DEV unsigned int plsRecIndex(unsigned int key) { return key & 0xffffu; }
+  LST_DEV int8_t plsRecQuad(unsigned int key) { return static_cast<int8_t>((key >> 16) & 0xffu); }
+  LST_DEV bool plsRecDup(unsigned int key) { return (key >> 24) & 1u; }
+
+  // Counting sort of the pLS by eta bin, one block per event; writes the
+  // bin starts and the sorted records.  isDup is sampled here, so the second
+  // pass (which reads the marks of the first) bins after the first pass ends.
   __global__ void __launch_bounds__(1024) kPLSBin(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sCount[kPLSBins + 1];
     __shared__ unsigned int sCursor[kPLSBins + 1];
     const EventView& ev = evs[blockIdx.y];
-    unsigned int nPix = ev.ls.nSegments[es.pixelModule];
+    const Segments& s = ev.ls;
+    unsigned int nPix = s.nSegments[es.pixelModule];
     if (nPix > kMaxPixelSegments)
       nPix = kMaxPixelSegments;
     for (int b = threadIdx.x; b <= kPLSBins; b += blockDim.x)
       sCount[b] = 0;
     __syncthreads();
     for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
-      atomicAdd(&sCount[plsEtaBin(ev.ls.eta[i])], 1u);
+      atomicAdd(&sCount[plsEtaBin(s.eta[i])], 1u);
     __syncthreads();
     unsigned int c = threadIdx.x <= kPLSBins ? sCount[threadIdx.x] : 0u;
     unsigned int tot;
@@ -1451,8 +1468,77 @@ namespace lst {
     if (threadIdx.x == 0)
       ev.plsBinStart[kPLSBins + 1] = tot;
     __syncthreads();
-    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
-      ev.plsOrder[atomicAdd(&sCursor[plsEtaBin(ev.ls.eta[i])], 1u)] = i;
+    const uint4* hits = reinterpret_cast<const uint4*>(s.pLSHitsIdxs);
+    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x) {
+      PLSRec r;
+      r.eta = s.eta[i];
+      r.phi = s.phi[i];
+      r.score = s.score[i];
+      r.key = i | (static_cast<unsigned int>(static_cast<uint8_t>(s.isQuad[i])) << 16) |
+              (static_cast<unsigned int>(s.isDup[i] & 1) << 24);
+      r.hits = hits[i];
+      ev.plsRec[atomicAdd(&sCursor[plsEtaBin(r.eta)], 1u)] = r;
+    }
+  }
+
+  // One candidate o (a sorted position after this thread's pLS me): the
+  // reference's test of the pair (SDL/Kernels.h:384-473) with the lower index
+  // in its outer role (ix, "1") and the higher in the inner (jx, "2").  The
+  // roles are picked by selects, not by a branch, because which of the two is
+  // lower differs from lane to lane.
+  LST_DEV void plsCleanPair(const EventView& ev, const PLSRec& me, const PLSRec& o, bool secondpass) {
+    const float etaO = o.eta;
+    if (fabs_(etaO - me.eta) > 0.1f)
+      return;
+    const unsigned int keyO = o.key;
+    if (secondpass && (!plsRecQuad(keyO) || plsRecDup(keyO)))
+      return;
+    const float phiO = o.phi, scoreO = o.score;
+    const uint4 hitsO = o.hits;
+    const bool meLow = plsRecIndex(me.key) < plsRecIndex(keyO);
+    const unsigned int key1 = meLow ? me.key : keyO, key2 = meLow ? keyO : me.key;
+    const float score1 = meLow ? me.score : scoreO, score2 = meLow ? scoreO : me.score;
+    const uint4 h1 = meLow ? me.hits : hitsO, h2 = meLow ? hitsO : me.hits;
+    const unsigned int ix = plsRecIndex(key1), jx = plsRecIndex(key2);
+    const int8_t quad_diff = plsRecQuad(key1) - plsRecQuad(key2);
+    const float score_diff = score1 - score2;
+    unsigned int idxToRemove;
+    if (quad_diff > 0)
+      idxToRemove = jx;
+    else if (quad_diff < 0)
+      idxToRemove = ix;
+    else if (score_diff < 0)
+      idxToRemove = jx;
+    else if (score_diff > 0)
+      idxToRemove = ix;
+    else
+      idxToRemove = ix;
+    const unsigned int h1a[4] = {h1.x, h1.y, h1.z, h1.w};
+    int npMatched = 0;
+    for (int k = 0; k < 4; k++) {
+      const bool pmatched = h1a[k] == h2.x || h1a[k] == h2.y || h1a[k] == h2.z || h1a[k] == h2.w;
+      if (pmatched) {
+        npMatched++;
+        if (secondpass)
+          break;
+      }
+    }
+    bool remove = npMatched >= 3;
+    if (secondpass) {
+      const float eta1 = meLow ? me.eta : etaO, eta2 = meLow ? etaO : me.eta;
+      const float phi1 = meLow ? me.phi : phiO, phi2 = meLow ? phiO : me.phi;
+      const float dEta = fabs_(eta1 - eta2);
+      const float dPhi = wrapDPhi(phi1, phi2);
+      const float dR2 = dEta * dEta + dPhi * dPhi;
+      if ((npMatched >= 1) || (dR2 < 1e-5f))
+        remove = true;
+    }
+    if (remove) {
+      if (secondpass)
+        ev.plsFlag[idxToRemove] = 1;
+      else
+        ev.ls.isDup[idxToRemove] = 1;
+    }
   }
 
   // pLS duplicate removal (SDL/Kernels.h:384-473).  Pass 1 sets bit 1 of
@@ -1463,125 +1549,72 @@ namespace lst {
   // the reference's result; pairs more than 0.1 apart in eta return at the
   // reference's first test.
   //
-  // Each block takes kPLSCleanTile consecutive pLS of the eta-sorted order (one
-  // per thread) and streams, through shared memory, the sorted positions that
-  // can lie within 0.1 in eta of any of them: the bins from kPLSBinReach below
-  // its first pLS's bin to kPLSBinReach above its last one, plus the
-  // non-finite bin, which meets every pLS (a NaN never satisfies the
-  // reference's skip).  A block holding a non-finite pLS streams all of them.
+  // Each pair is tested once, by the pLS that comes first in the eta-sorted
+  // order, with the lower index in the reference's outer role.  Each block
+  // takes kPLSCleanTile consecutive sorted pLS (one per thread) and streams,
+  // through shared memory, the later sorted positions that can lie within 0.1
+  // in eta of any of them: up to kPLSBinReach bins above its last pLS's bin,
+  // plus the non-finite bin, which meets every pLS (a NaN never satisfies the
+  // reference's skip); a block holding a non-finite pLS streams to the end.
+  // Each warp tests only the part of that stream its own pLS can reach.
   constexpr int kPLSCleanTile = 128;
-  struct PLSCleanTile {
-    float eta[kPLSCleanTile], phi[kPLSCleanTile], score[kPLSCleanTile];
-    unsigned int idx[kPLSCleanTile];
-    uint4 hits[kPLSCleanTile];
-    int8_t quad[kPLSCleanTile], dup[kPLSCleanTile];
-  };
 
   __global__ void __launch_bounds__(kPLSCleanTile) kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
-    __shared__ PLSCleanTile sT;
+    __shared__ PLSRec sT[kPLSCleanTile];
     const EventView& ev = evs[blockIdx.y];
     unsigned int nPix = ev.ls.nSegments[es.pixelModule];
     if (nPix > kMaxPixelSegments)
       nPix = kMaxPixelSegments;
-    const Segments& s = ev.ls;
-    const unsigned int* order = ev.plsOrder;
+    const PLSRec* rec = ev.plsRec;
     const unsigned int* binStart = ev.plsBinStart;
     const unsigned int nFinite = binStart[kPLSBins];
+    const unsigned int warp = threadIdx.x >> 5;
     for (unsigned int k0 = blockIdx.x * kPLSCleanTile; k0 < nPix; k0 += gridDim.x * kPLSCleanTile) {
       const unsigned int k = k0 + threadIdx.x;
       bool active = k < nPix;
-      unsigned int ix = 0;
-      float eta1 = 0.f, phi1 = 0.f, score1 = 0.f;
-      unsigned int h1[4] = {0, 0, 0, 0};
-      int8_t quad1 = 0;
+      PLSRec me{};
       if (active) {
-        ix = order[k];
-        eta1 = s.eta[ix];
-        phi1 = s.phi[ix];
-        score1 = s.score[ix];
-        quad1 = s.isQuad[ix];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-          h1[a] = s.pLSHitsIdxs[4 * ix + a];
-        if (secondpass && (!quad1 || (s.isDup[ix] & 1)))
+        me = rec[k];
+        if (secondpass && (!plsRecQuad(me.key) || plsRecDup(me.key)))
           active = false;
       }
-      // Sorted positions to stream: [lo, hi) then [nFinite, nPix).
+      // The block's stream of sorted positions, as offsets t: [0, lenA) are
+      // positions k0 + t, [lenA, span) are positions lo2 + (t - lenA).
       const unsigned int kLast = min(k0 + kPLSCleanTile, nPix) - 1;
-      unsigned int lo = 0, hi = nPix, lo2 = nPix;
-      if (kLast < nFinite) {
-        const int bFirst = plsEtaBin(s.eta[order[k0]]), bLast = plsEtaBin(s.eta[order[kLast]]);
-        lo = binStart[bFirst >= kPLSBinReach ? bFirst - kPLSBinReach : 0];
-        hi = binStart[(bLast + kPLSBinReach < kPLSBins ? bLast + kPLSBinReach : kPLSBins - 1) + 1];
+      const bool finiteBlock = kLast < nFinite;
+      unsigned int hiB = nPix, lo2 = nPix;
+      if (finiteBlock) {
+        hiB = binStart[min(plsEtaBin(rec[kLast].eta) + kPLSBinReach, kPLSBins - 1) + 1];
         lo2 = nFinite;
       }
-      const unsigned int span = (hi - lo) + (nPix - lo2);
+      const unsigned int lenA = hiB - k0;
+      const unsigned int span = lenA + (nPix - lo2);
+      // This warp's part of the stream: [tW0, tW1) and [tW2, span).
+      const unsigned int kW0 = k0 + warp * 32;
+      const unsigned int tW0 = warp * 32;
+      unsigned int tW1 = lenA, tW2 = lenA;
+      if (kW0 < nPix) {
+        const unsigned int kW1 = min(kW0 + 32, nPix) - 1;
+        if (kW1 < nFinite) {
+          tW1 = binStart[min(plsEtaBin(rec[kW1].eta) + kPLSBinReach, kPLSBins - 1) + 1] - k0;
+          tW2 = finiteBlock ? lenA : nFinite - k0;
+        }
+      }
       for (unsigned int t0 = 0; t0 < span; t0 += kPLSCleanTile) {
         __syncthreads();
         const unsigned int t = t0 + threadIdx.x;
-        if (t < span) {
-          const unsigned int pos = t < hi - lo ? lo + t : lo2 + (t - (hi - lo));
-          const unsigned int jx = order[pos];
-          sT.idx[threadIdx.x] = jx;
-          sT.eta[threadIdx.x] = s.eta[jx];
-          sT.phi[threadIdx.x] = s.phi[jx];
-          sT.score[threadIdx.x] = s.score[jx];
-          sT.quad[threadIdx.x] = s.isQuad[jx];
-          sT.dup[threadIdx.x] = s.isDup[jx];
-          sT.hits[threadIdx.x] = make_uint4(s.pLSHitsIdxs[4 * jx], s.pLSHitsIdxs[4 * jx + 1], s.pLSHitsIdxs[4 * jx + 2],
-                                            s.pLSHitsIdxs[4 * jx + 3]);
-        }
+        if (t < span)
+          sT[threadIdx.x] = rec[t < lenA ? k0 + t : lo2 + (t - lenA)];
         __syncthreads();
         if (!active)
           continue;
         const unsigned int nt = min(span - t0, unsigned(kPLSCleanTile));
-        for (unsigned int u = 0; u < nt; ++u) {
-          const unsigned int jx = sT.idx[u];
-          if (jx <= ix)
-            continue;
-          const float eta2 = sT.eta[u];
-          if (fabs_(eta2 - eta1) > 0.1f)
-            continue;
-          if (secondpass && (!sT.quad[u] || (sT.dup[u] & 1)))
-            continue;
-          const int8_t quad_diff = quad1 - sT.quad[u];
-          const float score_diff = score1 - sT.score[u];
-          unsigned int idxToRemove;
-          if (quad_diff > 0)
-            idxToRemove = jx;
-          else if (quad_diff < 0)
-            idxToRemove = ix;
-          else if (score_diff < 0)
-            idxToRemove = jx;
-          else if (score_diff > 0)
-            idxToRemove = ix;
-          else
-            idxToRemove = ix;
-          const uint4 h2 = sT.hits[u];
-          int npMatched = 0;
-          for (int a = 0; a < 4; a++) {
-            const bool pmatched = h1[a] == h2.x || h1[a] == h2.y || h1[a] == h2.z || h1[a] == h2.w;
-            if (pmatched) {
-              npMatched++;
-              if (secondpass)
-                break;
-            }
-          }
-          bool remove = npMatched >= 3;
-          if (secondpass) {
-            const float dEta = fabs_(eta1 - eta2);
-            const float dPhi = wrapDPhi(phi1, sT.phi[u]);
-            const float dR2 = dEta * dEta + dPhi * dPhi;
-            if ((npMatched >= 1) || (dR2 < 1e-5f))
-              remove = true;
-          }
-          if (remove) {
-            if (secondpass)
-              ev.plsFlag[idxToRemove] = 1;
-            else
-              s.isDup[idxToRemove] = 1;
-          }
-        }
+        const unsigned int uEnd1 = tW1 > t0 ? min(tW1 - t0, nt) : 0u;
+        for (unsigned int u = tW0 > t0 ? tW0 - t0 : 0u; u < uEnd1; ++u)
+          if (t0 + u > threadIdx.x)
+            plsCleanPair(ev, me, sT[u], secondpass);
+        for (unsigned int u = tW2 > t0 ? min(tW2 - t0, nt) : 0u; u < nt; ++u)
+          plsCleanPair(ev, me, sT[u], secondpass);
       }
     }
   }
