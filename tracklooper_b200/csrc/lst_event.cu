@@ -493,7 +493,7 @@ namespace {
         break;
       }
       case LST_STAGE_PLS_CLEANING:
-        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
+        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v, false);
         LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d, v,
                    false);
         break;
@@ -540,7 +540,7 @@ namespace {
         LST_LAUNCH(lst::kT5TCScan, one, 1024, d, v);
         LST_LAUNCH(lst::kT5TCEmit, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kT5TCFinish, one, 32, d, v);
-        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
+        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v, true);
         LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d, v,
                    true);
         LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);

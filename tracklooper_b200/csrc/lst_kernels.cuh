@@ -1429,22 +1429,27 @@ namespace lst {
 
   // One pLS as the cleaning passes read it, stored in eta-bin order so that a
   // tile of candidates is one coalesced read: eta, phi, score, the pLS index
-  // with its isQuad byte and bit 0 of its isDup packed above it, and its four
-  // pixel hits.
+  // with its isQuad byte packed above it, and its four pixel hits.
   struct __align__(16) PLSRec {
     float eta, phi, score;
-    unsigned int key;  // index | uint8(isQuad) << 16 | (isDup & 1) << 24
+    unsigned int key;  // index | uint8(isQuad) << 16
     uint4 hits;
   };
   static_assert(kMaxPixelSegments <= 0xffff, "pLS index must fit the record key's low 16 bits");
   LST_DEV unsigned int plsRecIndex(unsigned int key) { return key & 0xffffu; }
-  LST_DEV int8_t plsRecQuad(unsigned int key) { return static_cast<int8_t>((key >> 16) & 0xffu); }
-  LST_DEV bool plsRecDup(unsigned int key) { return (key >> 24) & 1u; }
+  LST_DEV int8_t plsRecQuad(unsigned int key) { return static_cast<int8_t>(key >> 16); }
 
-  // Counting sort of the pLS by eta bin, one block per event; writes the
-  // bin starts and the sorted records.  isDup is sampled here, so the second
-  // pass (which reads the marks of the first) bins after the first pass ends.
-  __global__ void __launch_bounds__(1024) kPLSBin(DeviceES es, const EventView* evs) {
+  // Counting sort, by eta bin, of the pLS a cleaning pass tests, one block per
+  // event: every pLS in the first pass; in the second, only the quads without
+  // a first-pass mark (the reference skips a pair unless both are such, so
+  // the rest take part in no test).  Writes the bin starts (the last entry
+  // being the number of records) and the sorted records.  The second pass
+  // bins after the first pass has ended, so it reads the first pass's marks.
+  LST_DEV bool plsCleanEligible(const Segments& s, unsigned int i, bool secondpass) {
+    return !secondpass || (s.isQuad[i] && !(s.isDup[i] & 1));
+  }
+
+  __global__ void __launch_bounds__(1024) kPLSBin(DeviceES es, const EventView* evs, bool secondpass) {
     __shared__ unsigned int sCount[kPLSBins + 1];
     __shared__ unsigned int sCursor[kPLSBins + 1];
     const EventView& ev = evs[blockIdx.y];
@@ -1456,7 +1461,8 @@ namespace lst {
       sCount[b] = 0;
     __syncthreads();
     for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
-      atomicAdd(&sCount[plsEtaBin(s.eta[i])], 1u);
+      if (plsCleanEligible(s, i, secondpass))
+        atomicAdd(&sCount[plsEtaBin(s.eta[i])], 1u);
     __syncthreads();
     unsigned int c = threadIdx.x <= kPLSBins ? sCount[threadIdx.x] : 0u;
     unsigned int tot;
@@ -1470,12 +1476,13 @@ namespace lst {
     __syncthreads();
     const uint4* hits = reinterpret_cast<const uint4*>(s.pLSHitsIdxs);
     for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x) {
+      if (!plsCleanEligible(s, i, secondpass))
+        continue;
       PLSRec r;
       r.eta = s.eta[i];
       r.phi = s.phi[i];
       r.score = s.score[i];
-      r.key = i | (static_cast<unsigned int>(static_cast<uint8_t>(s.isQuad[i])) << 16) |
-              (static_cast<unsigned int>(s.isDup[i] & 1) << 24);
+      r.key = i | (static_cast<unsigned int>(static_cast<uint8_t>(s.isQuad[i])) << 16);
       r.hits = hits[i];
       ev.plsRec[atomicAdd(&sCursor[plsEtaBin(r.eta)], 1u)] = r;
     }
@@ -1483,22 +1490,54 @@ namespace lst {
 
   // One candidate o (a sorted position after this thread's pLS me): the
   // reference's test of the pair (SDL/Kernels.h:384-473) with the lower index
-  // in its outer role (ix, "1") and the higher in the inner (jx, "2").  The
-  // roles are picked by selects, not by a branch, because which of the two is
-  // lower differs from lane to lane.
+  // in its outer role (ix, "1") and the higher in the inner (jx, "2").  Both
+  // are eligible for the pass (kPLSBin kept no other).  A pair without a
+  // common hit has npMatched 0, so it removes nothing in the first pass and
+  // only through dR2 in the second; that is settled before the role-dependent
+  // work, which only pairs with a common hit reach.  Roles are picked by
+  // selects, not by a branch, because which of the two is lower differs from
+  // lane to lane.
   LST_DEV void plsCleanPair(const EventView& ev, const PLSRec& me, const PLSRec& o, bool secondpass) {
     const float etaO = o.eta;
     if (fabs_(etaO - me.eta) > 0.1f)
       return;
-    const unsigned int keyO = o.key;
-    if (secondpass && (!plsRecQuad(keyO) || plsRecDup(keyO)))
+    const uint4 hO = o.hits, hM = me.hits;
+    const bool common = hM.x == hO.x || hM.x == hO.y || hM.x == hO.z || hM.x == hO.w || hM.y == hO.x ||
+                        hM.y == hO.y || hM.y == hO.z || hM.y == hO.w || hM.z == hO.x || hM.z == hO.y ||
+                        hM.z == hO.z || hM.z == hO.w || hM.w == hO.x || hM.w == hO.y || hM.w == hO.z ||
+                        hM.w == hO.w;
+    if (!common && !secondpass)
       return;
-    const float phiO = o.phi, scoreO = o.score;
-    const uint4 hitsO = o.hits;
+    const unsigned int keyO = o.key;
     const bool meLow = plsRecIndex(me.key) < plsRecIndex(keyO);
+    bool remove;
+    if (common) {
+      const uint4 h1 = meLow ? hM : hO, h2 = meLow ? hO : hM;
+      const unsigned int h1a[4] = {h1.x, h1.y, h1.z, h1.w};
+      int npMatched = 0;
+      for (int k = 0; k < 4; k++) {
+        const bool pmatched = h1a[k] == h2.x || h1a[k] == h2.y || h1a[k] == h2.z || h1a[k] == h2.w;
+        if (pmatched) {
+          npMatched++;
+          if (secondpass)
+            break;
+        }
+      }
+      remove = secondpass ? npMatched >= 1 : npMatched >= 3;
+    } else {
+      const float phiO = o.phi;
+      const float eta1 = meLow ? me.eta : etaO, eta2 = meLow ? etaO : me.eta;
+      const float phi1 = meLow ? me.phi : phiO, phi2 = meLow ? phiO : me.phi;
+      const float dEta = fabs_(eta1 - eta2);
+      const float dPhi = wrapDPhi(phi1, phi2);
+      const float dR2 = dEta * dEta + dPhi * dPhi;
+      remove = dR2 < 1e-5f;
+    }
+    if (!remove)
+      return;
+    const float scoreO = o.score;
     const unsigned int key1 = meLow ? me.key : keyO, key2 = meLow ? keyO : me.key;
     const float score1 = meLow ? me.score : scoreO, score2 = meLow ? scoreO : me.score;
-    const uint4 h1 = meLow ? me.hits : hitsO, h2 = meLow ? hitsO : me.hits;
     const unsigned int ix = plsRecIndex(key1), jx = plsRecIndex(key2);
     const int8_t quad_diff = plsRecQuad(key1) - plsRecQuad(key2);
     const float score_diff = score1 - score2;
@@ -1513,32 +1552,10 @@ namespace lst {
       idxToRemove = ix;
     else
       idxToRemove = ix;
-    const unsigned int h1a[4] = {h1.x, h1.y, h1.z, h1.w};
-    int npMatched = 0;
-    for (int k = 0; k < 4; k++) {
-      const bool pmatched = h1a[k] == h2.x || h1a[k] == h2.y || h1a[k] == h2.z || h1a[k] == h2.w;
-      if (pmatched) {
-        npMatched++;
-        if (secondpass)
-          break;
-      }
-    }
-    bool remove = npMatched >= 3;
-    if (secondpass) {
-      const float eta1 = meLow ? me.eta : etaO, eta2 = meLow ? etaO : me.eta;
-      const float phi1 = meLow ? me.phi : phiO, phi2 = meLow ? phiO : me.phi;
-      const float dEta = fabs_(eta1 - eta2);
-      const float dPhi = wrapDPhi(phi1, phi2);
-      const float dR2 = dEta * dEta + dPhi * dPhi;
-      if ((npMatched >= 1) || (dR2 < 1e-5f))
-        remove = true;
-    }
-    if (remove) {
-      if (secondpass)
-        ev.plsFlag[idxToRemove] = 1;
-      else
-        ev.ls.isDup[idxToRemove] = 1;
-    }
+    if (secondpass)
+      ev.plsFlag[idxToRemove] = 1;
+    else
+      ev.ls.isDup[idxToRemove] = 1;
   }
 
   // pLS duplicate removal (SDL/Kernels.h:384-473).  Pass 1 sets bit 1 of
@@ -1550,51 +1567,46 @@ namespace lst {
   // reference's first test.
   //
   // Each pair is tested once, by the pLS that comes first in the eta-sorted
-  // order, with the lower index in the reference's outer role.  Each block
-  // takes kPLSCleanTile consecutive sorted pLS (one per thread) and streams,
-  // through shared memory, the later sorted positions that can lie within 0.1
-  // in eta of any of them: up to kPLSBinReach bins above its last pLS's bin,
-  // plus the non-finite bin, which meets every pLS (a NaN never satisfies the
-  // reference's skip); a block holding a non-finite pLS streams to the end.
-  // Each warp tests only the part of that stream its own pLS can reach.
+  // records of the pass.  Each block takes kPLSCleanTile consecutive records
+  // (one per thread) and streams, through shared memory, the later records
+  // that can lie within 0.1 in eta of any of them: up to kPLSBinReach bins
+  // above its last record's bin, plus the non-finite bin, which meets every
+  // pLS (a NaN never satisfies the reference's skip); a block holding a
+  // non-finite record streams to the end.  Each warp tests only the part of
+  // that stream its own records can reach.
   constexpr int kPLSCleanTile = 128;
 
   __global__ void __launch_bounds__(kPLSCleanTile) kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
     __shared__ PLSRec sT[kPLSCleanTile];
     const EventView& ev = evs[blockIdx.y];
-    unsigned int nPix = ev.ls.nSegments[es.pixelModule];
-    if (nPix > kMaxPixelSegments)
-      nPix = kMaxPixelSegments;
     const PLSRec* rec = ev.plsRec;
     const unsigned int* binStart = ev.plsBinStart;
     const unsigned int nFinite = binStart[kPLSBins];
+    const unsigned int nRec = binStart[kPLSBins + 1];
     const unsigned int warp = threadIdx.x >> 5;
-    for (unsigned int k0 = blockIdx.x * kPLSCleanTile; k0 < nPix; k0 += gridDim.x * kPLSCleanTile) {
+    for (unsigned int k0 = blockIdx.x * kPLSCleanTile; k0 < nRec; k0 += gridDim.x * kPLSCleanTile) {
       const unsigned int k = k0 + threadIdx.x;
-      bool active = k < nPix;
+      const bool active = k < nRec;
       PLSRec me{};
-      if (active) {
+      if (active)
         me = rec[k];
-        if (secondpass && (!plsRecQuad(me.key) || plsRecDup(me.key)))
-          active = false;
-      }
       // The block's stream of sorted positions, as offsets t: [0, lenA) are
       // positions k0 + t, [lenA, span) are positions lo2 + (t - lenA).
-      const unsigned int kLast = min(k0 + kPLSCleanTile, nPix) - 1;
+      const unsigned int kLast = min(k0 + kPLSCleanTile, nRec) - 1;
       const bool finiteBlock = kLast < nFinite;
-      unsigned int hiB = nPix, lo2 = nPix;
+      unsigned int hiB = nRec, lo2 = nRec;
       if (finiteBlock) {
         hiB = binStart[min(plsEtaBin(rec[kLast].eta) + kPLSBinReach, kPLSBins - 1) + 1];
         lo2 = nFinite;
       }
       const unsigned int lenA = hiB - k0;
-      const unsigned int span = lenA + (nPix - lo2);
+      const unsigned int span = lenA + (nRec - lo2);
       // This warp's part of the stream: [tW0, tW1) and [tW2, span).
       const unsigned int kW0 = k0 + warp * 32;
       const unsigned int tW0 = warp * 32;
       unsigned int tW1 = lenA, tW2 = lenA;
-      if (kW0 < nPix) {
-        const unsigned int kW1 = min(kW0 + 32, nPix) - 1;
+      if (kW0 < nRec) {
+        const unsigned int kW1 = min(kW0 + 32, nRec) - 1;
         if (kW1 < nFinite) {
           tW1 = binStart[min(plsEtaBin(rec[kW1].eta) + kPLSBinReach, kPLSBins - 1) + 1] - k0;
           tW2 = finiteBlock ? lenA : nFinite - k0;
