@@ -387,6 +387,13 @@ namespace lst {
     es.maxTriplets = t3Total;
     es.maxQuintuplets = t5Total;
     buildDetHash(es);
+    // geoMapDetId is sorted and unique: the exact match a binary search finds
+    es.geoMapIndex.assign(es.detIds.size(), -1);
+    for (size_t i = 0; i < es.detIds.size(); ++i) {
+      const auto it = std::lower_bound(es.geoMapDetId.begin(), es.geoMapDetId.end(), es.detIds[i]);
+      if (it != es.geoMapDetId.end() && *it == es.detIds[i])
+        es.geoMapIndex[i] = static_cast<int>(it - es.geoMapDetId.begin());
+    }
     return std::string();
   }
 

@@ -36,6 +36,9 @@ namespace lst {
     // endcap 2S strip orientation, sorted by detId
     std::vector<unsigned int> geoMapDetId;
     std::vector<float> geoMapPhi;
+    // per module: position of its detId in geoMapDetId (-1 when absent), so
+    // that a hit finds its strip orientation without a search
+    std::vector<int> geoMapIndex;
 
     // static per-module offsets and caps (lower modules + the pixel module)
     std::vector<int> mdOffset, mdCap;    // nLowerModules + 1

@@ -196,6 +196,7 @@ namespace lst {
     // endcap 2S strip orientation map (SDL/EndcapGeometry.cc:43-70)
     const unsigned int* geoMapDetId;
     const float* geoMapPhi;
+    const int* geoMapIndex;  // per module: position of its detId in geoMapDetId, or -1
     unsigned int nEndCapMap;
     uint16_t nModules;
     uint16_t nLowerModules;

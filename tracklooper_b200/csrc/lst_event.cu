@@ -205,6 +205,7 @@ namespace {
     m.connectedPixels = upload(c, h.connectedPixels, copies, sizes);
     m.geoMapDetId = upload(c, h.geoMapDetId, copies, sizes);
     m.geoMapPhi = upload(c, h.geoMapPhi, copies, sizes);
+    m.geoMapIndex = upload(c, h.geoMapIndex, copies, sizes);
     m.nEndCapMap = static_cast<unsigned int>(h.geoMapDetId.size());
     m.nModules = h.nModules;
     m.nLowerModules = h.nLowerModules;

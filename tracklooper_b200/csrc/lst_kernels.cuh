@@ -227,7 +227,7 @@ namespace lst {
         }
       }
       if (m.subdets[mi] == Endcap && m.moduleType[mi] == TwoS) {
-        int f = sortedFind(m.geoMapDetId, detId, m.nEndCapMap);
+        const int f = m.geoMapIndex[mi];  // sortedFind(m.geoMapDetId, detId, m.nEndCapMap), per module
         if (f < 0) {
           atomicOr(&ev.sc->status, kStatusUnknownEndcapDetId);
         } else {
@@ -244,10 +244,16 @@ namespace lst {
       h.highEdgeYs[ihit] = hey;
       h.lowEdgeXs[ihit] = lex;
       h.lowEdgeYs[ihit] = ley;
-      int old = atomicCAS(&h.hitRanges[mi * 2], -1, static_cast<int>(ihit));
-      if (old != -1)
-        atomicMin(&h.hitRanges[mi * 2], static_cast<int>(ihit));
-      atomicMax(&h.hitRanges[mi * 2 + 1], static_cast<int>(ihit));
+      // The module's hit range [first, last]: the lanes of this warp on the
+      // same module combine first, and one lane per module updates it.  The
+      // first index starts at -1, the largest value as unsigned, so an
+      // unsigned minimum takes the place of the reference's set-or-minimum.
+      const unsigned int peers = __match_any_sync(__activemask(), static_cast<unsigned int>(mi));
+      const unsigned int first = __reduce_min_sync(peers, ihit), last = __reduce_max_sync(peers, ihit);
+      if (static_cast<unsigned int>(__ffs(peers) - 1) == (threadIdx.x & 31u)) {
+        atomicMin(reinterpret_cast<unsigned int*>(&h.hitRanges[mi * 2]), first);
+        atomicMax(&h.hitRanges[mi * 2 + 1], static_cast<int>(last));
+      }
     }
   }
 
