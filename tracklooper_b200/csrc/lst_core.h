@@ -20,9 +20,12 @@
 #if defined(__CUDACC__)
 #define LST_HD __host__ __device__ __forceinline__
 #define LST_DEV __device__ __forceinline__
-// Large cut algorithms stay out of line on the device: inlined at every call
-// site they overflow the instruction cache of the warps that diverge into them.
-#define LST_HD_BIG __host__ __device__ __noinline__
+// The large cut algorithms are inlined into their kernels.  Out of line, each
+// call saves and restores the caller's live registers through local memory,
+// which cost more than the instruction-cache misses of the larger inlined
+// code once candidates reach them through the sorted pre-selection queues.
+// The double-precision math routines (LST_HD_MATH) stay out of line.
+#define LST_HD_BIG __host__ __device__ __forceinline__
 #else
 #define LST_HD inline
 #define LST_DEV inline
