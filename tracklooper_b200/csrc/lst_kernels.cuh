@@ -368,19 +368,32 @@ namespace lst {
   // Register budgets of the cut kernels, as resident blocks per SM.  The cut
   // kernels wait mostly on dependent loads, so they run faster with more warps
   // resident even where the tighter budget spills a little; the values are
-  // the fastest of a sweep over 2..12 blocks on B200 (PU200 batches).
+  // the fastest of a sweep over 2..14 blocks on B200 (PU200 batches, launch
+  // shapes autotuned for each setting).
 #ifndef LST_LB_MD_B
-#define LST_LB_MD_B 2
+#define LST_LB_MD_B 3
 #endif
-#ifndef LST_LB_LST3_B
-#define LST_LB_LST3_B 8
+#ifndef LST_LB_LS_B
+#define LST_LB_LS_B 12
+#endif
+#ifndef LST_LB_T3_B
+#define LST_LB_T3_B 10
 #endif
 #ifndef LST_LB_EVAL_B
 #define LST_LB_EVAL_B 10
 #endif
+#ifndef LST_LB_T5EVAL_B
+#define LST_LB_T5EVAL_B 8
+#endif
+#ifndef LST_LB_PIXMID_B
+#define LST_LB_PIXMID_B 12
+#endif
 #define LST_LB_MD 256, LST_LB_MD_B
-#define LST_LB_LST3 128, LST_LB_LST3_B
+#define LST_LB_LS 128, LST_LB_LS_B
+#define LST_LB_T3 128, LST_LB_T3_B
 #define LST_LB_EVAL 128, LST_LB_EVAL_B
+#define LST_LB_T5EVAL 128, LST_LB_T5EVAL_B
+#define LST_LB_PIXMID 128, LST_LB_PIXMID_B
   __global__ void __launch_bounds__(LST_LB_MD) kCreateMD(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const int wpb = blockDim.x >> 5;
@@ -474,7 +487,7 @@ namespace lst {
     }
   }
 
-  __global__ void __launch_bounds__(LST_LB_LST3) kCreateLS(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(LST_LB_LS) kCreateLS(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kLSWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sOuter[kLSWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
@@ -681,7 +694,7 @@ namespace lst {
     }
   }
 
-  __global__ void __launch_bounds__(LST_LB_LST3) kCreateT3(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(LST_LB_T3) kCreateT3(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kT3Warps][kT3MaxInner + 1];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
@@ -966,7 +979,7 @@ namespace lst {
     }
   }
 
-  __global__ void __launch_bounds__(LST_LB_EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
+  __global__ void __launch_bounds__(LST_LB_T5EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow)
       return;
@@ -2274,7 +2287,7 @@ namespace lst {
   // are queued again, between the two ends of the first queue; without room
   // there, kPixEval takes the first queue instead.
   template <int K>
-  __global__ void __launch_bounds__(LST_LB_EVAL) kPixMid(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(LST_LB_PIXMID) kPixMid(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int front = ev.sc->pixQueueCount, back = ev.sc->pixQueueBack;
     if (!(front <= kCandQueueCap && back <= kCandQueueCap - front))
