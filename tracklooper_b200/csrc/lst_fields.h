@@ -249,6 +249,7 @@
   X(pixPassPLS, unsigned int, lst::kPixPassCap)       \
   X(pixPassV, float, 8 * lst::kPixPassCap)            \
   X(candQueue, unsigned int, lst::kCandQueueCap)        \
+  X(pixChunkPLS, unsigned int, lst::kPixChunkCap)       \
   X(hitMiniSlope, float, H)                           \
   X(t5Order, unsigned int, lst::kT5SortCap)           \
   X(t5OrderPos, uint16_t, lst::kT5SortCap)            \

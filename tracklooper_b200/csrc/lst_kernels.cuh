@@ -819,6 +819,7 @@ namespace lst {
   // candidates than the flag buffer holds take the walk instead.
   constexpr unsigned int kT5CandCap = 1u << 21;  // candidates per event
   constexpr unsigned int kCandQueueCap = 1u << 18;  // pre-selected candidates per event (T5, pT5, pT3)
+  constexpr unsigned int kPixChunkCap = 1u << 16;   // 32-candidate chunks of the pT5 / pT3 chunk table
   constexpr unsigned int kT5SortCap = 1u << 15;     // quintuplets per event sorted by eta for the TC cleaning
   constexpr unsigned int kT5PassCap = 1u << 16;  // passing candidates per event whose values are kept
   constexpr unsigned int kT5DnnCap = 1u << 14;   // candidates per event classified in kT5Dnn
@@ -2196,6 +2197,15 @@ namespace lst {
       ev.sc->pixQueueBack = 0;
       ev.sc->pixQueue2Count = 0;
     }
+    // The chunk table: candidate 32 j lies in pLS pixChunkPLS[j].
+    if (carry > 32u * kPixChunkCap)
+      return;
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < n; i += blockDim.x) {
+      const unsigned int a = ev.plsCandOff[i], b = ev.plsCandOff[i + 1];
+      for (unsigned int j = (a + 31u) >> 5; j < ((b + 31u) >> 5); ++j)
+        ev.pixChunkPLS[j] = i;
+    }
   }
 
   // (pLS, object) of candidate c.
@@ -2204,13 +2214,23 @@ namespace lst {
                                                unsigned int& obj, uint16_t& mod) {
     const unsigned int nPLS = ev.ls.nSegments[es.pixelModule];
     const unsigned int* off = ev.plsCandOff;
-    int lo = 0, hi = int(nPLS);
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (off[mid] <= c)
-        lo = mid;
-      else
-        hi = mid;
+    // The last pLS whose first candidate is at most c: from the chunk table
+    // and a short walk (pLS without candidates are stepped over), or by a
+    // binary search when the candidates outnumber the table.
+    int lo = 0;
+    if (ev.sc->pixCandTotal <= 32u * kPixChunkCap) {
+      lo = static_cast<int>(ev.pixChunkPLS[c >> 5]);
+      while (off[lo + 1] <= c)
+        ++lo;
+    } else {
+      int hi = int(nPLS);
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= c)
+          lo = mid;
+        else
+          hi = mid;
+      }
     }
     iPLS = lo;
     const unsigned int f = c - off[lo];
