@@ -2526,17 +2526,20 @@ namespace lst {
   }
 
   // ================================================== track candidates
-  // pT3 vs pT5 pixel eta/phi (SDL/TrackCandidate.h:204-243).
+  // pT3 vs pT5 pixel eta/phi (SDL/TrackCandidate.h:204-243).  One warp per
+  // pT3, its lanes splitting the pT5 loop; the outcome is an "any" over it.
   __global__ void kCrossCleanPT3(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nPT3 = *ev.pt3.nPixelTriplets;
     const unsigned int nPT5 = *ev.pt5.nPixelQuintuplets;
     const unsigned int prefix = es.lsOffset[es.nLowerModules];
-    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < nPT3; i += gridDim.x * blockDim.x) {
+    const unsigned int nWarps = gridDim.x * (blockDim.x >> 5);
+    for (unsigned int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nPT3; i += nWarps) {
       if (ev.pt3.isDup[i])
         continue;
-      float eta1 = ev.pt3.eta_pix[i], phi1 = ev.pt3.phi_pix[i];
-      for (unsigned int j = 0; j < nPT5; j++) {
+      const float eta1 = ev.pt3.eta_pix[i], phi1 = ev.pt3.phi_pix[i];
+      bool dup = false;
+      for (unsigned int j = laneId(); j < nPT5; j += 32) {
         unsigned int pLS_jx = ev.pt5.pixelIndices[j];
         float eta2 = ev.ls.eta[pLS_jx - prefix];
         float phi2 = ev.ls.phi[pLS_jx - prefix];
@@ -2544,8 +2547,10 @@ namespace lst {
         float dPhi = wrapDPhi(phi1, phi2);
         float dR2 = dEta * dEta + dPhi * dPhi;
         if (dR2 < 1e-5f)
-          ev.pt3.isDup[i] = 1;
+          dup = true;
       }
+      if (__any_sync(kFullMask, dup) && laneId() == 0)
+        ev.pt3.isDup[i] = 1;
     }
   }
 
@@ -2762,7 +2767,9 @@ namespace lst {
     }
   }
 
-  // T5 vs pT5/pT3 eta/phi (SDL/TrackCandidate.h:245-300); one warp per eligible module.
+  // T5 vs pT5/pT3 eta/phi (SDL/TrackCandidate.h:245-300); one warp per
+  // eligible module, taking its T5s one after the other with the lanes
+  // splitting the pT5 / pT3 loop (the outcome is an "any" over it).
   __global__ void kCrossCleanT5(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -2773,12 +2780,13 @@ namespace lst {
     unsigned int base = ev.rg.quintupletModuleIndices[lm];
     const unsigned int nPT5 = *ev.pt5.nPixelQuintuplets;
     const unsigned int loop_bound = nPT5 + *ev.pt3.nPixelTriplets;
-    for (unsigned int j = laneId(); j < n; j += 32) {
-      unsigned int q = base + j;
+    for (unsigned int j = 0; j < n; ++j) {
+      const unsigned int q = base + j;
       if (ev.t5.isDup[q] or ev.t5.partOfPT5[q])
         continue;
-      float eta1 = ev.t5.eta[q], phi1 = ev.t5.phi[q];
-      for (unsigned int jx = 0; jx < loop_bound; jx++) {
+      const float eta1 = ev.t5.eta[q], phi1 = ev.t5.phi[q];
+      bool dup = false;
+      for (unsigned int jx = laneId(); jx < loop_bound; jx += 32) {
         float eta2, phi2;
         if (jx < nPT5) {
           eta2 = ev.pt5.eta[jx];
@@ -2791,8 +2799,10 @@ namespace lst {
         float dPhi = wrapDPhi(phi1, phi2);
         float dR2 = dEta * dEta + dPhi * dPhi;
         if (dR2 < 1e-3f)
-          ev.t5.isDup[q] = 1;
+          dup = true;
       }
+      if (__any_sync(kFullMask, dup) && laneId() == 0)
+        ev.t5.isDup[q] = 1;
     }
   }
 
