@@ -404,18 +404,45 @@ namespace lst {
   }
 
   // Derived per-MD values for every stored MD (lower modules and the pixel
-  // module); one warp per module.
+  // module).  A warp takes 32 lower modules at a time (a module holds a few
+  // MDs) and shares their MDs out over its lanes: a lane-level prefix of the
+  // modules' counts, and per MD the owning lane by a search over it.
   // The pixel module's mini-doublets (two per pLS, thousands per event) are
-  // shared out over all of the event's threads rather than one warp.
+  // shared out over all of the event's threads.
   __global__ void kMDDerived(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
-    const int wpb = blockDim.x >> 5;
+    const unsigned int nWarps = gridDim.x * (blockDim.x >> 5);
+    const unsigned int lane = laneId();
     MiniDoublets md = ev.md;
-    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < es.nLowerModules; w += gridDim.x * wpb) {
-      const unsigned int n = md.nMDs[w];
-      const unsigned int base = es.mdOffset[w];
-      for (unsigned int k = laneId(); k < n; k += 32)
-        storeMDDerived(md, base + k);
+    for (unsigned int w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32u; w0 < es.nLowerModules;
+         w0 += nWarps * 32u) {
+      const unsigned int w = w0 + lane;
+      const unsigned int n = w < es.nLowerModules ? md.nMDs[w] : 0u;
+      const unsigned int base = w < es.nLowerModules ? static_cast<unsigned int>(es.mdOffset[w]) : 0u;
+      unsigned int incl = n;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(kFullMask, incl, o);
+        if (int(lane) >= o)
+          incl += y;
+      }
+      const unsigned int total = __shfl_sync(kFullMask, incl, 31);
+      for (unsigned int f0 = 0; f0 < total; f0 += 32) {
+        const unsigned int f = f0 + lane;
+        // owner: the first lane whose inclusive count exceeds f
+        int owner = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const unsigned int c = __shfl_sync(kFullMask, incl, owner + step - 1);
+          if (c <= f)
+            owner += step;
+        }
+        const unsigned int ownerIncl = __shfl_sync(kFullMask, incl, owner);
+        const unsigned int ownerN = __shfl_sync(kFullMask, n, owner);
+        const unsigned int ownerBase = __shfl_sync(kFullMask, base, owner);
+        if (f < total)
+          storeMDDerived(md, ownerBase + (f - (ownerIncl - ownerN)));
+      }
     }
     const unsigned int nPix = md.nMDs[es.nLowerModules];
     const unsigned int pixBase = es.mdOffset[es.nLowerModules];
