@@ -509,7 +509,7 @@ namespace {
         LST_LAUNCH(lst::kPT5Count, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
         LST_LAUNCH(lst::kPLSScan, one, 1024, d, v, 0);
         LST_LAUNCH(lst::kPT5Emit, warpGrid(P, lst::kPixWarps, count), 32 * lst::kPixWarps, d, v);
-        LST_LAUNCH_SMEM(lst::kPT5DedupSorted, dim3(1, count), 1024, lst::kPT5DedupSmem, d, v);
+        LST_LAUNCH_SMEM(lst::kPT5DedupHashed, dim3(lst::kPT5DedupBlocks, count), 1024, lst::kPT5DedupSmem, d, v);
         LST_LAUNCH(lst::kPT5Dedup, dim3(blocksFor(lst::kMaxPixelQuintuplets, count, lst::kDedupTile), count),
                    lst::kDedupTile, d, v);
         LST_LAUNCH(lst::kAddPT5TC, one, 1024, d, v);
@@ -652,7 +652,7 @@ namespace {
         {"kPT5Emit", (const void*)lst::kPT5Emit},
         {"kPLSScan", (const void*)lst::kPLSScan},
         {"kPT5Dedup", (const void*)lst::kPT5Dedup},
-        {"kPT5DedupSorted", (const void*)lst::kPT5DedupSorted},
+        {"kPT5DedupHashed", (const void*)lst::kPT5DedupHashed},
         {"kAddPT5TC", (const void*)lst::kAddPT5TC},
         {"kPT3Count", (const void*)lst::kPT3Count},
         {"kPT3Emit", (const void*)lst::kPT3Emit},
@@ -887,7 +887,7 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
   // Kernels whose shared memory exceeds the 48 KB default opt in (per device).
   LST_CUDA(cudaFuncSetAttribute(lst::kCrossCleanPLS, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(lst::kXCleanSmem)));
-  LST_CUDA(cudaFuncSetAttribute(lst::kPT5DedupSorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  LST_CUDA(cudaFuncSetAttribute(lst::kPT5DedupHashed, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(lst::kPT5DedupSmem)));
   LST_CUDA(cudaFuncSetAttribute(lst::kT5RankEmit, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(lst::kT5RankSmem)));

@@ -1833,30 +1833,35 @@ namespace lst {
     }
   }
 
-  // pT5 duplicate removal (SDL/Kernels.h:358-382): a pT5 is dropped if
-  // another shares >= 7 of its 14 hits and has a lower score (ties: the
-  // higher index is dropped).  The other candidates' hits are staged in
-  // shared memory 128 at a time; the outcome per pT5 is an "any" over the
-  // others, so the visiting order does not matter.
   // pT5 duplicate removal (SDL/Kernels.h:356-382): pT5 ix is removed if some
   // jx shares at least 7 of its 14 hit slots and has a lower score (ties: the
   // higher index goes).  The outcome is an OR over jx, and a pair sharing 7
   // slots shares at least one hit, so only pairs that meet in some hit need the
-  // full test.  kPT5DedupSorted (one block per event) sorts the event's
-  // (hit, pT5) entries in shared memory and tests each entry against the other
-  // pT5s of its hit; an event with more than kPT5DedupMaxN pT5s is left to
-  // kPT5Dedup, which tests every pair in shared-memory tiles.
+  // full test.  kPT5DedupHashed (kPT5DedupBlocks blocks per event) chains the
+  // event's (hit, pT5) entries by hit in a shared-memory hash table (a head
+  // per bucket, a next index per entry, filled by one atomicExch per entry),
+  // each block on its own, and tests its share of the entries against the
+  // other entries of the same hit (the marks are only ever set, so the
+  // blocks' marks combine and the walking order does not matter); an event
+  // with more than kPT5DedupMaxN pT5s is left to kPT5Dedup, which tests every
+  // pair in shared-memory tiles.
+  constexpr unsigned int kPT5DedupBlocks = 2;
   constexpr unsigned int kPT5DedupMaxEntries = 16384;
   constexpr unsigned int kPT5DedupMaxN = kPT5DedupMaxEntries / 14;
-  constexpr size_t kPT5DedupSmem = kPT5DedupMaxEntries * sizeof(unsigned long long) +
-                                   kPT5DedupMaxN * 14 * sizeof(unsigned int) + kPT5DedupMaxN * sizeof(float) +
-                                   kPT5DedupMaxN;
+  constexpr unsigned int kPT5DedupBucketBits = 13;
+  constexpr unsigned int kPT5DedupBuckets = 1u << kPT5DedupBucketBits;
+  constexpr unsigned int kPT5DedupNone = 0xffffffffu;
+  constexpr size_t kPT5DedupSmem = kPT5DedupBuckets * sizeof(unsigned int) +
+                                   2 * kPT5DedupMaxEntries * sizeof(unsigned int) +
+                                   kPT5DedupMaxN * sizeof(float) + kPT5DedupMaxN;
+  LST_DEV unsigned int pt5HitBucket(unsigned int h) { return (h * 2654435761u) >> (32 - kPT5DedupBucketBits); }
 
-  __global__ void __launch_bounds__(1024) kPT5DedupSorted(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(1024) kPT5DedupHashed(DeviceES es, const EventView* evs) {
     extern __shared__ __align__(16) unsigned char psm[];
-    unsigned long long* sKey = reinterpret_cast<unsigned long long*>(psm);
-    unsigned int* sHits = reinterpret_cast<unsigned int*>(sKey + kPT5DedupMaxEntries);
-    float* sScore = reinterpret_cast<float*>(sHits + kPT5DedupMaxN * 14);
+    unsigned int* sHead = reinterpret_cast<unsigned int*>(psm);
+    unsigned int* sNext = sHead + kPT5DedupBuckets;
+    unsigned int* sHits = sNext + kPT5DedupMaxEntries;
+    float* sScore = reinterpret_cast<float*>(sHits + kPT5DedupMaxEntries);
     unsigned char* sDup = reinterpret_cast<unsigned char*>(sScore + kPT5DedupMaxN);
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt5.nPixelQuintuplets;
@@ -1864,56 +1869,29 @@ namespace lst {
       return;
     PixelQuintuplets p = ev.pt5;
     const unsigned int E = 14 * n;
-    unsigned int N = 1;
-    while (N < E)
-      N <<= 1;
-    for (unsigned int t = threadIdx.x; t < N; t += blockDim.x) {
-      if (t < E) {
-        const unsigned int h = p.hitIndices[t];
-        sHits[t] = h;
-        sKey[t] = (static_cast<unsigned long long>(h) << 16) | (t / 14);
-      } else {
-        sKey[t] = ~0ull;
-      }
-    }
+    for (unsigned int t = threadIdx.x; t < kPT5DedupBuckets; t += blockDim.x)
+      sHead[t] = kPT5DedupNone;
     for (unsigned int t = threadIdx.x; t < n; t += blockDim.x) {
       sScore[t] = p.score[t];
       sDup[t] = 0;
     }
     __syncthreads();
-    // Bitonic sort of sKey[0, N).
-    for (unsigned int k = 2; k <= N; k <<= 1) {
-      for (unsigned int j = k >> 1; j > 0; j >>= 1) {
-        for (unsigned int i = threadIdx.x; i < N; i += blockDim.x) {
-          const unsigned int l = i ^ j;
-          if (l > i) {
-            const unsigned long long a = sKey[i], b = sKey[l];
-            if (((i & k) == 0) == (a > b)) {
-              sKey[i] = b;
-              sKey[l] = a;
-            }
-          }
-        }
-        __syncthreads();
-      }
+    for (unsigned int t = threadIdx.x; t < E; t += blockDim.x) {
+      const unsigned int h = p.hitIndices[t];
+      sHits[t] = h;
+      sNext[t] = atomicExch(&sHead[pt5HitBucket(h)], t);
     }
-    for (unsigned int e = threadIdx.x; e < E; e += blockDim.x) {
+    __syncthreads();
+    for (unsigned int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
       const unsigned int a = e / 14;
-      const unsigned long long h = sHits[e];
-      // first entry of this hit
-      unsigned int lo = 0, hi = E;
-      while (lo < hi) {
-        const unsigned int mid = (lo + hi) >> 1;
-        if ((sKey[mid] >> 16) < h)
-          lo = mid + 1;
-        else
-          hi = mid;
-      }
+      const unsigned int h = sHits[e];
       const float score1 = sScore[a];
-      for (unsigned int q = lo; q < E && (sKey[q] >> 16) == h; ++q) {
+      for (unsigned int q = sHead[pt5HitBucket(h)]; q != kPT5DedupNone; q = sNext[q]) {
         if (sDup[a])
           break;
-        const unsigned int b = static_cast<unsigned int>(sKey[q] & 0xffffu);
+        if (sHits[q] != h)
+          continue;
+        const unsigned int b = q / 14;
         if (b == a)
           continue;
         const float score2 = sScore[b];
@@ -1945,7 +1923,7 @@ namespace lst {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = *ev.pt5.nPixelQuintuplets;
     if (n <= kPT5DedupMaxN && !ev.forceWalk)
-      return;  // kPT5DedupSorted has done this event
+      return;  // kPT5DedupHashed has done this event
     PixelQuintuplets p = ev.pt5;
     for (unsigned int ixBase = blockIdx.x * kDedupTile; ixBase < n; ixBase += gridDim.x * kDedupTile) {
       const unsigned int ix = ixBase + threadIdx.x;
