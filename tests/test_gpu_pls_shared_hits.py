@@ -5,8 +5,9 @@ The generated events give every pLS hits of its own, so their cleaning passes
 remove pLS only through the second pass's dR2 test.  Here a pileup event gets
 extra pLS copied from its own with one to four hits in common with the
 original (in its order or permuted), with the kinematics kept, nudged or moved
-beyond the 0.1 eta window, and with some quads turned into triplets.  The
-full list is then shuffled, so that the copy is sometimes the lower index and
+beyond the 0.1 eta window, and with some quads turned into triplets; in one
+case some copies and some originals get a NaN or infinite eta.  The full list
+is then shuffled, so that the copy is sometimes the lower index and
 sometimes the higher.  Every store must match the reference's after each
 stage, and both passes must have marked pLS.
 """
@@ -23,7 +24,7 @@ pytestmark = pytest.mark.gpu
 STAGES = ("md", "ls", "t3", "t5", "pls_clean", "pt5", "pt3", "tc")
 
 
-def _with_shared_hit_pls(inp, n_extra, seed):
+def _with_shared_hit_pls(inp, n_extra, seed, n_nonfinite=0):
     rng = np.random.default_rng(seed)
     p = {k: np.asarray(v) for k, v in inp.pls.items()}
     n = inp.n_pls
@@ -63,6 +64,13 @@ def _with_shared_hit_pls(inp, n_extra, seed):
     order = rng.permutation(n + n_extra)
     pls = {k: np.concatenate([p[k], np.array(extra[k], dtype=p[k].dtype)])[order] for k in p}
     pls_sim = np.concatenate([inp.pls_sim, np.array(extra_sim, dtype=inp.pls_sim.dtype)])[order]
+    if n_nonfinite:
+        # NaN and infinite eta on copies (which share hits with others) and on
+        # originals: a NaN never satisfies the reference's |deta| > 0.1 skip
+        copies = rng.choice(np.nonzero(order >= n)[0], n_nonfinite, replace=False)
+        originals = rng.choice(np.nonzero(order < n)[0], n_nonfinite, replace=False)
+        for k, i in enumerate(np.concatenate([copies, originals])):
+            pls["eta"][i] = (np.nan, np.inf, -np.inf)[k % 3]
     return dataclasses.replace(inp, pls=pls, pls_sim=pls_sim, seeds=None)
 
 
@@ -82,9 +90,9 @@ def es():
     e.close()
 
 
-@pytest.mark.parametrize("config,index,n_extra", [(2, 5, 700), (3, 2, 300)])
-def test_shared_hit_pls_match_reference(ref, es, config, index, n_extra):
-    inp = _with_shared_hit_pls(gen.generate_event(config, index), n_extra, seed=17 + index)
+@pytest.mark.parametrize("config,index,n_extra,n_nonfinite", [(2, 5, 700, 0), (3, 2, 300, 0), (3, 4, 300, 24)])
+def test_shared_hit_pls_match_reference(ref, es, config, index, n_extra, n_nonfinite):
+    inp = _with_shared_hit_pls(gen.generate_event(config, index), n_extra, seed=17 + index, n_nonfinite=n_nonfinite)
     ev = lst.Event(es, max_hits=inp.n_hits + 1024)
     dtypes = lst.field_dtypes()
     names = list(dtypes)

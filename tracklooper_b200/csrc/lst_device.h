@@ -137,6 +137,7 @@ namespace lst {
     unsigned int* t5BinStart;   // start of each eta bin in t5Order (bins + 2 entries)
     unsigned int* candQueue;    // candidates passing a pre-selection (T5, then pT5 / pT3), any order
     unsigned int* pixChunkPLS;  // per 32 pT5 / pT3 candidates: the pLS of the first one
+    unsigned int* t5ChunkMod;   // per 32 T5 candidates: the eligible module of the first one
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
     struct PLSRec* plsRec;      // pLS records sorted by eta bin
     unsigned int* plsBinStart;  // start of each eta bin in plsRec (bins + 2 entries)

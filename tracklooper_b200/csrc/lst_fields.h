@@ -250,6 +250,7 @@
   X(pixPassV, float, 8 * lst::kPixPassCap)            \
   X(candQueue, unsigned int, lst::kCandQueueCap)        \
   X(pixChunkPLS, unsigned int, lst::kPixChunkCap)       \
+  X(t5ChunkMod, unsigned int, lst::kT5CandCap / 32)     \
   X(hitMiniSlope, float, H)                           \
   X(t5Order, unsigned int, lst::kT5SortCap)           \
   X(t5OrderPos, uint16_t, lst::kT5SortCap)            \

@@ -932,21 +932,27 @@ namespace lst {
       ev.sc->t5QueueCount = 0;
       ev.sc->t5QueueBack = 0;
     }
+    // The chunk table: candidate 32 j lies in eligible module t5ChunkMod[j]
+    // (filled whenever the candidates are decoded, i.e. without overflow).
+    if (carry > kT5CandCap)
+      return;
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < nE; i += blockDim.x) {
+      const unsigned int a = ev.t5ModOff[i], b = ev.t5ModOff[i + 1];
+      for (unsigned int j = (a + 31u) >> 5; j < ((b + 31u) >> 5); ++j)
+        ev.t5ChunkMod[j] = i;
+    }
   }
 
   // (inner T3, outer T3, lower modules) of quintuplet candidate c.
   __device__ __forceinline__ void t5Decode(const EventView& ev, unsigned int c, unsigned int& innerT3,
                                            unsigned int& outerT3, uint16_t* lm) {
-    const int nE = *ev.rg.nEligibleT5Modules;
+    // The largest w with off[w] <= c: from the chunk table and a short walk
+    // (eligible modules without candidates are stepped over).
     const unsigned int* off = ev.t5ModOff;
-    int lo = 0, hi = nE;  // largest w with off[w] <= c
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (off[mid] <= c)
-        lo = mid;
-      else
-        hi = mid;
-    }
+    int lo = static_cast<int>(ev.t5ChunkMod[c >> 5]);
+    while (off[lo + 1] <= c)
+      ++lo;
     const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
     t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
     lm[0] = lm1;
