@@ -462,13 +462,13 @@ namespace {
       case LST_STAGE_SEGMENTS:
         LST_LAUNCH(lst::kCreateLS, tunedWarpGrid(ev, kTuLS, nLower, count), tunedThreads(ev, kTuLS), d, v);
         LST_LAUNCH(lst::kLSRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
-        LST_LAUNCH(lst::kLSByMD, warpGrid(nLower, lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
+        LST_LAUNCH(lst::kLSByMD, warpGrid(ceilDiv(nLower, 32), lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
       case LST_STAGE_TRIPLETS:
         LST_LAUNCH(lst::kT3Offsets, one, 1024, d, v);
         LST_LAUNCH(lst::kCreateT3, tunedWarpGrid(ev, kTuT3, nLower, count), tunedThreads(ev, kTuT3), d, v);
         LST_LAUNCH(lst::kT3Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
-        LST_LAUNCH(lst::kT3ByMD, warpGrid(nLower, lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
+        LST_LAUNCH(lst::kT3ByMD, warpGrid(ceilDiv(nLower, 32), lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
       case LST_STAGE_QUINTUPLETS: {
         if (ev->t5Method == LST_T5_DNN && !ev->es->haveDnn)

@@ -597,47 +597,196 @@ namespace lst {
     }
   }
 
-  // Segments of each lower module grouped by inner MD (after kCreateLS).
+  // The same grouping for 32 consecutive modules at once (most modules hold a
+  // few objects): their bins lie side by side in bins[0, sum of the modules'
+  // MDs), each object is counted into its module's bin, and a module-relative
+  // start is the running count over all bins minus the objects of the
+  // group's earlier modules (each object lies in a bin of its own module).
+  // Placement takes the group's objects in storage order, so each group stays
+  // stable.  The module of the f-th object or b-th bin is found by a search
+  // over the lanes' prefix counts.  Returns false (having written nothing)
+  // when the bins do not fit, and the caller groups module by module.
+  // nOf(w) = objects of module w (0 for a module past the end), objBase(w) =
+  // its first object, firstMD(w, k) = module-relative first MD of object k.
+  constexpr unsigned int kByMDGroupBins = 512;
+  constexpr int kByMDKeptChunks = 8;  // bins of the first chunks kept in registers between the passes
+  __device__ __forceinline__ int laneOwner(unsigned int incl, unsigned int f) {
+    int owner = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const unsigned int c = __shfl_sync(kFullMask, incl, owner + step - 1);
+      if (c <= f)
+        owner += step;
+    }
+    return owner;
+  }
+  __device__ __forceinline__ unsigned int laneInclusiveSum(unsigned int v) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(kFullMask, v, o);
+      if (int(laneId()) >= o)
+        v += y;
+    }
+    return v;
+  }
+
+  template <typename NOf, typename ObjBase, typename FirstMD>
+  __device__ __forceinline__ bool buildByMDGroup(DeviceES const& es, const EventView& ev, unsigned int w0, NOf nOf,
+                                                 ObjBase objBase, FirstMD firstMD, uint16_t* start, uint16_t* count,
+                                                 uint16_t* perm, unsigned int* bins, unsigned int* cursor) {
+    const unsigned int lane = laneId();
+    const unsigned int w = w0 + lane;
+    const bool inRange = w < es.nLowerModules;
+    const unsigned int n = inRange ? nOf(w) : 0u;
+    const unsigned int nMD = (inRange && n > 0) ? ev.md.nMDs[w] : 0u;
+    const unsigned int mdBase = inRange ? static_cast<unsigned int>(es.mdOffset[w]) : 0u;
+    const unsigned int base = (inRange && n > 0) ? objBase(w) : 0u;
+    const unsigned int objIncl = laneInclusiveSum(n), binIncl = laneInclusiveSum(nMD);
+    const unsigned int nObj = __shfl_sync(kFullMask, objIncl, 31), nBins = __shfl_sync(kFullMask, binIncl, 31);
+    if (nBins > kByMDGroupBins)
+      return false;
+    if (nObj == 0)
+      return true;
+    const unsigned int objExcl = objIncl - n, binExcl = binIncl - nMD;
+    for (unsigned int b = lane; b < nBins; b += 32)
+      bins[b] = 0;
+    __syncwarp();
+    unsigned int kept[kByMDKeptChunks];
+    for (unsigned int f0 = 0; f0 < nObj; f0 += 32) {
+      const unsigned int f = f0 + lane;
+      const int o = laneOwner(objIncl, f);
+      const unsigned int oObjExcl = __shfl_sync(kFullMask, objExcl, o);
+      const unsigned int oBinExcl = __shfl_sync(kFullMask, binExcl, o);
+      unsigned int bin = 0xffffffffu;
+      if (f < nObj) {
+        bin = oBinExcl + firstMD(w0 + o, f - oObjExcl);
+        atomicAdd(&bins[bin], 1u);
+      }
+#pragma unroll
+      for (int c = 0; c < kByMDKeptChunks; ++c)
+        if (f0 == 32u * c)
+          kept[c] = bin;
+    }
+    __syncwarp();
+    // running count over all bins -> module-relative starts
+    unsigned int carry = 0;
+    for (unsigned int b0 = 0; b0 < nBins; b0 += 32) {
+      const unsigned int b = b0 + lane;
+      const unsigned int c = b < nBins ? bins[b] : 0u;
+      const unsigned int incl = laneInclusiveSum(c);
+      const int o = laneOwner(binIncl, b);
+      const unsigned int oObjExcl = __shfl_sync(kFullMask, objExcl, o);
+      const unsigned int oBinExcl = __shfl_sync(kFullMask, binExcl, o);
+      const unsigned int oMdBase = __shfl_sync(kFullMask, mdBase, o);
+      if (b < nBins) {
+        const unsigned int rel = carry + incl - c - oObjExcl;
+        cursor[b] = rel;
+        start[oMdBase + (b - oBinExcl)] = static_cast<uint16_t>(rel);
+        count[oMdBase + (b - oBinExcl)] = static_cast<uint16_t>(c);
+      }
+      carry += __shfl_sync(kFullMask, incl, 31);
+    }
+    __syncwarp();
+    // stable placement, 32 objects at a time
+    for (unsigned int f0 = 0; f0 < nObj; f0 += 32) {
+      const unsigned int f = f0 + lane;
+      const int o = laneOwner(objIncl, f);
+      const unsigned int oObjExcl = __shfl_sync(kFullMask, objExcl, o);
+      const unsigned int oBinExcl = __shfl_sync(kFullMask, binExcl, o);
+      const unsigned int oBase = __shfl_sync(kFullMask, base, o);
+      const bool valid = f < nObj;
+      const unsigned int k = f - oObjExcl;
+      unsigned int bin = 0xffffffffu;
+      if (f0 < 32u * kByMDKeptChunks) {
+#pragma unroll
+        for (int c = 0; c < kByMDKeptChunks; ++c)
+          if (f0 == 32u * c)
+            bin = kept[c];
+      } else if (valid) {
+        bin = oBinExcl + firstMD(w0 + o, k);
+      }
+      const unsigned int active = __ballot_sync(kFullMask, valid);
+      const unsigned int peers = __match_any_sync(kFullMask, bin) & active;
+      if (valid) {
+        const unsigned int rank = __popc(peers & lanesBelowMask());
+        perm[oBase + cursor[bin] + rank] = static_cast<uint16_t>(k);
+      }
+      __syncwarp();
+      if (valid && lane == 31u - __clz(peers))
+        cursor[bin] += __popc(peers);
+      __syncwarp();
+    }
+    return true;
+  }
+
+  // Segments of each lower module grouped by inner MD (after kCreateLS): a
+  // warp takes 32 modules at a time, module by module where their bins do
+  // not fit (or the fallback paths are forced).
   constexpr int kIdxWarps = 4;
   __global__ void kLSByMD(DeviceES es, const EventView* evs) {
-    __shared__ unsigned int sBins[kIdxWarps][kMaxModuleMDs];
-    __shared__ unsigned int sCursor[kIdxWarps][kMaxModuleMDs];
+    __shared__ unsigned int sBins[kIdxWarps][kByMDGroupBins];
+    __shared__ unsigned int sCursor[kIdxWarps][kByMDGroupBins];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
-    for (int w = blockIdx.x * kIdxWarps + wib; w < es.nLowerModules; w += gridDim.x * kIdxWarps) {
+    const unsigned int* mdIdx = ev.ls.mdIndices;
+    const unsigned int nWarps = gridDim.x * kIdxWarps;
+    for (unsigned int w0 = (blockIdx.x * kIdxWarps + wib) * 32u; w0 < es.nLowerModules; w0 += nWarps * 32u) {
       __syncwarp();
-      const unsigned int n = ev.ls.nSegments[w];
-      if (n == 0)
+      if (!ev.forceWalk &&
+          buildByMDGroup(
+              es, ev, w0, [&](unsigned int w) { return static_cast<unsigned int>(ev.ls.nSegments[w]); },
+              [&](unsigned int w) { return static_cast<unsigned int>(es.lsOffset[w]); },
+              [&](unsigned int w, unsigned int k) { return mdIdx[2 * (es.lsOffset[w] + k)] - es.mdOffset[w]; },
+              ev.mdLSStart, ev.mdLSCount, ev.lsByMD, sBins[wib], sCursor[wib]))
         continue;
-      const unsigned int mdBase = es.mdOffset[w];
-      const unsigned int nMD = ev.md.nMDs[w];
-      const unsigned int segBase = es.lsOffset[w];
-      const unsigned int* mdIdx = ev.ls.mdIndices;
-      buildByMD(
-          n, nMD, [&](unsigned int k) { return mdIdx[2 * (segBase + k)] - mdBase; }, ev.mdLSStart + mdBase,
-          ev.mdLSCount + mdBase, ev.lsByMD + segBase, sBins[wib], sCursor[wib]);
+      for (unsigned int w = w0; w < w0 + 32u && w < es.nLowerModules; ++w) {
+        __syncwarp();
+        const unsigned int n = ev.ls.nSegments[w];
+        if (n == 0)
+          continue;
+        const unsigned int mdBase = es.mdOffset[w];
+        const unsigned int nMD = ev.md.nMDs[w];
+        const unsigned int segBase = es.lsOffset[w];
+        buildByMD(
+            n, nMD, [&](unsigned int k) { return mdIdx[2 * (segBase + k)] - mdBase; }, ev.mdLSStart + mdBase,
+            ev.mdLSCount + mdBase, ev.lsByMD + segBase, sBins[wib], sCursor[wib]);
+      }
     }
   }
 
-  // Triplets of each lower module grouped by first MD (after kCreateT3).
+  // Triplets of each lower module grouped by first MD (after kCreateT3), in
+  // the same way.
   __global__ void kT3ByMD(DeviceES es, const EventView* evs) {
-    __shared__ unsigned int sBins[kIdxWarps][kMaxModuleMDs];
-    __shared__ unsigned int sCursor[kIdxWarps][kMaxModuleMDs];
+    __shared__ unsigned int sBins[kIdxWarps][kByMDGroupBins];
+    __shared__ unsigned int sCursor[kIdxWarps][kByMDGroupBins];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
-    for (int w = blockIdx.x * kIdxWarps + wib; w < es.nLowerModules; w += gridDim.x * kIdxWarps) {
+    const unsigned int* segIdx = ev.t3.segmentIndices;
+    const unsigned int* mdIdx = ev.ls.mdIndices;
+    const unsigned int nWarps = gridDim.x * kIdxWarps;
+    for (unsigned int w0 = (blockIdx.x * kIdxWarps + wib) * 32u; w0 < es.nLowerModules; w0 += nWarps * 32u) {
       __syncwarp();
-      const unsigned int n = ev.t3.nTriplets[w];
-      if (n == 0)
+      if (!ev.forceWalk &&
+          buildByMDGroup(
+              es, ev, w0, [&](unsigned int w) { return static_cast<unsigned int>(ev.t3.nTriplets[w]); },
+              [&](unsigned int w) { return static_cast<unsigned int>(ev.rg.tripletModuleIndices[w]); },
+              [&](unsigned int w, unsigned int k) {
+                return mdIdx[2 * segIdx[2 * (ev.rg.tripletModuleIndices[w] + k)]] - es.mdOffset[w];
+              },
+              ev.mdT3Start, ev.mdT3Count, ev.t3ByMD, sBins[wib], sCursor[wib]))
         continue;
-      const unsigned int mdBase = es.mdOffset[w];
-      const unsigned int nMD = ev.md.nMDs[w];
-      const unsigned int t3Base = ev.rg.tripletModuleIndices[w];
-      const unsigned int* segIdx = ev.t3.segmentIndices;
-      const unsigned int* mdIdx = ev.ls.mdIndices;
-      buildByMD(
-          n, nMD, [&](unsigned int k) { return mdIdx[2 * segIdx[2 * (t3Base + k)]] - mdBase; },
-          ev.mdT3Start + mdBase, ev.mdT3Count + mdBase, ev.t3ByMD + t3Base, sBins[wib], sCursor[wib]);
+      for (unsigned int w = w0; w < w0 + 32u && w < es.nLowerModules; ++w) {
+        __syncwarp();
+        const unsigned int n = ev.t3.nTriplets[w];
+        if (n == 0)
+          continue;
+        const unsigned int mdBase = es.mdOffset[w];
+        const unsigned int nMD = ev.md.nMDs[w];
+        const unsigned int t3Base = ev.rg.tripletModuleIndices[w];
+        buildByMD(
+            n, nMD, [&](unsigned int k) { return mdIdx[2 * segIdx[2 * (t3Base + k)]] - mdBase; },
+            ev.mdT3Start + mdBase, ev.mdT3Count + mdBase, ev.t3ByMD + t3Base, sBins[wib], sCursor[wib]);
+      }
     }
   }
 
