@@ -792,25 +792,29 @@ namespace lst {
 
   // ============================================================ triplets
   // Per-module triplet offsets (SDL/Triplet.h:1007-1102); one block per event.
+  // Each thread takes a contiguous range of modules, so that one block scan
+  // of the per-thread sums gives every module its offset.
   __global__ void __launch_bounds__(1024) kT3Offsets(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
-    unsigned int carry = 0;
-    for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
-      unsigned int i = base + threadIdx.x;
-      unsigned int occ = 0;
-      bool valid = i < es.nLowerModules;
-      if (valid && ev.ls.nSegments[i] != 0)
-        occ = static_cast<unsigned int>(es.t3CapIfUsed[i]);
-      unsigned int tot;
-      unsigned int ex = blockExclusiveScan(occ, tot);
-      if (valid) {
-        ev.rg.tripletModuleIndices[i] = static_cast<int>(carry + ex);
-        ev.rg.tripletModuleOccupancy[i] = static_cast<int>(occ);
-      }
-      carry += tot;
+    const unsigned int n = es.nLowerModules;
+    const unsigned int per = (n + blockDim.x - 1) / blockDim.x;
+    const unsigned int i0 = min(threadIdx.x * per, n), i1 = min(i0 + per, n);
+    auto occOf = [&](unsigned int i) {
+      return ev.ls.nSegments[i] != 0 ? static_cast<unsigned int>(es.t3CapIfUsed[i]) : 0u;
+    };
+    unsigned int mine = 0;
+    for (unsigned int i = i0; i < i1; ++i)
+      mine += occOf(i);
+    unsigned int tot;
+    unsigned int run = blockExclusiveScan(mine, tot);
+    for (unsigned int i = i0; i < i1; ++i) {
+      const unsigned int occ = occOf(i);
+      ev.rg.tripletModuleIndices[i] = static_cast<int>(run);
+      ev.rg.tripletModuleOccupancy[i] = static_cast<int>(occ);
+      run += occ;
     }
     if (threadIdx.x == 0)
-      *ev.rg.device_nTotalTrips = carry;
+      *ev.rg.device_nTotalTrips = tot;
   }
 
   // One warp per inner-inner lower module walking (inner segment, outer
@@ -897,28 +901,34 @@ namespace lst {
 
   // ========================================================= quintuplets
   // Eligible T5 seed modules and their offsets (SDL/Quintuplet.h:3117-3213).
+  // Contiguous module ranges per thread, as in kT3Offsets.
   __global__ void __launch_bounds__(1024) kT5Eligible(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
-    unsigned int carryN = 0, carryQ = 0;
-    for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
-      unsigned int i = base + threadIdx.x;
-      bool valid = i < es.nLowerModules;
-      bool elig = valid && ev.t3.nTriplets[i] != 0 && es.t5CapIfEligible[i] >= 0;
-      unsigned int occ = elig ? static_cast<unsigned int>(es.t5CapIfEligible[i]) : 0u;
-      unsigned int totN, totQ;
-      unsigned int exN = blockExclusiveScan(elig ? 1u : 0u, totN);
-      unsigned int exQ = blockExclusiveScan(occ, totQ);
-      if (elig) {
-        ev.rg.indicesOfEligibleT5Modules[carryN + exN] = static_cast<uint16_t>(i);
-        ev.rg.quintupletModuleIndices[i] = static_cast<int>(carryQ + exQ);
-        ev.rg.quintupletModuleOccupancy[i] = static_cast<int>(occ);
+    const unsigned int n = es.nLowerModules;
+    const unsigned int per = (n + blockDim.x - 1) / blockDim.x;
+    const unsigned int i0 = min(threadIdx.x * per, n), i1 = min(i0 + per, n);
+    auto eligible = [&](unsigned int i) { return ev.t3.nTriplets[i] != 0 && es.t5CapIfEligible[i] >= 0; };
+    unsigned int myN = 0, myQ = 0;
+    for (unsigned int i = i0; i < i1; ++i)
+      if (eligible(i)) {
+        ++myN;
+        myQ += static_cast<unsigned int>(es.t5CapIfEligible[i]);
       }
-      carryN += totN;
-      carryQ += totQ;
+    unsigned int totN, totQ;
+    unsigned int runN = blockExclusiveScan(myN, totN);
+    unsigned int runQ = blockExclusiveScan(myQ, totQ);
+    for (unsigned int i = i0; i < i1; ++i) {
+      if (!eligible(i))
+        continue;
+      const unsigned int occ = static_cast<unsigned int>(es.t5CapIfEligible[i]);
+      ev.rg.indicesOfEligibleT5Modules[runN++] = static_cast<uint16_t>(i);
+      ev.rg.quintupletModuleIndices[i] = static_cast<int>(runQ);
+      ev.rg.quintupletModuleOccupancy[i] = static_cast<int>(occ);
+      runQ += occ;
     }
     if (threadIdx.x == 0) {
-      *ev.rg.nEligibleT5Modules = static_cast<uint16_t>(carryN);
-      *ev.rg.device_nTotalQuints = carryQ;
+      *ev.rg.nEligibleT5Modules = static_cast<uint16_t>(totN);
+      *ev.rg.device_nTotalQuints = totQ;
     }
   }
 
@@ -3275,14 +3285,19 @@ namespace lst {
     const unsigned int nT5TC = *ev.tc.nTrackCandidatesT5;
     TrackCandidates tc = ev.tc;
     const Segments& s = ev.ls;
-    unsigned int carry = 0;
-    for (unsigned int base = 0; base < n; base += blockDim.x) {
-      unsigned int i = base + threadIdx.x;
-      bool f = i < n && s.isQuad[i] && !s.isDup[i];
-      unsigned int tot;
-      unsigned int ex = blockExclusiveScan(f ? 1u : 0u, tot);
-      unsigned int idx = start + carry + ex;
-      if (f && idx - nT5TC < kMaxPixelTrackCandidates) {
+    // Each thread takes a contiguous range of pLS, so that one block scan of
+    // the per-thread counts gives every accepted pLS its place in pLS order.
+    const unsigned int per = (n + blockDim.x - 1) / blockDim.x;
+    const unsigned int i0 = min(threadIdx.x * per, n), i1 = min(i0 + per, n);
+    unsigned int mine = 0;
+    for (unsigned int i = i0; i < i1; ++i)
+      mine += (s.isQuad[i] && !s.isDup[i]) ? 1u : 0u;
+    unsigned int carry;
+    unsigned int idx = start + blockExclusiveScan(mine, carry);
+    for (unsigned int i = i0; i < i1; ++i) {
+      if (!(s.isQuad[i] && !s.isDup[i]))
+        continue;
+      if (idx - nT5TC < kMaxPixelTrackCandidates) {
         tc.trackCandidateType[idx] = 8;
         tc.directObjectIndices[idx] = i;
         tc.pixelSeedIndex[idx] = static_cast<int>(s.seedIdx[i]);
@@ -3302,7 +3317,7 @@ namespace lst {
         tc.centerY[idx] = 0;
         tc.radius[idx] = 0;
       }
-      carry += tot;
+      ++idx;
     }
     if (threadIdx.x == 0) {
       unsigned int room = (start - nT5TC < kMaxPixelTrackCandidates) ? kMaxPixelTrackCandidates - (start - nT5TC) : 0u;
