@@ -139,7 +139,9 @@ namespace lst {
     unsigned int* pixChunkPLS;  // per 32 pT5 / pT3 candidates: the pLS of the first one
     unsigned int* t5ChunkMod;   // per 32 T5 candidates: the eligible module of the first one
     struct TCCleanInfo* tcCleanInfo;  // per track candidate: the pLS cross-cleaning record
-    struct PLSRec* plsRec;      // pLS records sorted by eta bin
+    struct PLSRec* plsRec;      // pass-2 pLS records sorted by eta bin
+    unsigned int* plsHitHead;   // hit -> pLS index of the pLS cleaning: chain head per bucket
+    unsigned int* plsHitNext;   //   and the next entry (4 pLS + hit slot) per entry
     unsigned int* plsBinStart;  // start of each eta bin in plsRec (bins + 2 entries)
     unsigned int maxHits;
     unsigned int forceWalk;  // take the fallback paths (walks, pair-by-pair tests) for testing them

@@ -419,6 +419,7 @@ namespace {
   int runPixelIngest(lst_event* ev, int first, int count) {
     const lst::DeviceES& d = ev->es->view;
     cudaStream_t s = ev->stream;
+    LST_LAUNCH(lst::kPLSHitReset, dim3(blocksFor(lst::kPLSHitBuckets, count), count), kThreads, ev->dv + first);
     LST_LAUNCH(lst::kPixelIngest, dim3(blocksFor(lst::kMaxPixelSegments, count), count), kThreads, d, ev->dv + first);
     return 0;
   }
@@ -494,9 +495,7 @@ namespace {
         break;
       }
       case LST_STAGE_PLS_CLEANING:
-        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v, false);
-        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d, v,
-                   false);
+        LST_LAUNCH(lst::kPLSCleanHits, dim3(blocksFor(P, count), count), kThreads, d, v, false);
         break;
       case LST_STAGE_PIXEL_QUINTUPLETS:
         LST_LAUNCH(lst::kPixelConnect, dim3(blocksFor(P, count), count), kThreads, d, v);
@@ -541,9 +540,10 @@ namespace {
         LST_LAUNCH(lst::kT5TCScan, one, 1024, d, v);
         LST_LAUNCH(lst::kT5TCEmit, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kT5TCFinish, one, 32, d, v);
-        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v, true);
-        LST_LAUNCH(lst::kPLSClean, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d, v,
-                   true);
+        LST_LAUNCH(lst::kPLSBin, one, 1024, d, v);
+        LST_LAUNCH(lst::kPLSCleanHits, dim3(blocksFor(P, count), count), kThreads, d, v, true);
+        LST_LAUNCH(lst::kPLSCleanNear, dim3(blocksFor(P, count, lst::kPLSCleanTile), count), lst::kPLSCleanTile, d,
+                   v);
         LST_LAUNCH(lst::kMergePLSFlag, dim3(blocksFor(P, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kTCCleanInfo, dim3(blocksFor(lst::kMaxTrackCandidates, count), count), kThreads, d, v);
         LST_LAUNCH_SMEM(lst::kCrossCleanPLS, dim3(lst::kXCleanBlocksPerEvent, count), 1024, lst::kXCleanSmem, d, v);
@@ -633,7 +633,9 @@ namespace {
         {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
         {"kT5Ranges", (const void*)lst::kT5Ranges},
         {"kPLSBin", (const void*)lst::kPLSBin},
-        {"kPLSClean", (const void*)lst::kPLSClean},
+        {"kPLSHitReset", (const void*)lst::kPLSHitReset},
+        {"kPLSCleanHits", (const void*)lst::kPLSCleanHits},
+        {"kPLSCleanNear", (const void*)lst::kPLSCleanNear},
         {"kMergePLSFlag", (const void*)lst::kMergePLSFlag},
         {"kPixelConnect", (const void*)lst::kPixelConnect},
         {"kPixPrefix<5>", (const void*)lst::kPixPrefix<5>},

@@ -260,4 +260,6 @@
   X(hitShiftZn, float, H)                             \
   X(tcCleanInfo, lst::TCCleanInfo, TC)                \
   X(plsRec, lst::PLSRec, P)                           \
+  X(plsHitHead, unsigned int, lst::kPLSHitBuckets)      \
+  X(plsHitNext, unsigned int, 4 * P)                   \
   X(plsBinStart, unsigned int, lst::kPLSBins + 2)

@@ -112,6 +112,21 @@ namespace lst {
   }
 
   // =============================================================== reset
+  // Hit -> pLS index of the pLS cleaning: chains of (pLS, hit slot) entries
+  // e = 4 pLS + slot in a hash table keyed by the stored pixel hit
+  // (pLSHitsIdxs[e]): a head per bucket, a next entry per entry.  kPLSHitReset
+  // empties the heads right before kPixelIngest inserts every entry once.
+  constexpr unsigned int kPLSHitBucketBits = 15;
+  constexpr unsigned int kPLSHitBuckets = 1u << kPLSHitBucketBits;
+  constexpr unsigned int kPLSHitNone = 0xffffffffu;
+  LST_DEV unsigned int plsHitBucket(unsigned int h) { return (h * 2654435761u) >> (32 - kPLSHitBucketBits); }
+
+  __global__ void kPLSHitReset(const EventView* evs) {
+    const EventView& ev = evs[blockIdx.y];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < kPLSHitBuckets; i += gridDim.x * blockDim.x)
+      ev.plsHitHead[i] = kPLSHitNone;
+  }
+
   __global__ void kResetEvent(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nMod = es.nModules, nLower = es.nLowerModules;
@@ -297,6 +312,10 @@ namespace lst {
       storePixelSegment(
           es.m, ev.hits, md, ls, pix, mdBase, lsBase, tid, hit[0], hit[1], hit[2], hit[3], ev.plsDPhiChange[tid]);
       ls.partOfPT5[tid] = 0;
+      for (unsigned int slot = 0; slot < 4; ++slot) {
+        const unsigned int e = 4 * tid + slot;
+        ev.plsHitNext[e] = atomicExch(&ev.plsHitHead[plsHitBucket(ls.pLSHitsIdxs[e])], e);
+      }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       md.nMDs[pix] = 2 * nPLS;
@@ -1639,120 +1658,12 @@ namespace lst {
     return static_cast<int>(t);
   }
 
-  // One pLS as the cleaning passes read it, stored in eta-bin order so that a
-  // tile of candidates is one coalesced read: eta, phi, score, the pLS index
-  // with its isQuad byte packed above it, and its four pixel hits.
-  struct __align__(16) PLSRec {
-    float eta, phi, score;
-    unsigned int key;  // index | uint8(isQuad) << 16
-    uint4 hits;
-  };
-  static_assert(kMaxPixelSegments <= 0xffff, "pLS index must fit the record key's low 16 bits");
-  LST_DEV unsigned int plsRecIndex(unsigned int key) { return key & 0xffffu; }
-  LST_DEV int8_t plsRecQuad(unsigned int key) { return static_cast<int8_t>(key >> 16); }
-
-  // Counting sort, by eta bin, of the pLS a cleaning pass tests, one block per
-  // event: every pLS in the first pass; in the second, only the quads without
-  // a first-pass mark (the reference skips a pair unless both are such, so
-  // the rest take part in no test).  Writes the bin starts (the last entry
-  // being the number of records) and the sorted records.  The second pass
-  // bins after the first pass has ended, so it reads the first pass's marks.
-  LST_DEV bool plsCleanEligible(const Segments& s, unsigned int i, bool secondpass) {
-    return !secondpass || (s.isQuad[i] && !(s.isDup[i] & 1));
-  }
-
-  __global__ void __launch_bounds__(1024) kPLSBin(DeviceES es, const EventView* evs, bool secondpass) {
-    __shared__ unsigned int sCount[kPLSBins + 1];
-    __shared__ unsigned int sCursor[kPLSBins + 1];
-    const EventView& ev = evs[blockIdx.y];
+  // The removal of one tested pLS pair (SDL/Kernels.h:384-473): ix the lower
+  // index (the reference's outer loop), jx the higher; marks the one to go.
+  LST_DEV void plsRemoveOf(const EventView& ev, unsigned int ix, unsigned int jx, bool secondpass) {
     const Segments& s = ev.ls;
-    unsigned int nPix = s.nSegments[es.pixelModule];
-    if (nPix > kMaxPixelSegments)
-      nPix = kMaxPixelSegments;
-    for (int b = threadIdx.x; b <= kPLSBins; b += blockDim.x)
-      sCount[b] = 0;
-    __syncthreads();
-    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
-      if (plsCleanEligible(s, i, secondpass))
-        atomicAdd(&sCount[plsEtaBin(s.eta[i])], 1u);
-    __syncthreads();
-    unsigned int c = threadIdx.x <= kPLSBins ? sCount[threadIdx.x] : 0u;
-    unsigned int tot;
-    unsigned int ex = blockExclusiveScan(c, tot);
-    if (threadIdx.x <= kPLSBins) {
-      sCursor[threadIdx.x] = ex;
-      ev.plsBinStart[threadIdx.x] = ex;
-    }
-    if (threadIdx.x == 0)
-      ev.plsBinStart[kPLSBins + 1] = tot;
-    __syncthreads();
-    const uint4* hits = reinterpret_cast<const uint4*>(s.pLSHitsIdxs);
-    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x) {
-      if (!plsCleanEligible(s, i, secondpass))
-        continue;
-      PLSRec r;
-      r.eta = s.eta[i];
-      r.phi = s.phi[i];
-      r.score = s.score[i];
-      r.key = i | (static_cast<unsigned int>(static_cast<uint8_t>(s.isQuad[i])) << 16);
-      r.hits = hits[i];
-      ev.plsRec[atomicAdd(&sCursor[plsEtaBin(r.eta)], 1u)] = r;
-    }
-  }
-
-  // One candidate o (a sorted position after this thread's pLS me): the
-  // reference's test of the pair (SDL/Kernels.h:384-473) with the lower index
-  // in its outer role (ix, "1") and the higher in the inner (jx, "2").  Both
-  // are eligible for the pass (kPLSBin kept no other).  A pair without a
-  // common hit has npMatched 0, so it removes nothing in the first pass and
-  // only through dR2 in the second; that is settled before the role-dependent
-  // work, which only pairs with a common hit reach.  Roles are picked by
-  // selects, not by a branch, because which of the two is lower differs from
-  // lane to lane.
-  LST_DEV void plsCleanPair(const EventView& ev, const PLSRec& me, const PLSRec& o, bool secondpass) {
-    const float etaO = o.eta;
-    if (fabs_(etaO - me.eta) > 0.1f)
-      return;
-    const uint4 hO = o.hits, hM = me.hits;
-    const bool common = hM.x == hO.x || hM.x == hO.y || hM.x == hO.z || hM.x == hO.w || hM.y == hO.x ||
-                        hM.y == hO.y || hM.y == hO.z || hM.y == hO.w || hM.z == hO.x || hM.z == hO.y ||
-                        hM.z == hO.z || hM.z == hO.w || hM.w == hO.x || hM.w == hO.y || hM.w == hO.z ||
-                        hM.w == hO.w;
-    if (!common && !secondpass)
-      return;
-    const unsigned int keyO = o.key;
-    const bool meLow = plsRecIndex(me.key) < plsRecIndex(keyO);
-    bool remove;
-    if (common) {
-      const uint4 h1 = meLow ? hM : hO, h2 = meLow ? hO : hM;
-      const unsigned int h1a[4] = {h1.x, h1.y, h1.z, h1.w};
-      int npMatched = 0;
-      for (int k = 0; k < 4; k++) {
-        const bool pmatched = h1a[k] == h2.x || h1a[k] == h2.y || h1a[k] == h2.z || h1a[k] == h2.w;
-        if (pmatched) {
-          npMatched++;
-          if (secondpass)
-            break;
-        }
-      }
-      remove = secondpass ? npMatched >= 1 : npMatched >= 3;
-    } else {
-      const float phiO = o.phi;
-      const float eta1 = meLow ? me.eta : etaO, eta2 = meLow ? etaO : me.eta;
-      const float phi1 = meLow ? me.phi : phiO, phi2 = meLow ? phiO : me.phi;
-      const float dEta = fabs_(eta1 - eta2);
-      const float dPhi = wrapDPhi(phi1, phi2);
-      const float dR2 = dEta * dEta + dPhi * dPhi;
-      remove = dR2 < 1e-5f;
-    }
-    if (!remove)
-      return;
-    const float scoreO = o.score;
-    const unsigned int key1 = meLow ? me.key : keyO, key2 = meLow ? keyO : me.key;
-    const float score1 = meLow ? me.score : scoreO, score2 = meLow ? scoreO : me.score;
-    const unsigned int ix = plsRecIndex(key1), jx = plsRecIndex(key2);
-    const int8_t quad_diff = plsRecQuad(key1) - plsRecQuad(key2);
-    const float score_diff = score1 - score2;
+    const int8_t quad_diff = s.isQuad[ix] - s.isQuad[jx];
+    const float score_diff = s.score[ix] - s.score[jx];
     unsigned int idxToRemove;
     if (quad_diff > 0)
       idxToRemove = jx;
@@ -1767,7 +1678,11 @@ namespace lst {
     if (secondpass)
       ev.plsFlag[idxToRemove] = 1;
     else
-      ev.ls.isDup[idxToRemove] = 1;
+      s.isDup[idxToRemove] = 1;
+  }
+
+  LST_DEV bool plsCleanEligible(const Segments& s, unsigned int i, bool secondpass) {
+    return !secondpass || (s.isQuad[i] && !(s.isDup[i] & 1));
   }
 
   // pLS duplicate removal (SDL/Kernels.h:384-473).  Pass 1 sets bit 1 of
@@ -1775,70 +1690,167 @@ namespace lst {
   // afterwards, so that pass 2 reads the pass-1 bit while other threads mark
   // removals.  The outcome of a pair (ix < jx) depends only on the two pLS, and
   // marks are only ever set, so any visiting order and any repeat visit give
-  // the reference's result; pairs more than 0.1 apart in eta return at the
-  // reference's first test.
+  // the reference's result.  A pair removes a pLS
+  //   pass 1: if ix has at least 3 of its 4 hits among jx's (npMatched >= 3),
+  //   pass 2: if they have a hit in common (npMatched >= 1) or dR2 < 1e-5,
+  // in both cases unless |deta| > 0.1 (a NaN never satisfies that skip), and
+  // in pass 2 only between quads without a pass-1 mark.
   //
-  // Each pair is tested once, by the pLS that comes first in the eta-sorted
-  // records of the pass.  Each block takes kPLSCleanTile consecutive records
-  // (one per thread) and streams, through shared memory, the later records
-  // that can lie within 0.1 in eta of any of them: up to kPLSBinReach bins
-  // above its last record's bin, plus the non-finite bin, which meets every
-  // pLS (a NaN never satisfies the reference's skip); a block holding a
-  // non-finite record streams to the end.  Each warp tests only the part of
-  // that stream its own records can reach.
+  // kPLSCleanHits finds every pair of the hit conditions: one thread per pLS
+  // ix walks the hit index for its hits (pass 1: hits 0 and 1, one of which
+  // is among jx's when three of the four are; pass 2: all four) and tests the
+  // higher-index pLS jx found there.  A pair met through several hits is
+  // tested again, which changes nothing.
+  __global__ void kPLSCleanHits(DeviceES es, const EventView* evs, bool secondpass) {
+    const EventView& ev = evs[blockIdx.y];
+    const Segments& s = ev.ls;
+    unsigned int nPix = s.nSegments[es.pixelModule];
+    if (nPix > kMaxPixelSegments)
+      nPix = kMaxPixelSegments;
+    const unsigned int maxSteps = 4 * nPix;  // a chain holds each entry once: no walk takes more
+    const uint4* hits = reinterpret_cast<const uint4*>(s.pLSHitsIdxs);
+    for (unsigned int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < nPix; ix += gridDim.x * blockDim.x) {
+      if (!plsCleanEligible(s, ix, secondpass))
+        continue;
+      const uint4 h1 = hits[ix];
+      const unsigned int h1a[4] = {h1.x, h1.y, h1.z, h1.w};
+      const float eta1 = s.eta[ix];
+      const int nSlots = secondpass ? 4 : 2;
+      for (int slot = 0; slot < nSlots; ++slot) {
+        const unsigned int h = h1a[slot];
+        unsigned int steps = 0;
+        for (unsigned int e = ev.plsHitHead[plsHitBucket(h)]; e != kPLSHitNone; e = ev.plsHitNext[e]) {
+          if (++steps > maxSteps) {
+            atomicOr(&ev.sc->status, kStatusInvalidInput);
+            break;
+          }
+          const unsigned int jx = e >> 2;
+          if (jx <= ix || jx >= nPix || s.pLSHitsIdxs[e] != h)
+            continue;
+          if (fabs_(s.eta[jx] - eta1) > 0.1f)
+            continue;
+          if (!plsCleanEligible(s, jx, secondpass))
+            continue;
+          bool remove = true;  // pass 2: a hit in common
+          if (!secondpass) {
+            const uint4 h2 = hits[jx];
+            int npMatched = 0;
+            for (int k = 0; k < 4; k++)
+              if (h1a[k] == h2.x || h1a[k] == h2.y || h1a[k] == h2.z || h1a[k] == h2.w)
+                npMatched++;
+            remove = npMatched >= 3;
+          }
+          if (remove)
+            plsRemoveOf(ev, ix, jx, secondpass);
+        }
+      }
+    }
+  }
+
+  // One pass-2 pLS as kPLSCleanNear reads it, stored in eta-bin order so that
+  // a tile of candidates is one coalesced read.
+  struct __align__(16) PLSRec {
+    float eta, phi;
+    unsigned int index, pad;
+  };
+
+  // Counting sort, by eta bin, of the pLS that pass 2 tests (the quads
+  // without a pass-1 mark), one block per event; writes the bin starts (the
+  // last entry being the number of records) and the sorted records.
+  __global__ void __launch_bounds__(1024) kPLSBin(DeviceES es, const EventView* evs) {
+    __shared__ unsigned int sCount[kPLSBins + 1];
+    __shared__ unsigned int sCursor[kPLSBins + 1];
+    const EventView& ev = evs[blockIdx.y];
+    const Segments& s = ev.ls;
+    unsigned int nPix = s.nSegments[es.pixelModule];
+    if (nPix > kMaxPixelSegments)
+      nPix = kMaxPixelSegments;
+    for (int b = threadIdx.x; b <= kPLSBins; b += blockDim.x)
+      sCount[b] = 0;
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x)
+      if (plsCleanEligible(s, i, true))
+        atomicAdd(&sCount[plsEtaBin(s.eta[i])], 1u);
+    __syncthreads();
+    unsigned int c = threadIdx.x <= kPLSBins ? sCount[threadIdx.x] : 0u;
+    unsigned int tot;
+    unsigned int ex = blockExclusiveScan(c, tot);
+    if (threadIdx.x <= kPLSBins) {
+      sCursor[threadIdx.x] = ex;
+      ev.plsBinStart[threadIdx.x] = ex;
+    }
+    if (threadIdx.x == 0)
+      ev.plsBinStart[kPLSBins + 1] = tot;
+    __syncthreads();
+    for (unsigned int i = threadIdx.x; i < nPix; i += blockDim.x) {
+      if (!plsCleanEligible(s, i, true))
+        continue;
+      PLSRec r;
+      r.eta = s.eta[i];
+      r.phi = s.phi[i];
+      r.index = i;
+      r.pad = 0;
+      ev.plsRec[atomicAdd(&sCursor[plsEtaBin(r.eta)], 1u)] = r;
+    }
+  }
+
+  // kPLSCleanNear finds the pass-2 pairs of the dR2 condition.  dR2 < 1e-5
+  // needs |deta| < 0.0032, so both lie in the same or adjacent eta bins, and
+  // a NaN or infinite eta never passes (the non-finite bin is left out).  Each
+  // pair is tested once, by the record that comes first in the eta-sorted
+  // order: each block takes kPLSCleanTile consecutive finite records (one per
+  // thread) and streams, through shared memory, the later records up to one
+  // bin above its last record's bin; each warp tests only the part its own
+  // records can reach.  dEta and dPhi are taken with the lower index first,
+  // as in the reference.
   constexpr int kPLSCleanTile = 128;
 
-  __global__ void __launch_bounds__(kPLSCleanTile) kPLSClean(DeviceES es, const EventView* evs, bool secondpass) {
+  __global__ void __launch_bounds__(kPLSCleanTile) kPLSCleanNear(DeviceES es, const EventView* evs) {
     __shared__ PLSRec sT[kPLSCleanTile];
     const EventView& ev = evs[blockIdx.y];
     const PLSRec* rec = ev.plsRec;
     const unsigned int* binStart = ev.plsBinStart;
     const unsigned int nFinite = binStart[kPLSBins];
-    const unsigned int nRec = binStart[kPLSBins + 1];
     const unsigned int warp = threadIdx.x >> 5;
-    for (unsigned int k0 = blockIdx.x * kPLSCleanTile; k0 < nRec; k0 += gridDim.x * kPLSCleanTile) {
+    for (unsigned int k0 = blockIdx.x * kPLSCleanTile; k0 < nFinite; k0 += gridDim.x * kPLSCleanTile) {
       const unsigned int k = k0 + threadIdx.x;
-      const bool active = k < nRec;
+      const bool active = k < nFinite;
       PLSRec me{};
       if (active)
         me = rec[k];
-      // The block's stream of sorted positions, as offsets t: [0, lenA) are
-      // positions k0 + t, [lenA, span) are positions lo2 + (t - lenA).
-      const unsigned int kLast = min(k0 + kPLSCleanTile, nRec) - 1;
-      const bool finiteBlock = kLast < nFinite;
-      unsigned int hiB = nRec, lo2 = nRec;
-      if (finiteBlock) {
-        hiB = binStart[min(plsEtaBin(rec[kLast].eta) + kPLSBinReach, kPLSBins - 1) + 1];
-        lo2 = nFinite;
-      }
-      const unsigned int lenA = hiB - k0;
-      const unsigned int span = lenA + (nRec - lo2);
-      // This warp's part of the stream: [tW0, tW1) and [tW2, span).
+      const unsigned int kLast = min(k0 + kPLSCleanTile, nFinite) - 1;
+      const unsigned int span = binStart[min(plsEtaBin(rec[kLast].eta) + 1, kPLSBins - 1) + 1] - k0;
+      // this warp's part of the stream: offsets [tW0, tW1)
       const unsigned int kW0 = k0 + warp * 32;
       const unsigned int tW0 = warp * 32;
-      unsigned int tW1 = lenA, tW2 = lenA;
-      if (kW0 < nRec) {
-        const unsigned int kW1 = min(kW0 + 32, nRec) - 1;
-        if (kW1 < nFinite) {
-          tW1 = binStart[min(plsEtaBin(rec[kW1].eta) + kPLSBinReach, kPLSBins - 1) + 1] - k0;
-          tW2 = finiteBlock ? lenA : nFinite - k0;
-        }
+      unsigned int tW1 = 0;
+      if (kW0 < nFinite) {
+        const unsigned int kW1 = min(kW0 + 32, nFinite) - 1;
+        tW1 = binStart[min(plsEtaBin(rec[kW1].eta) + 1, kPLSBins - 1) + 1] - k0;
       }
       for (unsigned int t0 = 0; t0 < span; t0 += kPLSCleanTile) {
         __syncthreads();
         const unsigned int t = t0 + threadIdx.x;
         if (t < span)
-          sT[threadIdx.x] = rec[t < lenA ? k0 + t : lo2 + (t - lenA)];
+          sT[threadIdx.x] = rec[k0 + t];
         __syncthreads();
         if (!active)
           continue;
         const unsigned int nt = min(span - t0, unsigned(kPLSCleanTile));
-        const unsigned int uEnd1 = tW1 > t0 ? min(tW1 - t0, nt) : 0u;
-        for (unsigned int u = tW0 > t0 ? tW0 - t0 : 0u; u < uEnd1; ++u)
-          if (t0 + u > threadIdx.x)
-            plsCleanPair(ev, me, sT[u], secondpass);
-        for (unsigned int u = tW2 > t0 ? min(tW2 - t0, nt) : 0u; u < nt; ++u)
-          plsCleanPair(ev, me, sT[u], secondpass);
+        const unsigned int uEnd = tW1 > t0 ? min(tW1 - t0, nt) : 0u;
+        for (unsigned int u = tW0 > t0 ? tW0 - t0 : 0u; u < uEnd; ++u) {
+          if (t0 + u <= threadIdx.x)
+            continue;
+          const PLSRec o = sT[u];
+          const bool meLow = me.index < o.index;
+          const float eta1 = meLow ? me.eta : o.eta, eta2 = meLow ? o.eta : me.eta;
+          const float phi1 = meLow ? me.phi : o.phi, phi2 = meLow ? o.phi : me.phi;
+          const float dEta = fabs_(eta1 - eta2);
+          const float dPhi = wrapDPhi(phi1, phi2);
+          const float dR2 = dEta * dEta + dPhi * dPhi;
+          if (dR2 < 1e-5f)
+            plsRemoveOf(ev, meLow ? me.index : o.index, meLow ? o.index : me.index, true);
+        }
       }
     }
   }
