@@ -244,10 +244,16 @@ namespace lst {
     MDValues zero{0, 0, 0, 0, 0, 0, 0, 0, 0};
     storeMD(m, h, md, hit0, hit1, pixelModule, zero, innerMD);
     storeMD(m, h, md, hit2, hit3, pixelModule, zero, outerMD);
+    // The anchor and outer hits storeMD has just stored (its rule), so that
+    // the values below are read from the hits directly rather than back
+    // through the stored mini-doublets.
+    const bool swap = m.moduleType[pixelModule] == PS and m.moduleLayerType[pixelModule] == Strip;
+    const unsigned int inAnchor = swap ? hit1 : hit0, inOuter = swap ? hit0 : hit1;
+    const unsigned int outAnchor = swap ? hit3 : hit2, outOuter = swap ? hit2 : hit3;
 
-    float slope = fsinh(h.ys[md.outerHitIndices[innerMD]]);
-    float intercept = h.zs[md.anchorHitIndices[innerMD]] - slope * h.rts[md.anchorHitIndices[innerMD]];
-    float score_lsq = (h.rts[md.anchorHitIndices[outerMD]] * slope + intercept) - (h.zs[md.anchorHitIndices[outerMD]]);
+    float slope = fsinh(h.ys[inOuter]);
+    float intercept = h.zs[inAnchor] - slope * h.rts[inAnchor];
+    float score_lsq = (h.rts[outAnchor] * slope + intercept) - (h.zs[outAnchor]);
     score_lsq = score_lsq * score_lsq;
 
     s.mdIndices[pls * 2] = innerMD;
@@ -259,22 +265,22 @@ namespace lst {
     s.dPhiChanges[pls] = dPhiChange;
     s.isDup[tid] = 0;
     s.score[tid] = score_lsq;
-    s.pLSHitsIdxs[4 * tid + 0] = h.idxs[md.anchorHitIndices[innerMD]];
-    s.pLSHitsIdxs[4 * tid + 1] = h.idxs[md.anchorHitIndices[outerMD]];
-    s.pLSHitsIdxs[4 * tid + 2] = h.idxs[md.outerHitIndices[innerMD]];
-    s.pLSHitsIdxs[4 * tid + 3] = h.idxs[md.outerHitIndices[outerMD]];
+    s.pLSHitsIdxs[4 * tid + 0] = h.idxs[inAnchor];
+    s.pLSHitsIdxs[4 * tid + 1] = h.idxs[outAnchor];
+    s.pLSHitsIdxs[4 * tid + 2] = h.idxs[inOuter];
+    s.pLSHitsIdxs[4 * tid + 3] = h.idxs[outOuter];
 
-    float circleRadius = md.outerX[innerMD] / (2 * k2Rinv1GeVf);
-    float circlePhi = md.outerZ[innerMD];
-    float candidateCenterXs[2] = {md.anchorX[innerMD] + circleRadius * fsin(circlePhi),
-                                  md.anchorX[innerMD] - circleRadius * fsin(circlePhi)};
-    float candidateCenterYs[2] = {md.anchorY[innerMD] - circleRadius * fcos(circlePhi),
-                                  md.anchorY[innerMD] + circleRadius * fcos(circlePhi)};
+    float circleRadius = h.xs[inOuter] / (2 * k2Rinv1GeVf);
+    float circlePhi = h.zs[inOuter];
+    const float inAnchorX = h.xs[inAnchor], inAnchorY = h.ys[inAnchor];
+    const float outAnchorX = h.xs[outAnchor], outAnchorY = h.ys[outAnchor];
+    float candidateCenterXs[2] = {inAnchorX + circleRadius * fsin(circlePhi), inAnchorX - circleRadius * fsin(circlePhi)};
+    float candidateCenterYs[2] = {inAnchorY - circleRadius * fcos(circlePhi), inAnchorY + circleRadius * fcos(circlePhi)};
     float bestChiSquared = kInf;
     int bestIndex = 0;
     for (int i = 0; i < 2; i++) {
-      float chiSquared = fabs_(fsqrt((md.anchorX[outerMD] - candidateCenterXs[i]) * (md.anchorX[outerMD] - candidateCenterXs[i]) +
-                                     (md.anchorY[outerMD] - candidateCenterYs[i]) * (md.anchorY[outerMD] - candidateCenterYs[i])) -
+      float chiSquared = fabs_(fsqrt((outAnchorX - candidateCenterXs[i]) * (outAnchorX - candidateCenterXs[i]) +
+                                     (outAnchorY - candidateCenterYs[i]) * (outAnchorY - candidateCenterYs[i])) -
                                circleRadius);
       if (chiSquared < bestChiSquared) {
         bestChiSquared = chiSquared;
