@@ -290,7 +290,9 @@ namespace lst {
 
   // ========================================================= pixel segments
   // SDL/Segment.h:1031-1117
-  __global__ void kPixelIngest(DeviceES es, const EventView* evs) {
+  // Register budget: four 256-thread blocks per SM (at 154 registers a thread
+  // only one fitted, and the kernel waits on gathers).
+  __global__ void __launch_bounds__(256, 4) kPixelIngest(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nPLS = ev.sc->nPLS;
     const uint16_t pix = es.pixelModule;
