@@ -186,7 +186,7 @@ namespace lst {
 
   // ================================================================ hits
   // SDL/Hit.h:217-269
-  __global__ void kHitPrep(DeviceES es, const EventView* evs) {
+  __global__ void __launch_bounds__(256, 4) kHitPrep(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int nHits = ev.sc->nHits;
     const Modules& m = es.m;
@@ -3495,12 +3495,36 @@ namespace lst {
     const PackedLayout L = packedLayout(reject ? 0u : nHits, reject ? 0u : nPLSIn);
     const unsigned int stride = gridDim.x * blockDim.x;
     const unsigned int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-    for (unsigned int i = t0; i < nHits; i += stride) {
-      ev.hits.xs[i] = reinterpret_cast<const float*>(b + L.x)[i];
-      ev.hits.ys[i] = reinterpret_cast<const float*>(b + L.y)[i];
-      ev.hits.zs[i] = reinterpret_cast<const float*>(b + L.z)[i];
-      ev.hits.detid[i] = reinterpret_cast<const unsigned int*>(b + L.detId)[i];
-      ev.hits.idxs[i] = reinterpret_cast<const unsigned int*>(b + L.idx)[i];
+    // Two hits per thread and step: ten loads in flight before the stores.
+    for (unsigned int i = t0; i < nHits; i += 2 * stride) {
+      const unsigned int j = i + stride;
+      const bool two = j < nHits;
+      const float x0 = reinterpret_cast<const float*>(b + L.x)[i];
+      const float y0 = reinterpret_cast<const float*>(b + L.y)[i];
+      const float z0 = reinterpret_cast<const float*>(b + L.z)[i];
+      const unsigned int d0 = reinterpret_cast<const unsigned int*>(b + L.detId)[i];
+      const unsigned int n0 = reinterpret_cast<const unsigned int*>(b + L.idx)[i];
+      float x1 = 0.f, y1 = 0.f, z1 = 0.f;
+      unsigned int d1 = 0, n1 = 0;
+      if (two) {
+        x1 = reinterpret_cast<const float*>(b + L.x)[j];
+        y1 = reinterpret_cast<const float*>(b + L.y)[j];
+        z1 = reinterpret_cast<const float*>(b + L.z)[j];
+        d1 = reinterpret_cast<const unsigned int*>(b + L.detId)[j];
+        n1 = reinterpret_cast<const unsigned int*>(b + L.idx)[j];
+      }
+      ev.hits.xs[i] = x0;
+      ev.hits.ys[i] = y0;
+      ev.hits.zs[i] = z0;
+      ev.hits.detid[i] = d0;
+      ev.hits.idxs[i] = n0;
+      if (two) {
+        ev.hits.xs[j] = x1;
+        ev.hits.ys[j] = y1;
+        ev.hits.zs[j] = z1;
+        ev.hits.detid[j] = d1;
+        ev.hits.idxs[j] = n1;
+      }
     }
     for (unsigned int i = t0; i < nPLS; i += stride) {
       ev.plsHit0[i] = reinterpret_cast<const unsigned int*>(b + L.h0)[i];
