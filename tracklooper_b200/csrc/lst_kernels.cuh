@@ -813,29 +813,25 @@ namespace lst {
 
   // ============================================================ triplets
   // Per-module triplet offsets (SDL/Triplet.h:1007-1102); one block per event.
-  // Each thread takes a contiguous range of modules, so that one block scan
-  // of the per-thread sums gives every module its offset.
   __global__ void __launch_bounds__(1024) kT3Offsets(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
-    const unsigned int n = es.nLowerModules;
-    const unsigned int per = (n + blockDim.x - 1) / blockDim.x;
-    const unsigned int i0 = min(threadIdx.x * per, n), i1 = min(i0 + per, n);
-    auto occOf = [&](unsigned int i) {
-      return ev.ls.nSegments[i] != 0 ? static_cast<unsigned int>(es.t3CapIfUsed[i]) : 0u;
-    };
-    unsigned int mine = 0;
-    for (unsigned int i = i0; i < i1; ++i)
-      mine += occOf(i);
-    unsigned int tot;
-    unsigned int run = blockExclusiveScan(mine, tot);
-    for (unsigned int i = i0; i < i1; ++i) {
-      const unsigned int occ = occOf(i);
-      ev.rg.tripletModuleIndices[i] = static_cast<int>(run);
-      ev.rg.tripletModuleOccupancy[i] = static_cast<int>(occ);
-      run += occ;
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < es.nLowerModules; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      unsigned int occ = 0;
+      bool valid = i < es.nLowerModules;
+      if (valid && ev.ls.nSegments[i] != 0)
+        occ = static_cast<unsigned int>(es.t3CapIfUsed[i]);
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(occ, tot);
+      if (valid) {
+        ev.rg.tripletModuleIndices[i] = static_cast<int>(carry + ex);
+        ev.rg.tripletModuleOccupancy[i] = static_cast<int>(occ);
+      }
+      carry += tot;
     }
     if (threadIdx.x == 0)
-      *ev.rg.device_nTotalTrips = tot;
+      *ev.rg.device_nTotalTrips = carry;
   }
 
   // One warp per inner-inner lower module walking (inner segment, outer
@@ -922,7 +918,8 @@ namespace lst {
 
   // ========================================================= quintuplets
   // Eligible T5 seed modules and their offsets (SDL/Quintuplet.h:3117-3213).
-  // Contiguous module ranges per thread, as in kT3Offsets.
+  // Each thread takes a contiguous range of modules, so that one block scan
+  // of the per-thread sums gives every eligible module its place.
   __global__ void __launch_bounds__(1024) kT5Eligible(DeviceES es, const EventView* evs) {
     const EventView& ev = evs[blockIdx.y];
     const unsigned int n = es.nLowerModules;
@@ -3299,19 +3296,14 @@ namespace lst {
     const unsigned int nT5TC = *ev.tc.nTrackCandidatesT5;
     TrackCandidates tc = ev.tc;
     const Segments& s = ev.ls;
-    // Each thread takes a contiguous range of pLS, so that one block scan of
-    // the per-thread counts gives every accepted pLS its place in pLS order.
-    const unsigned int per = (n + blockDim.x - 1) / blockDim.x;
-    const unsigned int i0 = min(threadIdx.x * per, n), i1 = min(i0 + per, n);
-    unsigned int mine = 0;
-    for (unsigned int i = i0; i < i1; ++i)
-      mine += (s.isQuad[i] && !s.isDup[i]) ? 1u : 0u;
-    unsigned int carry;
-    unsigned int idx = start + blockExclusiveScan(mine, carry);
-    for (unsigned int i = i0; i < i1; ++i) {
-      if (!(s.isQuad[i] && !s.isDup[i]))
-        continue;
-      if (idx - nT5TC < kMaxPixelTrackCandidates) {
+    unsigned int carry = 0;
+    for (unsigned int base = 0; base < n; base += blockDim.x) {
+      unsigned int i = base + threadIdx.x;
+      bool f = i < n && s.isQuad[i] && !s.isDup[i];
+      unsigned int tot;
+      unsigned int ex = blockExclusiveScan(f ? 1u : 0u, tot);
+      unsigned int idx = start + carry + ex;
+      if (f && idx - nT5TC < kMaxPixelTrackCandidates) {
         tc.trackCandidateType[idx] = 8;
         tc.directObjectIndices[idx] = i;
         tc.pixelSeedIndex[idx] = static_cast<int>(s.seedIdx[i]);
@@ -3331,7 +3323,7 @@ namespace lst {
         tc.centerY[idx] = 0;
         tc.radius[idx] = 0;
       }
-      ++idx;
+      carry += tot;
     }
     if (threadIdx.x == 0) {
       unsigned int room = (start - nT5TC < kMaxPixelTrackCandidates) ? kMaxPixelTrackCandidates - (start - nT5TC) : 0u;
