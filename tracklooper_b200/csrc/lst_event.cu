@@ -533,7 +533,7 @@ namespace {
         LST_LAUNCH(lst::kAddPT3TC, one, 1024, d, v);
         LST_LAUNCH(lst::kT5Bin, one, 1024, d, v);
         LST_LAUNCH(lst::kT5DedupBinned, dim3(blocksFor(4096, count), count), kThreads, d, v);
-        LST_LAUNCH(lst::kT5DedupBeforeTC, eligGrid, 256, d, v);
+        LST_LAUNCH(lst::kT5DedupBeforeTC, dim3(blocksFor(nE * 32, count), count), 256, d, v);
         LST_LAUNCH(lst::kMergeT5Flag, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kCrossCleanT5, eligGrid, 256, d, v);
         LST_LAUNCH(lst::kT5TCCount, eligGrid, 256, d, v);

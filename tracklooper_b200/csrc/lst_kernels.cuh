@@ -2885,47 +2885,47 @@ namespace lst {
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5SortCount <= kT5SortCap && !ev.forceWalk)
       return;  // kT5DedupBinned has done this event
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    // A warp per eligible module, grid-stride (the grid is kept small: most
+    // events return above).
     const int nE = *ev.rg.nEligibleT5Modules;
-    if (warp >= nE)
-      return;
+    const int nWarps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
     const Quintuplets& q = ev.t5;
-    uint16_t lowmod1 = ev.rg.indicesOfEligibleT5Modules[warp];
-    unsigned int n1 = q.nQuintuplets[lowmod1];
-    if (n1 == 0)
-      return;
-    unsigned int base1 = ev.rg.quintupletModuleIndices[lowmod1];
-    for (unsigned int ix1 = laneId(); ix1 < n1; ix1 += 32) {
-      unsigned int ix = base1 + ix1;
-      if (q.partOfPT5[ix] || (q.isDup[ix] & 1))
-        continue;
-      float eta1 = q.eta[ix], phi1 = q.phi[ix], score1 = q.score_rphisum[ix];
-      for (int idx2 = warp; idx2 < nE; idx2++) {
-        uint16_t lowmod2 = ev.rg.indicesOfEligibleT5Modules[idx2];
-        unsigned int n2 = q.nQuintuplets[lowmod2];
-        unsigned int base2 = ev.rg.quintupletModuleIndices[lowmod2];
-        for (unsigned int jx1 = 0; jx1 < n2; jx1++) {
-          unsigned int jx = base2 + jx1;
-          if (ix == jx)
-            continue;
-          if (q.partOfPT5[jx] || (q.isDup[jx] & 1))
-            continue;
-          float eta2 = q.eta[jx], phi2 = q.phi[jx], score2 = q.score_rphisum[jx];
-          float dEta = fabs_(eta1 - eta2);
-          float dPhi = wrapDPhi(phi1, phi2);
-          if (dEta > 0.1f)
-            continue;
-          if (fabs_(dPhi) > 0.1f)
-            continue;
-          float dR2 = dEta * dEta + dPhi * dPhi;
-          int nMatched = sharedHitsT5(q, ix, jx);
-          if (dR2 < 0.001f || nMatched >= 5) {
-            if (score1 > score2)
-              ev.t5Flag[ix] = 1;
-            else if (score1 < score2)
-              ev.t5Flag[jx] = 1;
-            else
-              ev.t5Flag[ix < jx ? ix : jx] = 1;
+    for (int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); warp < nE; warp += nWarps) {
+      uint16_t lowmod1 = ev.rg.indicesOfEligibleT5Modules[warp];
+      unsigned int n1 = q.nQuintuplets[lowmod1];
+      unsigned int base1 = ev.rg.quintupletModuleIndices[lowmod1];
+      for (unsigned int ix1 = laneId(); ix1 < n1; ix1 += 32) {
+        unsigned int ix = base1 + ix1;
+        if (q.partOfPT5[ix] || (q.isDup[ix] & 1))
+          continue;
+        float eta1 = q.eta[ix], phi1 = q.phi[ix], score1 = q.score_rphisum[ix];
+        for (int idx2 = warp; idx2 < nE; idx2++) {
+          uint16_t lowmod2 = ev.rg.indicesOfEligibleT5Modules[idx2];
+          unsigned int n2 = q.nQuintuplets[lowmod2];
+          unsigned int base2 = ev.rg.quintupletModuleIndices[lowmod2];
+          for (unsigned int jx1 = 0; jx1 < n2; jx1++) {
+            unsigned int jx = base2 + jx1;
+            if (ix == jx)
+              continue;
+            if (q.partOfPT5[jx] || (q.isDup[jx] & 1))
+              continue;
+            float eta2 = q.eta[jx], phi2 = q.phi[jx], score2 = q.score_rphisum[jx];
+            float dEta = fabs_(eta1 - eta2);
+            float dPhi = wrapDPhi(phi1, phi2);
+            if (dEta > 0.1f)
+              continue;
+            if (fabs_(dPhi) > 0.1f)
+              continue;
+            float dR2 = dEta * dEta + dPhi * dPhi;
+            int nMatched = sharedHitsT5(q, ix, jx);
+            if (dR2 < 0.001f || nMatched >= 5) {
+              if (score1 > score2)
+                ev.t5Flag[ix] = 1;
+              else if (score1 < score2)
+                ev.t5Flag[jx] = 1;
+              else
+                ev.t5Flag[ix < jx ? ix : jx] = 1;
+            }
           }
         }
       }
