@@ -1,5 +1,5 @@
-"""Seeded synthetic event generator: reproducible, shaped like BASELINE's
-configurations."""
+"""Seeded synthetic event generator: reproducible, shaped like the workloads
+it stands in for (single-muon events, PU200 events, uneven pileup batches)."""
 import numpy as np
 import pytest
 
