@@ -1302,7 +1302,10 @@ namespace lst {
 
   // The warp-per-module walk, for events whose candidates overflow the flag
   // buffer (a no-op for the others).
-  __global__ void kT5Walk(DeviceES es, const EventView* evs, bool useDnn) {
+  // Register budget: this fallback does work only for events whose candidates
+  // overflow the lists; for the others its blocks return at once, and the
+  // budget lets more of them be resident, so the launch drains in fewer waves.
+  __global__ void __launch_bounds__(128, 8) kT5Walk(DeviceES es, const EventView* evs, bool useDnn) {
     __shared__ unsigned int sPre[kT5Warps][kT5MaxInner + 1];
     const EventView& ev = evs[blockIdx.y];
     if (!ev.sc->t5CandOverflow)
@@ -1406,7 +1409,10 @@ namespace lst {
     }
   }
 
-  __global__ void kT5Emit(DeviceES es, const EventView* evs, bool useDnn) {
+  // Register budget: this fallback does work only for events whose candidates
+  // overflow the lists; for the others its blocks return at once, and the
+  // budget lets more of them be resident, so the launch drains in fewer waves.
+  __global__ void __launch_bounds__(256, 4) kT5Emit(DeviceES es, const EventView* evs, bool useDnn) {
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow || (ev.sc->t5PassCount <= kT5RankCap && !ev.forceWalk))
       return;
@@ -1945,7 +1951,10 @@ namespace lst {
       ev.plsCount[iPLS] = count;
   }
 
-  __global__ void kPT5Count(DeviceES es, const EventView* evs) {
+  // Register budget: this fallback does work only for events whose candidates
+  // overflow the lists; for the others its blocks return at once, and the
+  // budget lets more of them be resident, so the launch drains in fewer waves.
+  __global__ void __launch_bounds__(128, 8) kPT5Count(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
@@ -1961,7 +1970,10 @@ namespace lst {
     }
   }
 
-  __global__ void kPT5Emit(DeviceES es, const EventView* evs) {
+  // Register budget: this fallback does work only for events whose candidates
+  // overflow the lists; for the others its blocks return at once, and the
+  // budget lets more of them be resident, so the launch drains in fewer waves.
+  __global__ void __launch_bounds__(128, 8) kPT5Emit(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
@@ -2271,7 +2283,10 @@ namespace lst {
       ev.plsCount[iPLS] = count;
   }
 
-  __global__ void kPT3Count(DeviceES es, const EventView* evs) {
+  // Register budget: this fallback does work only for events whose candidates
+  // overflow the lists; for the others its blocks return at once, and the
+  // budget lets more of them be resident, so the launch drains in fewer waves.
+  __global__ void __launch_bounds__(128, 8) kPT3Count(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
@@ -2287,7 +2302,10 @@ namespace lst {
     }
   }
 
-  __global__ void kPT3Emit(DeviceES es, const EventView* evs) {
+  // Register budget: this fallback does work only for events whose candidates
+  // overflow the lists; for the others its blocks return at once, and the
+  // budget lets more of them be resident, so the launch drains in fewer waves.
+  __global__ void __launch_bounds__(128, 8) kPT3Emit(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kPixWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sMods[kPixWarps][kMaxConnectedModules];
     const EventView& ev = evs[blockIdx.y];
