@@ -175,18 +175,24 @@ def hbm_peak():
 
 
 def committed_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled
-    to the bench workload there; None if no capture is committed."""
+    """(DRAM bytes per launch of `kernel`, how they were captured) from the
+    committed ncu summary (profiles/dram_traffic.txt: '# ' comment lines
+    saying how the capture was made, then '<kernel> <bytes>' lines);
+    (None, None) if no capture of that kernel is committed."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    note = []
     try:
         with open(path) as f:
             for line in f:
+                if line.startswith("#"):
+                    note.append(line[1:].strip())
+                    continue
                 parts = line.split()
                 if len(parts) >= 2 and parts[0] == kernel:
-                    return float(parts[1])
+                    return float(parts[1]), " ".join(note)
     except OSError:
         pass
-    return None
+    return None, None
 
 
 # --------------------------------------------------------------------- ours
@@ -396,7 +402,8 @@ def run_ours(args, rank, world, local, events):
         "peak_kind": f"{peak_kind} (copy bandwidth)",
         "unit": "GB/s",
         "frac": round(achieved / peak, 5) if achieved else None,
-        "traffic": committed_traffic(dominant),
+        "traffic": committed_traffic(dominant)[0],
+        "traffic_source": committed_traffic(dominant)[1],
         "algorithmic_bytes_per_launch": algo,
         "launch_ms": round(dms / dlaunches, 4),
         "share_of_device_time": round(dms / tot, 4) if tot else None,
@@ -478,6 +485,22 @@ def run_reference_cpu(events, threads: int, min_events: int, budget_s: float = 0
     return done[0] / dt, done[0], threads, dt
 
 
+def reference_cpu_baseline(events, ncpu: int, min_events: int, budget_s: float = 12.0) -> dict:
+    """The reference CPU backend on this host: all usable cores, then one
+    thread, each a sustained sample of at least budget_s seconds (threads keep
+    taking the next event until both the event count and the time are
+    reached, so only the last wave of the whole sample has a tail)."""
+    threads = cpu_threads(ncpu)
+    r_all, n_all, th, dt_all = run_reference_cpu(events, threads, max(min_events, threads), budget_s=budget_s)
+    r_one, n_one, _, dt_one = run_reference_cpu(events, 1, 1, budget_s=budget_s)
+    return {"value": r_all, "unit": "events/s", "cores": th, "kind": "reference",
+            "sample": f"{n_all} events of this batch (cycled), one event per thread on {th} threads, "
+                      f"{dt_all:.1f} s wall, liblstref_fast.so (reference compiler flags)",
+            "one_thread": {"value": r_one, "unit": "events/s", "cores": 1,
+                           "sample": f"{n_one} events, {dt_one:.1f} s wall"},
+            "host_cpus": ncpu}
+
+
 def cpu_threads(ncpu: int) -> int:
     """Host threads for the reference CPU backend: all cores, bounded by memory
     (each in-flight reference event holds ~0.6 GB of object arenas)."""
@@ -492,7 +515,24 @@ def cpu_threads(ncpu: int) -> int:
     return ncpu
 
 
-def main():
+def launcher_command(argv, n_gpus: int, port: int) -> list:
+    """The command that runs this script as n_gpus local ranks (one process
+    per GPU), as the torchrun launch of a multi-GPU bench does."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n_gpus}",
+            "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
+def _free_port() -> int:
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
@@ -501,10 +541,25 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--cpu-events", type=int, default=0, help="reference CPU sample size (0: 2 per thread)")
-    args = ap.parse_args()
+    args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
+    return args
+
+
+def main(argv=None, runner=None, backend: str = "nccl"):
+    """Runs the bench; `runner(args, rank, world, local, events)` replaces the
+    GPU replica (run_ours) and `backend` the process-group backend, which is
+    how the CPU tests drive the multi-rank harness with gloo."""
+    argv = sys.argv[1:] if argv is None else list(argv)
+    args = parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch as args.gpus local ranks
+        rc = subprocess.call(launcher_command(argv, args.gpus, _free_port()))
+        sys.exit(rc)
     rank, world, local = dist_env()
+    if world != args.gpus and rank == 0:
+        log(f"note: --gpus {args.gpus} but WORLD_SIZE={world}; running {world} ranks")
     ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
 
     config = {"workload": f"PU200-shaped events (generator configuration {args.config}), batch of {args.batch} per GPU",
@@ -519,20 +574,20 @@ def main():
             return
         events = generate(args.config, 0, args.batch, ncpu)
         threads = cpu_threads(ncpu)
-        n = args.cpu_events or 2 * threads
-        for _ in range(min(1, args.warmup)):
-            run_reference_cpu(events, threads, threads)
-        rates = []
-        t_all = 0.0
-        for _ in range(args.steps):
-            r, ne, th, dt = run_reference_cpu(events, threads, n)
-            rates.append(r)
-            t_all += dt
-        value = statistics.mean(rates)
+        # warm-up: one event per thread (page-in, allocator)
+        run_reference_cpu(events, threads, threads)
+        # one sustained sample covering all steps' events (steps x batch), at
+        # least 12 s, with threads taking the next event as they finish: no
+        # per-step wave tail
+        n_events = args.cpu_events or args.steps * args.batch
+        cpu = reference_cpu_baseline(events, ncpu, n_events, budget_s=12.0)
+        value = cpu["value"]
         line = dict(base)
-        line.update({"impl": "reference", "value": value, "ms_per_step": 1e3 * t_all / args.steps,
-                     "cpu_baseline": {"value": value, "unit": "events/s", "cores": threads, "kind": "reference",
-                                      "sample": f"{n} events per step, one event per thread, liblstref_fast.so"},
+        line["config"] = dict(config, events_per_step=args.batch,
+                              reference_sample=f"{args.steps} steps of {args.batch} events, timed as one sustained "
+                                               f"sample; a step is {args.batch} events")
+        line.update({"impl": "reference", "value": value, "ms_per_step": 1e3 * args.batch / value,
+                     "cpu_baseline": cpu,
                      "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         print(json.dumps(line), flush=True)
         return
@@ -541,18 +596,14 @@ def main():
         import torch.distributed as tdist
         import datetime
 
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     events = generate(args.config, rank_first_event(rank, args.batch), args.batch, ncpu)
-    res = run_ours(args, rank, world, local, events)
+    res = (runner or run_ours)(args, rank, world, local, events)
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and runner is None:
         try:
-            threads = cpu_threads(ncpu)
-            r, ne, th, dt = run_reference_cpu(events, threads, args.cpu_events or 2 * threads, budget_s=12.0)
-            cpu = {"value": r, "unit": "events/s", "cores": th, "kind": "reference",
-                   "sample": f"{ne} events of this batch (cycled), one event per thread, {dt:.1f} s wall, "
-                             f"liblstref_fast.so"}
+            cpu = reference_cpu_baseline(events, ncpu, args.cpu_events or 2 * cpu_threads(ncpu), budget_s=12.0)
         except Exception as e:  # the CPU baseline is reported, not required
             cpu = {"value": None, "unit": "events/s", "cores": ncpu, "kind": "reference", "sample": f"failed: {e}"}
 

@@ -353,7 +353,10 @@ int lst_run(lst_event* ev, int slot, const lst_seed_input* in, lst_output* out);
  * events per call) and rejects a call whose output does not fit (or of more
  * than 1023 events) with an error naming the size: split the slot range.  The
  * first call on each device looks the array up (cudaGetSymbolAddress with
- * that device current); make that first call before any stream capture.  All
+ * that device current); make that first call before any stream capture.  The
+ * looked-up address is kept while an event setup (lst_es) is alive on the
+ * device and forgotten when the last one is freed; a cudaDeviceReset while one
+ * is alive invalidates it together with its event sets.  All
  * event sets of a device share the array, so calls that overlap in time (on
  * different streams or host threads) race: serialise them. */
 int lst_batch_get_output_static(lst_event* ev, int first, int count, lst_output* out);

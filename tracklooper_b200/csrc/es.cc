@@ -41,14 +41,23 @@ namespace lst {
 #pragma pack(pop)
 
     // {u32 key, u32 n, n x u32} records; a later record with the same key
-    // replaces an earlier one; a truncated trailing record is ignored.
+    // replaces an earlier one; a truncated trailing record is ignored, as
+    // SDL/ModuleConnectionMap.cc:17-48 drops it at end of file.  A record
+    // whose n exceeds what is left of the file is such a record: it is
+    // dropped before anything is allocated for it, so a corrupt count cannot
+    // ask for gigabytes.
     bool readConnectionMap(const std::string& path, std::map<uint32_t, std::vector<uint32_t>>& out) {
-      std::ifstream f(path, std::ios::binary);
+      std::ifstream f(path, std::ios::binary | std::ios::ate);
       if (!f.is_open())
         return false;
+      const std::streamoff fileSize = f.tellg();
+      f.seekg(0);
       while (true) {
         uint32_t key, n;
         if (!f.read(reinterpret_cast<char*>(&key), 4) || !f.read(reinterpret_cast<char*>(&n), 4))
+          break;
+        const std::streamoff left = fileSize - std::streamoff(f.tellg());
+        if (std::streamoff(n) > left / 4)
           break;
         std::vector<uint32_t> v(n);
         if (n && !f.read(reinterpret_cast<char*>(v.data()), std::streamsize(n) * 4))

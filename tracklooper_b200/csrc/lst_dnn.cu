@@ -150,6 +150,19 @@ namespace {
 
 }  // namespace
 
+// No C++ exception crosses the C ABI (see lst_event.cu): host-side failures
+// become a -1 status with a message.
+#define LST_ABI_TRY try {
+#define LST_ABI_CATCH_INT        \
+  }                              \
+  catch (...) {                  \
+    try {                        \
+      g_dnnError = "host error"; \
+    } catch (...) {              \
+    }                            \
+    return -1;                   \
+  }
+
 extern "C" {
 
 size_t lst_t5dnn_scratch_floats(int n) {
@@ -158,6 +171,7 @@ size_t lst_t5dnn_scratch_floats(int n) {
 }
 
 int lst_t5dnn_forward(const float* weights, const float* x, int n, float* h1, float* h2, float* logit, void* stream) {
+  LST_ABI_TRY
   if (n <= 0)
     return 0;
   if (!weights || !x || !h1 || !h2 || !logit)
@@ -168,10 +182,12 @@ int lst_t5dnn_forward(const float* weights, const float* x, int n, float* h1, fl
   if (cudaPeekAtLastError() != cudaSuccess)
     return dnnFail("kDnnForward");
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_t5dnn_backward(const float* weights, const float* x, const float* h1, const float* h2, const float* dlogit,
                        int n, float* grad, float* scratch, void* stream) {
+  LST_ABI_TRY
   if (!weights || !x || !h1 || !h2 || !dlogit || !grad || !scratch)
     return -1;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -195,6 +211,7 @@ int lst_t5dnn_backward(const float* weights, const float* x, const float* h1, co
   if (cudaPeekAtLastError() != cudaSuccess)
     return dnnFail("kDnnGradReduce");
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 const char* lst_t5dnn_last_error(void) { return g_dnnError.c_str(); }

@@ -31,8 +31,46 @@ namespace {
   thread_local std::string g_lastError;
 
   int setError(const std::string& msg) {
-    g_lastError = msg;
+    try {
+      g_lastError = msg;
+    } catch (...) {
+    }
     return -1;
+  }
+
+  // Records "<prefix><what>" without letting an allocation failure escape.
+  int abiFail(const char* prefix, const char* what) noexcept {
+    try {
+      g_lastError = std::string(prefix) + what;
+    } catch (...) {
+    }
+    return -1;
+  }
+
+  // Live event setups per device; the cached device address of the static
+  // output staging (lst_batch_get_output_static) is dropped when the last
+  // one on a device is freed.  Defined with that staging below.
+  void staticOutputDeviceRetain(int device);
+  void staticOutputDeviceRelease(int device);
+
+  // No C++ exception crosses the C ABI: every entry point runs its body
+  // between LST_ABI_TRY and LST_ABI_CATCH_INT (or _VOID), which turn a host
+  // allocation failure or any other exception into a -1 status and a message.
+#define LST_ABI_TRY try {
+#define LST_ABI_CATCH_INT                          \
+  }                                                \
+  catch (const std::bad_alloc&) {                  \
+    return abiFail("out of host memory", "");      \
+  }                                                \
+  catch (const std::exception& e_) {               \
+    return abiFail("internal error: ", e_.what()); \
+  }                                                \
+  catch (...) {                                    \
+    return abiFail("internal error", "");          \
+  }
+#define LST_ABI_CATCH_VOID \
+  }                        \
+  catch (...) {            \
   }
 
   int cudaFail(cudaError_t e, const char* what) {
@@ -689,10 +727,15 @@ extern "C" {
 
 const char* lst_last_error(void) { return g_lastError.c_str(); }
 
-int lst_kernel_count(void) { return static_cast<int>(kernelTable().size()); }
+int lst_kernel_count(void) {
+  LST_ABI_TRY
+  return static_cast<int>(kernelTable().size());
+  LST_ABI_CATCH_INT
+}
 
 int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_threads_per_block, size_t* local_bytes,
                           size_t* static_smem_bytes) {
+  LST_ABI_TRY
   const auto& t = kernelTable();
   if (i < 0 || i >= static_cast<int>(t.size()))
     return setError("kernel index out of range");
@@ -709,9 +752,11 @@ int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_thre
   if (static_smem_bytes)
     *static_smem_bytes = a.sharedSizeBytes;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out) {
+  LST_ABI_TRY
   if (!geometry_dir || !out)
     return setError("lst_es_load: null argument");
   *out = nullptr;
@@ -725,6 +770,12 @@ int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int de
   for (int v : es->host.t5CapIfEligible)
     if (v >= 0)
       es->nEligibleMax++;
+  // Every input file is read and checked before the first CUDA call.
+  if (t5dnn_weights_path) {
+    int rc = loadWeightsFile(t5dnn_weights_path, es->dnn);
+    if (rc)
+      return rc;
+  }
   LST_CUDA(cudaSetDevice(device));
   std::vector<std::pair<void*, const void*>> copies;
   std::vector<size_t> sizes;
@@ -738,22 +789,20 @@ int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int de
   for (size_t i = 0; i < copies.size(); ++i)
     LST_CUDA(cudaMemcpy(copies[i].first, copies[i].second, sizes[i], cudaMemcpyHostToDevice));
   if (t5dnn_weights_path) {
-    int rc = loadWeightsFile(t5dnn_weights_path, es->dnn);
-    if (rc) {
-      cudaFree(es->arena);
-      return rc;
-    }
-    rc = uploadWeights(es.get());
+    int rc = uploadWeights(es.get());
     if (rc) {
       cudaFree(es->arena);
       return rc;
     }
   }
+  staticOutputDeviceRetain(device);
   *out = es.release();
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_es_load_host(const char* geometry_dir, lst_es** out) {
+  LST_ABI_TRY
   if (!geometry_dir || !out)
     return setError("lst_es_load_host: null argument");
   *out = nullptr;
@@ -766,9 +815,11 @@ int lst_es_load_host(const char* geometry_dir, lst_es** out) {
     return setError(err);
   *out = es.release();
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_es_host_array(const lst_es* es, const char* name, const void** data, size_t* n_elems, size_t* elem_size) {
+  LST_ABI_TRY
   if (!es || !name || !data)
     return setError("lst_es_host_array: null argument");
   const lst::EsHost& h = es->host;
@@ -821,19 +872,24 @@ int lst_es_host_array(const lst_es* es, const char* name, const void** data, siz
   LST_ES_ARRAY("caps.", t5CapIfEligible)
 #undef LST_ES_ARRAY
   return setError("unknown event-setup array " + key);
+  LST_ABI_CATCH_INT
 }
 
 void lst_es_free(lst_es* es) {
+  LST_ABI_TRY
   if (!es)
     return;
   if (es->arena) {
     cudaSetDevice(es->device);
     cudaFree(es->arena);
+    staticOutputDeviceRelease(es->device);
   }
   delete es;
+  LST_ABI_CATCH_VOID
 }
 
 int lst_es_get_info(const lst_es* es, lst_es_info* out) {
+  LST_ABI_TRY
   if (!es || !out)
     return setError("lst_es_get_info: null argument");
   out->nModules = es->host.nModules;
@@ -845,18 +901,22 @@ int lst_es_get_info(const lst_es* es, lst_es_info* out) {
   out->maxTriplets = es->host.maxTriplets;
   out->maxQuintuplets = es->host.maxQuintuplets;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_es_set_t5dnn_weights(lst_es* es, const float* weights, size_t n) {
+  LST_ABI_TRY
   if (!es || !weights)
     return setError("lst_es_set_t5dnn_weights: null argument");
   if (n != lst::kT5DnnParams)
     return setError("T5 DNN weights must hold 2337 values");
   es->dnn.assign(weights, weights + n);
   return uploadWeights(es);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, lst_event** out) {
+  LST_ABI_TRY
   if (!es || !out || n_slots <= 0 || max_hits == 0)
     return setError("lst_event_create: bad argument");
   if (es->device < 0 || !es->arena)
@@ -933,9 +993,11 @@ int lst_event_create(lst_es* es, int n_slots, uint32_t max_hits, void* stream, l
   LST_CUDA(cudaStreamSynchronize(ev->stream));
   *out = ev.release();
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 void lst_event_destroy(lst_event* ev) {
+  LST_ABI_TRY
   if (!ev)
     return;
   cudaSetDevice(ev->device);
@@ -972,25 +1034,31 @@ void lst_event_destroy(lst_event* ev) {
   if (ev->ownStream)
     cudaStreamDestroy(ev->stream);
   delete ev;
+  LST_ABI_CATCH_VOID
 }
 
 int lst_event_memory(const lst_event* ev, size_t* bytes) {
+  LST_ABI_TRY
   if (!ev || !bytes)
     return setError("lst_event_memory: null argument");
   *bytes = ev->totalBytes + ev->inboxBytes + ev->stage[0].bytes + ev->stage[1].bytes;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_sync(lst_event* ev) {
+  LST_ABI_TRY
   if (!ev)
     return setError("null event set");
   LST_CUDA(cudaStreamSynchronize(ev->stream));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 void* lst_event_stream(lst_event* ev) { return ev ? static_cast<void*>(ev->stream) : nullptr; }
 
 int lst_event_set_t5_method(lst_event* ev, int method) {
+  LST_ABI_TRY
   if (!ev)
     return setError("null event set");
   if (method != LST_T5_DNN && method != LST_T5_CUTS)
@@ -999,9 +1067,11 @@ int lst_event_set_t5_method(lst_event* ev, int method) {
     return setError("the DNN T5 method needs weights");
   ev->t5Method = method;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_set_walk(lst_event* ev, int on) {
+  LST_ABI_TRY
   if (!ev)
     return setError("null event set");
   LST_CUDA(cudaStreamSynchronize(ev->stream));
@@ -1009,17 +1079,21 @@ int lst_event_set_walk(lst_event* ev, int on) {
     v.forceWalk = on ? 1u : 0u;
   LST_CUDA(cudaMemcpy(ev->dv, ev->hv.data(), sizeof(lst::EventView) * ev->nSlots, cudaMemcpyHostToDevice));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_reset(lst_event* ev, int slot) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
   return runReset(ev, slot, 1);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_add_hits(lst_event* ev, int slot, uint32_t n, const float* x, const float* y, const float* z,
                        const uint32_t* detId, const uint32_t* idxInNtuple) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
@@ -1041,6 +1115,7 @@ int lst_event_add_hits(lst_event* ev, int slot, uint32_t n, const float* x, cons
   }
   LST_LAUNCH(lst::kSetInputCounts, 1, 1, ev->dv, slot, 1, n, 1, 0u, 0u);
   return runHitKernels(ev, slot, 1);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_add_pixel_segments(lst_event* ev, int slot, uint32_t n, const uint32_t* hitIndices0,
@@ -1050,6 +1125,7 @@ int lst_event_add_pixel_segments(lst_event* ev, int slot, uint32_t n, const uint
                                  const float* eta, const float* etaErr, const float* phi, const int32_t* charge,
                                  const uint32_t* seedIdx, const int32_t* superbin, const int8_t* pixelType,
                                  const int8_t* isQuad) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
@@ -1087,37 +1163,61 @@ int lst_event_add_pixel_segments(lst_event* ev, int slot, uint32_t n, const uint
   }
   LST_LAUNCH(lst::kSetInputCounts, 1, 1, ev->dv, slot, 0, 0u, 1, size, status);
   return runPixelIngest(ev, slot, 1);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_run_stage(lst_event* ev, int slot, int stage) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
   return runStage(ev, slot, 1, stage);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_create_mini_doublets(lst_event* ev, int slot) {
+  LST_ABI_TRY
   return lst_event_run_stage(ev, slot, LST_STAGE_MINI_DOUBLETS);
+  LST_ABI_CATCH_INT
 }
-int lst_event_create_segments(lst_event* ev, int slot) { return lst_event_run_stage(ev, slot, LST_STAGE_SEGMENTS); }
-int lst_event_create_triplets(lst_event* ev, int slot) { return lst_event_run_stage(ev, slot, LST_STAGE_TRIPLETS); }
+int lst_event_create_segments(lst_event* ev, int slot) {
+  LST_ABI_TRY
+  return lst_event_run_stage(ev, slot, LST_STAGE_SEGMENTS);
+  LST_ABI_CATCH_INT
+}
+int lst_event_create_triplets(lst_event* ev, int slot) {
+  LST_ABI_TRY
+  return lst_event_run_stage(ev, slot, LST_STAGE_TRIPLETS);
+  LST_ABI_CATCH_INT
+}
 int lst_event_create_quintuplets(lst_event* ev, int slot) {
+  LST_ABI_TRY
   return lst_event_run_stage(ev, slot, LST_STAGE_QUINTUPLETS);
+  LST_ABI_CATCH_INT
 }
 int lst_event_pixel_line_segment_cleaning(lst_event* ev, int slot) {
+  LST_ABI_TRY
   return lst_event_run_stage(ev, slot, LST_STAGE_PLS_CLEANING);
+  LST_ABI_CATCH_INT
 }
 int lst_event_create_pixel_quintuplets(lst_event* ev, int slot) {
+  LST_ABI_TRY
   return lst_event_run_stage(ev, slot, LST_STAGE_PIXEL_QUINTUPLETS);
+  LST_ABI_CATCH_INT
 }
 int lst_event_create_pixel_triplets(lst_event* ev, int slot) {
+  LST_ABI_TRY
   return lst_event_run_stage(ev, slot, LST_STAGE_PIXEL_TRIPLETS);
+  LST_ABI_CATCH_INT
 }
 int lst_event_create_track_candidates(lst_event* ev, int slot) {
+  LST_ABI_TRY
   return lst_event_run_stage(ev, slot, LST_STAGE_TRACK_CANDIDATES);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_get_counts(lst_event* ev, int slot, lst_counts* out) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
@@ -1127,10 +1227,12 @@ int lst_event_get_counts(lst_event* ev, int slot, lst_counts* out) {
   if (rc)
     return rc;
   return static_cast<int>(out->status & 0x7fffffffu);
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_get_field(lst_event* ev, int slot, const char* name, void* dst, size_t capacity, size_t* n_elems,
                         size_t* elem_size) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
@@ -1150,10 +1252,12 @@ int lst_event_get_field(lst_event* ev, int slot, const char* name, void* dst, si
     LST_CUDA(cudaStreamSynchronize(ev->stream));
   }
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_field_device_ptr(lst_event* ev, int slot, const char* name, void** dptr, size_t* n_elems,
                                size_t* elem_size) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
@@ -1167,18 +1271,28 @@ int lst_event_field_device_ptr(lst_event* ev, int slot, const char* name, void**
   if (elem_size)
     *elem_size = esz;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
-int lst_field_count(void) { return static_cast<int>(fieldTable().size()); }
+int lst_field_count(void) {
+  LST_ABI_TRY
+  return static_cast<int>(fieldTable().size());
+  LST_ABI_CATCH_INT
+}
 
 const char* lst_field_name(int i) {
-  const auto& t = fieldTable();
-  if (i < 0 || i >= static_cast<int>(t.size()))
+  try {
+    const auto& t = fieldTable();
+    if (i < 0 || i >= static_cast<int>(t.size()))
+      return nullptr;
+    return t[i].name.c_str();
+  } catch (...) {
     return nullptr;
-  return t[i].name.c_str();
+  }
 }
 
 int lst_field_info(int i, const char** name, size_t* elem_size, char* kind) {
+  LST_ABI_TRY
   const auto& t = fieldTable();
   if (i < 0 || i >= static_cast<int>(t.size()))
     return setError("field index out of range");
@@ -1189,6 +1303,7 @@ int lst_field_info(int i, const char** name, size_t* elem_size, char* kind) {
   if (kind)
     *kind = t[i].kind;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 size_t lst_packed_size(uint32_t n_hits, uint32_t n_pls) { return lst::packedLayout(n_hits, n_pls).end; }
@@ -1234,16 +1349,21 @@ namespace {
 
 int lst_batch_upload(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
                      const uint64_t* blob_offsets) {
+  LST_ABI_TRY
   return uploadInbox(ev, first, count, blobs, total_bytes, blob_offsets, 0, "lst_batch_upload");
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_upload_seeds(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
                            const uint64_t* blob_offsets) {
+  LST_ABI_TRY
   return uploadInbox(ev, first, count, blobs, total_bytes, blob_offsets, 1, "lst_batch_upload_seeds");
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_stage(lst_event* ev, int first, int count, const void* blobs, size_t total_bytes,
                     const uint64_t* blob_offsets, int seed_layout) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1290,9 +1410,11 @@ int lst_batch_stage(lst_event* ev, int first, int count, const void* blobs, size
   ev->staged.total = total_bytes;
   ev->stageNext ^= 1;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_ingest_staged(lst_event* ev) {
+  LST_ABI_TRY
   if (!ev)
     return setError("null event set");
   if (!ev->staged.pending)
@@ -1312,9 +1434,11 @@ int lst_batch_ingest_staged(lst_event* ev) {
     return rc;
   LST_CUDA(cudaEventRecord(b.freed, ev->stream));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_ingest(lst_event* ev, int first, int count) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1331,6 +1455,7 @@ int lst_batch_ingest(lst_event* ev, int first, int count) {
     if (b.ptr && ev->inbox == b.ptr)
       LST_CUDA(cudaEventRecord(b.freed, ev->stream));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 size_t lst_seed_packed_size(uint32_t n_ph2, uint32_t n_seeds, uint32_t n_seed_hits) {
@@ -1338,6 +1463,7 @@ size_t lst_seed_packed_size(uint32_t n_ph2, uint32_t n_seeds, uint32_t n_seed_hi
 }
 
 int lst_seed_pack(const lst_seed_input* in, void* dst, size_t capacity) {
+  LST_ABI_TRY
   if (!in || !dst)
     return setError("lst_seed_pack: null argument");
   const uint32_t nS = in->n_seeds, nH = in->n_ph2;
@@ -1400,9 +1526,11 @@ int lst_seed_pack(const lst_seed_input* in, void* dst, size_t capacity) {
   if (L.end > L.hitIdx + 4 * size_t(nSH))
     std::memset(d + L.hitIdx + 4 * size_t(nSH), 0, L.end - L.hitIdx - 4 * size_t(nSH));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_prepare_input(lst_event* ev, int slot, const lst_seed_input* in) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, slot, 1);
   if (rc)
     return rc;
@@ -1419,9 +1547,11 @@ int lst_event_prepare_input(lst_event* ev, int slot, const lst_seed_input* in) {
     return rc;
   const uint64_t offset = 0;
   return lst_batch_upload_seeds(ev, slot, 1, ev->hostPack.data(), need, &offset);
+  LST_ABI_CATCH_INT
 }
 
 int lst_run(lst_event* ev, int slot, const lst_seed_input* in, lst_output* out) {
+  LST_ABI_TRY
   int rc = lst_event_prepare_input(ev, slot, in);
   if (rc)
     return rc;
@@ -1429,9 +1559,11 @@ int lst_run(lst_event* ev, int slot, const lst_seed_input* in, lst_output* out) 
   if (rc)
     return rc;
   return out ? lst_batch_get_output(ev, slot, 1, out) : 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last_stage) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1457,9 +1589,11 @@ int lst_batch_run(lst_event* ev, int first, int count, int first_stage, int last
       return rc;
   }
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_run_graph(lst_event* ev, int first, int count, int first_stage, int last_stage) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1491,11 +1625,13 @@ int lst_batch_run_graph(lst_event* ev, int first, int count, int first_stage, in
   LST_CUDA(cudaGraphLaunch(it->second.exec, ev->stream));
   ev->launches += it->second.kernels;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_t5_probe(lst_event* ev, int first, int count, float* feat, float* score, uint8_t* cut_pass,
                        uint8_t* rz_tight, uint32_t* hits, int32_t* event_index, uint32_t capacity,
                        uint32_t* n_found) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1521,18 +1657,22 @@ int lst_batch_t5_probe(lst_event* ev, int first, int count, float* feat, float* 
   LST_CUDA(cudaStreamSynchronize(s));
   *n_found = n;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_es_set_t5dnn_threshold(lst_es* es, float wp) {
+  LST_ABI_TRY
   if (!es || es->device < 0)
     return setError("lst_es_set_t5dnn_threshold: no device event setup");
   LST_CUDA(cudaSetDevice(es->device));
   LST_CUDA(cudaMemcpyToSymbol(lst::c_t5dnnWP, &wp, sizeof(float)));
   LST_CUDA(cudaDeviceSynchronize());
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1541,9 +1681,11 @@ int lst_batch_get_counts(lst_event* ev, int first, int count, lst_counts* out) {
   if (count == 0)
     return 0;
   return readCounts(ev, first, count, out);
+  LST_ABI_CATCH_INT
 }
 
 int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1605,6 +1747,7 @@ int lst_batch_get_output(lst_event* ev, int first, int count, lst_output* out) {
   LST_CUDA(cudaMemcpyAsync(out->type, dType, nTC * sizeof(short), cudaMemcpyDeviceToHost, s));
   LST_CUDA(cudaStreamSynchronize(s));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 }  // extern "C"
@@ -1628,10 +1771,30 @@ namespace {
   static __device__ __align__(256) unsigned char g_staticOutput[kStaticOutputBytes];
 
   // Device address of g_staticOutput per device, looked up once per device
-  // with that device current.
+  // with that device current.  The address is cached only while an event
+  // setup is alive on the device: freeing the last one forgets it, so a
+  // device reset between two event setups cannot leave a stale address.  (A
+  // cudaDeviceReset while an event setup is still alive invalidates that
+  // event setup and its event sets as well, and is not supported.)
   constexpr int kMaxDevices = 64;
   std::mutex g_staticOutputMutex;
   unsigned char* g_staticOutputPtr[kMaxDevices] = {};
+  int g_liveEsPerDevice[kMaxDevices] = {};
+
+  void staticOutputDeviceRetain(int device) {
+    if (device < 0 || device >= kMaxDevices)
+      return;
+    std::lock_guard<std::mutex> lock(g_staticOutputMutex);
+    ++g_liveEsPerDevice[device];
+  }
+
+  void staticOutputDeviceRelease(int device) {
+    if (device < 0 || device >= kMaxDevices)
+      return;
+    std::lock_guard<std::mutex> lock(g_staticOutputMutex);
+    if (g_liveEsPerDevice[device] > 0 && --g_liveEsPerDevice[device] == 0)
+      g_staticOutputPtr[device] = nullptr;
+  }
 
   int staticOutputScratch(int device, unsigned char** out) {
     if (device < 0 || device >= kMaxDevices)
@@ -1670,6 +1833,7 @@ namespace {
 extern "C" {
 
 int lst_batch_get_output_static(lst_event* ev, int first, int count, lst_output* out) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -1731,16 +1895,20 @@ int lst_batch_get_output_static(lst_event* ev, int first, int count, lst_output*
   LST_CUDA(cudaMemcpyAsync(out->type, dType, nTC * sizeof(short), cudaMemcpyDeviceToHost, s));
   LST_CUDA(cudaStreamSynchronize(s));
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_launches(const lst_event* ev, uint64_t* n) {
+  LST_ABI_TRY
   if (!ev || !n)
     return setError("lst_event_launches: null argument");
   *n = ev->launches;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_set_profiling(lst_event* ev, int on) {
+  LST_ABI_TRY
   if (!ev)
     return setError("null event set");
   LST_CUDA(cudaStreamSynchronize(ev->stream));
@@ -1748,9 +1916,11 @@ int lst_event_set_profiling(lst_event* ev, int on) {
   ev->profile.clear();
   ev->poolUsed = 0;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int* n_kernels) {
+  LST_ABI_TRY
   if (!ev || !n_kernels)
     return setError("lst_event_get_profile: null argument");
   LST_CUDA(cudaStreamSynchronize(ev->stream));
@@ -1777,6 +1947,7 @@ int lst_event_get_profile(lst_event* ev, lst_kernel_time* out, int capacity, int
   ev->profile.clear();
   ev->poolUsed = 0;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 }  // extern "C"
@@ -1886,11 +2057,16 @@ namespace {
 
 extern "C" {
 
-int lst_tune_kernel_count(void) { return kTuCount; }
+int lst_tune_kernel_count(void) {
+  LST_ABI_TRY
+  return kTuCount;
+  LST_ABI_CATCH_INT
+}
 
 const char* lst_tune_kernel_name(int k) { return (k >= 0 && k < kTuCount) ? kTuneSpecs[k].name : nullptr; }
 
 int lst_event_set_launch_shape(lst_event* ev, int k, int warps_per_block, int blocks_per_sm) {
+  LST_ABI_TRY
   if (!ev)
     return setError("null event set");
   if (k < 0 || k >= kTuCount)
@@ -1906,9 +2082,11 @@ int lst_event_set_launch_shape(lst_event* ev, int k, int warps_per_block, int bl
     ev->shape[k].perSM = blocks_per_sm;
   }
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 int lst_event_get_launch_shape(const lst_event* ev, int k, int* warps_per_block, int* blocks_per_sm) {
+  LST_ABI_TRY
   if (!ev || !warps_per_block || !blocks_per_sm)
     return setError("lst_event_get_launch_shape: null argument");
   if (k < 0 || k >= kTuCount)
@@ -1916,11 +2094,19 @@ int lst_event_get_launch_shape(const lst_event* ev, int k, int* warps_per_block,
   *warps_per_block = ev->shape[k].warps;
   *blocks_per_sm = ev->shape[k].perSM;
   return 0;
+  LST_ABI_CATCH_INT
 }
 
-uint64_t lst_es_geometry_hash(const lst_es* es) { return es ? geometryHash(es) : 0; }
+uint64_t lst_es_geometry_hash(const lst_es* es) {
+  try {
+    return es ? geometryHash(es) : 0;
+  } catch (...) {
+    return 0;
+  }
+}
 
 int lst_autotune_load(lst_event* ev, int count, const char* cache_path) {
+  LST_ABI_TRY
   if (!ev || !cache_path)
     return setError("lst_autotune_load: null argument");
   std::ifstream in(cache_path);
@@ -1942,9 +2128,11 @@ int lst_autotune_load(lst_event* ev, int count, const char* cache_path) {
       return rc;
   }
   return 1;
+  LST_ABI_CATCH_INT
 }
 
 int lst_autotune(lst_event* ev, int first, int count, const char* cache_path) {
+  LST_ABI_TRY
   int rc = checkSlots(ev, first, count);
   if (rc)
     return rc;
@@ -2055,6 +2243,7 @@ int lst_autotune(lst_event* ev, int first, int count, const char* cache_path) {
       return setError(std::string("lst_autotune: cannot replace ") + cache_path);
   }
   return 0;
+  LST_ABI_CATCH_INT
 }
 
 }  // extern "C"
