@@ -1,0 +1,203 @@
+"""CUDA path vs the reference CPU backend on the wider workloads.
+
+* PU250 events with 5% displaced tracks (generator configuration 5), whose
+  large-dxy and endcap-heavy patterns reach T5 and pT3 branches that prompt
+  pileup rarely takes (SDL/Quintuplet.h:2508-2984, SDL/PixelTriplet.h:826-1025);
+* a sweep of 64 uneven events (configuration 3) run as one batch and each
+  compared with the reference, the reference events spread over host threads;
+* dense events whose per-module occupancy caps overflow, where the reference
+  keeps the first objects in its serial loop order (SDL/MiniDoublet.h:960-968,
+  SDL/Segment.h:879-885, SDL/Triplet.h, SDL/Quintuplet.h);
+* degenerate inputs: an event without hits or pLS, and hits with NaN
+  coordinates.
+
+The oracle is oracle/_ref/liblstref_cr.so, the unmodified reference built
+for the CPU with strict IEEE arithmetic; every live field of every store must
+match bit for bit."""
+import os
+import threading
+
+import numpy as np
+import pytest
+
+from oracle import compare, identity, reflib
+from tracklooper_b200 import gen, lst
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not reflib.available("cr"):
+        pytest.fail("reference library oracle/_ref/liblstref_cr.so is not built")
+    r = reflib.RefLST("cr")
+    yield r
+    r.close()
+
+
+@pytest.fixture(scope="module")
+def es():
+    e = lst.ES(device=0)
+    yield e
+    e.close()
+
+
+def _sizes(es, max_hits):
+    info = es.info
+    return {"H": max_hits, "MD": info["nTotalMDs"], "LS": info["nTotalSegments"],
+            "T3": info["maxTriplets"], "T5": info["maxQuintuplets"]}
+
+
+def _run_both(ref, ev, inp):
+    ref.run_event(inp)
+    ev.run(inp)
+
+
+def _compare_all(ref, es, get_gpu, n_hits, max_hits):
+    dtypes = lst.field_dtypes()
+    return compare.compare_stores(get_gpu, lambda n: ref.field(n, dtype=dtypes[n]), list(dtypes),
+                                  es.info["nLowerModules"], n_hits, _sizes(es, max_hits))
+
+
+@pytest.mark.parametrize("index", range(8))
+def test_pu250_displaced_events(ref, es, index):
+    inp = gen.generate_event(5, index)
+    ev = lst.Event(es, max_hits=inp.n_hits + 1024)
+    try:
+        _run_both(ref, ev, inp)
+        problems = _compare_all(ref, es, ev.field, inp.n_hits, ev.event_set.max_hits)
+        assert not problems, "; ".join(problems[:8])
+        c = ev.counts()
+        assert c["nQuintuplets"] > 0 and c["nPixelTriplets"] > 0 and c["nTrackCandidates"] > 1000
+    finally:
+        ev.event_set.close()
+
+
+def test_sweep_64_uneven_events_batched(es):
+    """64 events of uneven pileup (140-250) in one batch, every slot compared
+    with its own reference run."""
+    n = 64
+    inputs = [gen.generate_event(3, 100 + i) for i in range(n)]
+    max_hits = max(i.n_hits for i in inputs) + 1024
+    eset = lst.EventSet(es, n_slots=n, max_hits=max_hits)
+    try:
+        blob, offsets = lst.pack_events(inputs)
+        eset.upload_packed(0, blob, offsets)
+        eset.run(0, n)
+        counts = eset.batch_counts(0, n)
+        dtypes = lst.field_dtypes()
+        names = list(dtypes)
+        sizes = _sizes(es, max_hits)
+        workers = max(1, min(8, (os.cpu_count() or 2) // 2))
+        base = reflib.RefLST("cr")
+        refs = [base] + [base.fork() for _ in range(workers - 1)]
+        gpu_lock = threading.Lock()
+        failures = []
+        next_slot = [0]
+        lock = threading.Lock()
+
+        def gpu_field(slot, name):
+            with gpu_lock:
+                return eset.field(slot, name)
+
+        def work(r):
+            while True:
+                with lock:
+                    slot = next_slot[0]
+                    next_slot[0] += 1
+                if slot >= n:
+                    return
+                r.run_event(inputs[slot])
+                p = compare.compare_stores(lambda nm: gpu_field(slot, nm), lambda nm: r.field(nm, dtype=dtypes[nm]),
+                                           names, es.info["nLowerModules"], inputs[slot].n_hits, sizes)
+                n_tc = int(r.field("tc.nTrackCandidates", dtype=np.uint32)[0])
+                if p or counts[slot]["nTrackCandidates"] != n_tc:
+                    with lock:
+                        failures.append((slot, p[:4]))
+
+        ths = [threading.Thread(target=work, args=(r,)) for r in refs]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        for r in refs[1:]:
+            r.close()
+        base.close()
+        assert not failures, failures[:4]
+    finally:
+        eset.close()
+
+
+@pytest.mark.parametrize("config,index,pileup", [(2, 1, 0.0), (3, 1, 400.0)])
+def test_occupancy_cap_overflow_keeps_reference_order(ref, es, config, index, pileup):
+    """Events where per-module caps drop objects: the CUDA path flags it and
+    keeps exactly the reference's objects (the first ones in serial order)."""
+    inp = gen.generate_event(config, index, pileup)
+    ev = lst.Event(es, max_hits=inp.n_hits + 1024)
+    try:
+        _run_both(ref, ev, inp)
+        problems = _compare_all(ref, es, ev.field, inp.n_hits, ev.event_set.max_hits)
+        assert not problems, "; ".join(problems[:8])
+        c = ev.counts()
+        assert c["status"] & 0x20, "expected an occupancy-cap overflow"
+        L = es.info["nLowerModules"]
+        dropped = {}
+        for st, nname, tname in (("md", "md.nMDs", "md.totOccupancyMDs"), ("ls", "ls.nSegments", "ls.totOccupancySegments"),
+                                 ("t3", "t3.nTriplets", "t3.totOccupancyTriplets"),
+                                 ("t5", "t5.nQuintuplets", "t5.totOccupancyQuintuplets")):
+            kept = ev.field(nname)[:L].astype(np.int64)
+            tot = ev.field(tname)[:L].astype(np.int64)
+            dropped[st] = int((tot - kept).clip(0).sum())
+        # LS and T3 caps overflow in these events, MD and T5 caps in the first
+        assert dropped["ls"] > 0 and dropped["t3"] > 0
+        if config == 2:
+            assert dropped["md"] > 0 and dropped["t5"] > 0
+    finally:
+        ev.event_set.close()
+
+
+def test_empty_event(ref, es):
+    inp = gen.generate_event(1, 0)
+    empty = gen.EventInput(inp.x[:0], inp.y[:0], inp.z[:0], inp.detId[:0], inp.idxInNtuple[:0],
+                           {k: v[:0] for k, v in inp.pls.items()}, inp.hit_sim[:0], inp.pls_sim[:0], 0,
+                           inp.particles[:0])
+    ev = lst.Event(es, max_hits=4096)
+    try:
+        ev.run(empty)
+        c = ev.counts()
+        assert c["status"] == 0
+        assert all(c[k] == 0 for k in ("nHits", "nMiniDoublets", "nSegments", "nTriplets", "nQuintuplets",
+                                       "nPixelTriplets", "nPixelQuintuplets", "nTrackCandidates"))
+        hits, ln, seed, typ = ev.getOutput()
+        assert len(hits) == 0 and ln.size == 0
+    finally:
+        ev.event_set.close()
+
+
+def test_nan_hit_coordinates(ref, es):
+    """Hits with NaN coordinates make no objects, on either side, and the
+    rest of the event is unchanged: the same objects as the reference."""
+    inp = gen.generate_event(2, 20)
+    rng = np.random.default_rng(3)
+    bad = rng.choice(inp.n_hits, size=200, replace=False)
+    x = inp.x.copy()
+    z = inp.z.copy()
+    x[bad[:100]] = np.nan
+    z[bad[100:]] = np.nan
+    nan_inp = gen.EventInput(x, inp.y, z, inp.detId, inp.idxInNtuple, inp.pls, inp.hit_sim, inp.pls_sim,
+                             inp.n_ot_hits, inp.particles)
+    ev = lst.Event(es, max_hits=inp.n_hits + 1024)
+    try:
+        _run_both(ref, ev, nan_inp)
+        dtypes = lst.field_dtypes()
+        L = es.info["nLowerModules"]
+        a = identity.Objects(ev.field, L, inp.n_hits)
+        b = identity.Objects(lambda n: ref.field(n, dtype=dtypes[n]), L, inp.n_hits)
+        d = identity.diff(a, b)
+        for st, r in d.items():
+            assert r["only_a"] == 0 and r["only_b"] == 0 and r["state_differ"] == 0, (st, r)
+        bad_set = set(int(i) for i in bad)
+        assert not any(h in bad_set for k in a.keys["md"] for h in k)
+        assert ev.counts()["nTrackCandidates"] > 1000
+    finally:
+        ev.event_set.close()
