@@ -10,15 +10,15 @@ object before it flips):
   ls   the four hits of its two MDs                  Segment.h:358-390
   pls  pLS index with its isDup bits                 Segment.h:392-453, Kernels.h:384
   t3   its 6 hit indices                             Triplet.h:181-239
-  t5   its 10 hit indices (+ isDup / TightCutFlag)   Quintuplet.h:150-216
+  t5   its 10 hit indices (+ isDup / TightCutFlag / partOfPT5)  Quintuplet.h:150-216
   pt3  (pLS index, 10 hit indices)                   PixelTriplet.h:134-204
   pt5  (pLS index, 14 hit indices)                   PixelTriplet.h:1961-2036
   tc   (type, pixel seed index, 14 hit slots)        TrackCandidate.h:111-163
 
 An object present on one side only is a *root* flip when every constituent
-it is built from (hits, MDs, LS, T3, T5, pLS) exists on the other side too:
-the two sides then evaluated the same candidate and decided differently.
-Otherwise it is a *cascade* of a flip upstream.
+it is built from (hits, MDs, LS, T3, T5, pLS) exists on the other side too,
+with the same flags: the two sides then evaluated the same candidate and
+decided differently.  Otherwise it is a *cascade* of a flip upstream.
 
 Float values of objects present on both sides are compared as well: the
 largest relative difference per field is reported.
@@ -87,19 +87,22 @@ class Objects:
 
         h3 = get("t3.hitIndices")
         segi = get("t3.segmentIndices")
+        t3_p5 = get("t3.partOfPT5")
         t3_key = {}
-        t3_parts = []
+        t3_parts, t3_state = [], []
         for i in si.t3:
             i = int(i)
             t3_key[i] = tuple(int(x) for x in h3[6 * i: 6 * i + 6])
             s0, s1 = int(segi[2 * i]), int(segi[2 * i + 1])
             t3_parts.append((("ls", ls_key.get(s0, ("?", s0))), ("ls", ls_key.get(s1, ("?", s1)))))
-        self._put("t3", si.t3, [t3_key[int(i)] for i in si.t3], t3_parts)
+            t3_state.append((int(t3_p5[i]),))
+        self._put("t3", si.t3, [t3_key[int(i)] for i in si.t3], t3_parts, t3_state)
 
         h5 = get("t5.hitIndices")
         tri = get("t5.tripletIndices")
         dup5 = get("t5.isDup")
         tight = get("t5.TightCutFlag")
+        t5_p5 = get("t5.partOfPT5")
         t5_key = {}
         t5_parts, t5_state = [], []
         for i in si.t5:
@@ -107,7 +110,7 @@ class Objects:
             t5_key[i] = tuple(int(x) for x in h5[10 * i: 10 * i + 10])
             a, b = int(tri[2 * i]), int(tri[2 * i + 1])
             t5_parts.append((("t3", t3_key.get(a, ("?", a))), ("t3", t3_key.get(b, ("?", b)))))
-            t5_state.append((int(dup5[i]), int(tight[i])))
+            t5_state.append((int(dup5[i]), int(tight[i]), int(t5_p5[i])))
         self._put("t5", si.t5, [t5_key[int(i)] for i in si.t5], t5_parts, t5_state)
 
         p3 = get("pt3.pixelSegmentIndices")
@@ -170,6 +173,12 @@ class Objects:
     def key_set(self, store):
         return set(self.keys[store])
 
+    def state_map(self):
+        """{store: {key: flags}} over all stores (cached)."""
+        if not hasattr(self, "_state_map"):
+            self._state_map = {st: dict(zip(self.keys[st], self.state[st])) for st in STORES}
+        return self._state_map
+
 
 def diff(a: Objects, b: Objects, stores=STORES, max_examples: int = 20) -> dict:
     """Per store: objects only in a / only in b (multiset difference), how many
@@ -180,16 +189,17 @@ def diff(a: Objects, b: Objects, stores=STORES, max_examples: int = 20) -> dict:
         ca, cb = Counter(a.keys[st]), Counter(b.keys[st])
         only_a = list((ca - cb).elements())
         only_b = list((cb - ca).elements())
-        sets = {"a": {s: a.key_set(s) for s in STORES}, "b": {s: b.key_set(s) for s in STORES}}
+        states = {"a": a.state_map(), "b": b.state_map()}
         pos_a = {k: j for j, k in enumerate(a.keys[st])}
         pos_b = {k: j for j, k in enumerate(b.keys[st])}
 
         def roots(only, side, other):
             pos = pos_a if side is a else pos_b
+            mine, theirs = (states["a"], states["b"]) if side is a else (states["b"], states["a"])
             r = []
             for k in only:
                 parts = side.parts[st][pos[k]]
-                if all(pk in sets["b" if other is b else "a"][ps] for ps, pk in parts):
+                if all(pk in theirs[ps] and theirs[ps][pk] == mine[ps].get(pk) for ps, pk in parts):
                     r.append(k)
             return r
 

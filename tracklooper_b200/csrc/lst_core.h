@@ -79,6 +79,10 @@ namespace lst {
 #else
 #define LST_HD_MATH inline
 #endif
+  // A host build that evaluates these headers in another arithmetic (the
+  // cut-flip tracer under oracle/trace/) defines LST_MATH_BINDING_PROVIDED and
+  // supplies the functions of this block itself.
+#if !defined(LST_MATH_BINDING_PROVIDED)
   LST_HD_MATH float fsin(float x) { return static_cast<float>(::sin(static_cast<double>(x))); }
   LST_HD_MATH float fcos(float x) { return static_cast<float>(::cos(static_cast<double>(x))); }
   LST_HD_MATH float ftan(float x) { return static_cast<float>(::tan(static_cast<double>(x))); }
@@ -102,6 +106,8 @@ namespace lst {
   LST_HD float fsqrt(float x) { return ::sqrtf(x); }
   LST_HD double dsqrt(double x) { return ::sqrt(x); }
   LST_HD bool fisnan(float x) { return x != x; }
+  LST_HD float fround_(float x) { return ::roundf(x); }
+#endif  // LST_MATH_BINDING_PROVIDED
 
   // ------------------------------------------------------ geometric helpers
   // SDL/Hit.h:111-192.
@@ -114,7 +120,7 @@ namespace lst {
     if (fabs_(x) <= float(M_PI))
       return x;
     constexpr float o2pi = 1.f / (2.f * float(M_PI));
-    float n = ::roundf(x * o2pi);
+    float n = fround_(x * o2pi);
     return x - n * float(2.f * float(M_PI));
   }
 
