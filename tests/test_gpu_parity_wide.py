@@ -175,8 +175,10 @@ def test_empty_event(ref, es):
 
 
 def test_nan_hit_coordinates(ref, es):
-    """Hits with NaN coordinates make no objects, on either side, and the
-    rest of the event is unchanged: the same objects as the reference."""
+    """Hits with NaN coordinates: the CUDA path keeps exactly the
+    reference's objects.  Some cut comparisons are false for NaN and some
+    are true, so the reference keeps a few mini-doublets with a NaN hit
+    (about 40 of 38 000 here), but no segment or longer object reaches one."""
     inp = gen.generate_event(2, 20)
     rng = np.random.default_rng(3)
     bad = rng.choice(inp.n_hits, size=200, replace=False)
@@ -197,7 +199,9 @@ def test_nan_hit_coordinates(ref, es):
         for st, r in d.items():
             assert r["only_a"] == 0 and r["only_b"] == 0 and r["state_differ"] == 0, (st, r)
         bad_set = set(int(i) for i in bad)
-        assert not any(h in bad_set for k in a.keys["md"] for h in k)
+        skip = {"ls": 0, "t3": 0, "t5": 0, "pt3": 1, "pt5": 1, "tc": 2}  # key entries before the hits
+        for st, n0 in skip.items():
+            assert not any(h in bad_set for k in a.keys[st] for h in k[n0:]), st
         assert ev.counts()["nTrackCandidates"] > 1000
     finally:
         ev.event_set.close()

@@ -63,7 +63,6 @@ namespace lst {
     unsigned int pixCandTotal;    // pT5 / pT3 candidates of the current pixel stage
     unsigned int pixPassCount;    // passing candidates found by kPixEval
     unsigned int pixFallback;     // the pixel stage overflowed the staging: walk instead
-    unsigned int t5DnnCount;      // candidates buffered for kT5Dnn
     unsigned int pixQueueCount;   // candidates passing the pixel pre-selection
     unsigned int t5QueueCount;    // candidates passing the quintuplet pre-selection
     unsigned int pixQueueBack;    // pixel candidates queued from the back (endcap tracklet algorithm)
@@ -117,10 +116,6 @@ namespace lst {
     unsigned int* t5CandFlag;   // per candidate: 0 = fails, else 1 + slot of its values in t5PassValues
     T5Values* t5PassValues;     // selection values of passing candidates
     unsigned int* t5PassC;      //   and their candidate index
-    float* t5DnnFeat;           // candidates at the classifier: features (38 each)
-    unsigned int* t5DnnCand;    //   candidate index
-    T5Values* t5DnnVals;        //   selection values so far
-    uint8_t* t5DnnTight;        //   rz-fit tight flag
     unsigned int* plsModPre;    // per pLS: candidate prefix over its connected modules (41 entries)
     unsigned int* plsCand;      // per pLS: candidates
     unsigned int* plsCandOff;   // per pLS: first candidate (nPLS + 1 entries)

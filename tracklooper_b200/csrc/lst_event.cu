@@ -518,8 +518,6 @@ namespace {
         LST_LAUNCH(lst::kT5ModScan, one, 1024, d, v);
         LST_LAUNCH(lst::kT5Pre, dim3(blocksFor(size_t(1) << 20, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kT5Eval, tunedFlatGrid(ev, kTuT5Eval, count), tunedThreads(ev, kTuT5Eval), d, v, useDnn);
-        if (useDnn)
-          LST_LAUNCH(lst::kT5Dnn, dim3(blocksFor(lst::kT5DnnCap, count, 128), count), 128, d, v);
         LST_LAUNCH(lst::kT5Walk, warpGrid(ev->es->nEligibleMax, lst::kT5Warps, count), 32 * lst::kT5Warps, d, v,
                    useDnn);
         LST_LAUNCH_SMEM(lst::kT5RankEmit, dim3(1, count), 1024, lst::kT5RankSmem, d, v);
@@ -666,7 +664,6 @@ namespace {
         {"kT5Emit", (const void*)lst::kT5Emit},
         {"kT5RankEmit", (const void*)lst::kT5RankEmit},
         {"kT5Walk", (const void*)lst::kT5Walk},
-        {"kT5Dnn", (const void*)lst::kT5Dnn},
         {"kT5Probe", (const void*)lst::kT5Probe},
         {"kT5DedupAfterBuild", (const void*)lst::kT5DedupAfterBuild},
         {"kT5Ranges", (const void*)lst::kT5Ranges},

@@ -237,10 +237,6 @@
   X(t5CandFlag, unsigned int, lst::kT5CandCap)        \
   X(t5PassValues, lst::T5Values, lst::kT5PassCap)     \
   X(t5PassC, unsigned int, lst::kT5PassCap)           \
-  X(t5DnnFeat, float, 38 * lst::kT5DnnCap)            \
-  X(t5DnnCand, unsigned int, lst::kT5DnnCap)          \
-  X(t5DnnVals, lst::T5Values, lst::kT5DnnCap)         \
-  X(t5DnnTight, uint8_t, lst::kT5DnnCap)              \
   X(plsModPre, unsigned int, P * (lst::kMaxConnectedModules + 1)) \
   X(plsCand, unsigned int, P)                         \
   X(plsCandOff, unsigned int, P + 1)                  \

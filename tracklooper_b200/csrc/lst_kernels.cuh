@@ -1026,7 +1026,6 @@ namespace lst {
   constexpr unsigned int kPixChunkCap = 1u << 16;   // 32-candidate chunks of the pT5 / pT3 chunk table
   constexpr unsigned int kT5SortCap = 1u << 15;     // quintuplets per event sorted by eta for the TC cleaning
   constexpr unsigned int kT5PassCap = 1u << 16;  // passing candidates per event whose values are kept
-  constexpr unsigned int kT5DnnCap = 1u << 14;   // candidates per event classified in kT5Dnn
 
   __device__ __forceinline__ unsigned int t5CandidatesOf(const EventView& ev, unsigned int innerT3) {
     const Triplets& t3 = ev.t3;
@@ -1105,7 +1104,6 @@ namespace lst {
       ev.sc->t5CandTotal = carry;
       ev.sc->t5CandOverflow = (carry > kT5CandCap || ev.forceWalk) ? 1u : 0u;
       ev.sc->t5PassCount = 0;
-      ev.sc->t5DnnCount = 0;
       ev.sc->t5QueueCount = 0;
       ev.sc->t5QueueBack = 0;
     }
@@ -1190,113 +1188,147 @@ namespace lst {
     }
   }
 
-  __global__ void __launch_bounds__(LST_LB_T5EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
-    const EventView& ev = evs[blockIdx.y];
-    if (ev.sc->t5CandOverflow)
-      return;
-    const unsigned int total = ev.sc->t5CandTotal;
-    const unsigned int front = ev.sc->t5QueueCount, back = ev.sc->t5QueueBack;
-    const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
-    const unsigned int n = fromQueue ? front + back : total;
-    ConstDnn dnn;
-    for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-      const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
-      unsigned int innerT3, outerT3;
-      uint16_t lm[5];
-      t5Decode(ev, c, innerT3, outerT3, lm);
-      T5Values v;
-      unsigned int flag = 0;
-      T5Stage st;
-      if (!t5SelectPre(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st)) {
-        ev.t5CandFlag[c] = 0;
-        continue;
-      }
-      if (useDnn) {
-        // The classifier runs in kT5Dnn over all candidates that reach it;
-        // without room in its buffer, it runs here.
-        const unsigned int k = atomicAdd(&ev.sc->t5DnnCount, 1u);
-        if (k < kT5DnnCap) {
-          t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius, v.outerRadius,
-                        v.bridgeRadius, ev.t5DnnFeat + size_t(k) * 38);
-          ev.t5DnnCand[k] = c;
-          ev.t5DnnVals[k] = v;
-          ev.t5DnnTight[k] = st.tight ? 1 : 0;
-          ev.t5CandFlag[c] = 0;
-          continue;
-        }
-      }
-      if (t5Classify(es.m, ev.md, ev.ls, ev.t3, dnn.get(), useDnn, c_t5dnnWP, lm, innerT3, v, st)) {
-        // keep the values of a passing candidate (flag = slot + 1), or mark
-        // it for re-evaluation (flag = kT5PassCap + 1) when the buffer is full
-        const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
-        if (slot < kT5PassCap) {
-          ev.t5PassValues[slot] = v;
-          ev.t5PassC[slot] = c;
-          flag = slot + 1;
-        } else {
-          flag = kT5PassCap + 1;
-        }
-      }
-      ev.t5CandFlag[c] = flag;
+  // Candidates of one block tile that reached the classifier, kept in shared
+  // memory until the tile's DNN pass (kT5Eval).
+  constexpr int kT5DnnTile = 64;
+  struct T5DnnSlot {
+    float feat[38];
+    T5Values v;
+    unsigned int mdIdx[5];
+    unsigned int cand;
+    float score;
+    uint16_t lm[5];
+    uint8_t tight;
+  };
+
+  // t5DnnForward (SDL/NeuralNetwork.h:21-165) evaluated by one warp for one
+  // candidate: lane j computes hidden unit j of each layer, summing its
+  // inputs in the same order as the serial loops, so the score is
+  // bit-identical; the layer-1 outputs reach the other lanes by shuffles.
+  // Every lane returns the score.
+  __device__ __forceinline__ float t5DnnForwardWarp(const T5DnnWeights& w, const float* x) {
+    const unsigned int lane = laneId();
+    float acc = 0;
+    for (int in = 0; in < 38; ++in)
+      acc += x[in] * w.w0[in * 32 + lane];
+    acc += w.b0[lane];
+    const float h1 = (acc > 0.f) ? acc : 0.f;
+    acc = 0;
+    for (int in = 0; in < 32; ++in)
+      acc += __shfl_sync(kFullMask, h1, in) * w.w2[in * 32 + lane];
+    acc += w.b2[lane];
+    const float h2 = (acc > 0.f) ? acc : 0.f;
+    float out = 0;
+    for (int in = 0; in < 32; ++in)
+      out += __shfl_sync(kFullMask, h2, in) * w.w4[in];
+    out += w.b4[0];
+    return fexp(out) / (fexp(out) + 1);
+  }
+
+  // Records a candidate that passes the T5 selection: its values go to the
+  // pass buffer (flag = slot + 1), or, when the buffer is full, the flag asks
+  // for re-evaluation at emission (flag = kT5PassCap + 1).
+  __device__ __forceinline__ void t5Keep(const EventView& ev, unsigned int c, const T5Values& v) {
+    const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
+    if (slot < kT5PassCap) {
+      ev.t5PassValues[slot] = v;
+      ev.t5PassC[slot] = c;
+      ev.t5CandFlag[c] = slot + 1;
+    } else {
+      ev.t5CandFlag[c] = kT5PassCap + 1;
     }
   }
 
-  // The DNN decision for the candidates kT5Eval buffered: one thread per
-  // candidate with the weights in shared memory (same arithmetic as the
-  // in-line classifier), then the values stored with a selected candidate.
-  __global__ void __launch_bounds__(128) kT5Dnn(DeviceES es, const EventView* evs) {
+  // The T5 selection of the queued candidates, with the DNN classifier fused
+  // in (SDL/Quintuplet.h:2921-2941 evaluates it inline).  The block takes its
+  // candidates in tiles of blockDim.  Each thread runs every test before the
+  // classifier on one candidate; those that reach it leave their 38 DNN
+  // inputs and selection values in shared memory.  After a barrier each warp
+  // classifies the tile's waiting candidates one at a time, a lane per hidden
+  // unit, with the weights in shared memory (t5DnnForwardWarp); after a
+  // second, each thread finishes one classified candidate.  So the
+  // classifier runs on full warps although only some candidates of a warp
+  // reach it, and nothing goes through global memory.  A candidate that finds
+  // the tile's slots full is classified by its own thread at once; the
+  // arithmetic is the same in every case.
+  __global__ void __launch_bounds__(LST_LB_T5EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
     __shared__ T5DnnWeights sW;
+    __shared__ T5DnnSlot sSlot[kT5DnnTile];
+    __shared__ unsigned int sCount;
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow)
       return;
-    {
+    if (useDnn) {
       const float* src = reinterpret_cast<const float*>(&c_t5dnn);
       float* dst = reinterpret_cast<float*>(&sW);
       for (int i = threadIdx.x; i < kT5DnnParams; i += blockDim.x)
         dst[i] = src[i];
     }
-    __syncthreads();
-    const unsigned int n = ev.sc->t5DnnCount < kT5DnnCap ? ev.sc->t5DnnCount : kT5DnnCap;
-    const int nE = *ev.rg.nEligibleT5Modules;
-    const unsigned int* off = ev.t5ModOff;
-    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-      float feat[38];
-#pragma unroll
-      for (int i = 0; i < 38; ++i)
-        feat[i] = ev.t5DnnFeat[size_t(k) * 38 + i];
-      const float inference = t5DnnForward(sW, feat);
-      if (!(inference > c_t5dnnWP))
-        continue;
-      const unsigned int c = ev.t5DnnCand[k];
-      T5Values v = ev.t5DnnVals[k];
-      int lo = 0, hi = nE;
-      while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (off[mid] <= c)
-          lo = mid;
-        else
-          hi = mid;
+    const float wp = c_t5dnnWP;
+    const unsigned int total = ev.sc->t5CandTotal;
+    const unsigned int front = ev.sc->t5QueueCount, back = ev.sc->t5QueueBack;
+    const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
+    const unsigned int n = fromQueue ? front + back : total;
+    const unsigned int tileStride = gridDim.x * blockDim.x;
+    const unsigned int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    // every thread of the block runs the same number of tiles (barriers inside)
+    for (unsigned int tile = blockIdx.x * blockDim.x; tile < n; tile += tileStride) {
+      if (threadIdx.x == 0)
+        sCount = 0;
+      __syncthreads();
+      const unsigned int q = tile + threadIdx.x;
+      if (q < n) {
+        const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
+        unsigned int innerT3, outerT3;
+        uint16_t lm[5];
+        t5Decode(ev, c, innerT3, outerT3, lm);
+        T5Values v;
+        T5Stage st;
+        if (!t5SelectPre(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st)) {
+          ev.t5CandFlag[c] = 0;
+        } else {
+          const unsigned int k = useDnn ? atomicAdd(&sCount, 1u) : unsigned(kT5DnnTile);
+          if (k < unsigned(kT5DnnTile)) {
+            T5DnnSlot& sl = sSlot[k];
+            t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius,
+                          v.outerRadius, v.bridgeRadius, sl.feat);
+            sl.v = v;
+            for (int i = 0; i < 5; ++i) {
+              sl.mdIdx[i] = st.mdIdx[i];
+              sl.lm[i] = lm[i];
+            }
+            sl.cand = c;
+            sl.tight = st.tight ? 1 : 0;
+          } else if (t5Classify(es.m, ev.md, ev.ls, ev.t3, sW, useDnn, wp, lm, innerT3, v, st)) {
+            t5Keep(ev, c, v);
+          } else {
+            ev.t5CandFlag[c] = 0;
+          }
+        }
       }
-      const uint16_t lm1 = ev.rg.indicesOfEligibleT5Modules[lo];
-      unsigned int innerT3, outerT3;
-      t5Candidate(ev, ev.rg.tripletModuleIndices[lm1], ev.t3.nTriplets[lm1], c - off[lo], innerT3, outerT3);
-      const Triplets& t3 = ev.t3;
-      uint16_t lm[5] = {lm1, t3.lowerModuleIndices[3 * innerT3 + 1], t3.lowerModuleIndices[3 * innerT3 + 2],
-                        t3.lowerModuleIndices[3 * outerT3 + 1], t3.lowerModuleIndices[3 * outerT3 + 2]};
-      const unsigned int* mi = ev.ls.mdIndices;
-      const unsigned int seg1 = t3.segmentIndices[2 * innerT3], seg2 = t3.segmentIndices[2 * innerT3 + 1];
-      const unsigned int seg3 = t3.segmentIndices[2 * outerT3], seg4 = t3.segmentIndices[2 * outerT3 + 1];
-      const unsigned int mdIdx[5] = {mi[2 * seg1], mi[2 * seg2], mi[2 * seg2 + 1], mi[2 * seg3 + 1], mi[2 * seg4 + 1]};
-      t5NonAnchor(es.m, ev.md, lm, mdIdx, v);
-      v.tightCutFlag = ev.t5DnnTight[k] != 0 and (inference > c_t5dnnWP);
-      const unsigned int slot = atomicAdd(&ev.sc->t5PassCount, 1u);
-      if (slot < kT5PassCap) {
-        ev.t5PassValues[slot] = v;
-        ev.t5PassC[slot] = c;
-        ev.t5CandFlag[c] = slot + 1;
-      } else {
-        ev.t5CandFlag[c] = kT5PassCap + 1;
+      __syncthreads();
+      const unsigned int m = sCount < unsigned(kT5DnnTile) ? sCount : unsigned(kT5DnnTile);
+      if (m == 0)
+        continue;  // uniform over the block: no candidate of the tile waits
+      for (unsigned int k = warp; k < m; k += nWarps) {
+        const float score = t5DnnForwardWarp(sW, sSlot[k].feat);
+        if (laneId() == 0)
+          sSlot[k].score = score;
       }
+      __syncthreads();
+      for (unsigned int k = threadIdx.x; k < m; k += blockDim.x) {
+        const T5DnnSlot& sl = sSlot[k];
+        const float inference = sl.score;
+        if (!(inference > wp)) {
+          ev.t5CandFlag[sl.cand] = 0;
+          continue;
+        }
+        T5Values v = sl.v;
+        t5NonAnchor(es.m, ev.md, sl.lm, sl.mdIdx, v);
+        v.tightCutFlag = sl.tight != 0 and (inference > wp);
+        t5Keep(ev, sl.cand, v);
+      }
+      __syncthreads();
     }
   }
 
