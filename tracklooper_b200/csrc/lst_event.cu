@@ -493,7 +493,7 @@ namespace {
     const dim3 one(1, count);
     switch (stage) {
       case LST_STAGE_MINI_DOUBLETS:
-        LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, nLower, count), tunedThreads(ev, kTuMD), d, v);
+        LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, 32), count), tunedThreads(ev, kTuMD), d, v);
         LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kMDDerived, tunedWarpGrid(ev, kTuMDDerived, nLower + 1, count), tunedThreads(ev, kTuMDDerived),
                    d, v);

@@ -74,20 +74,28 @@ namespace lst {
     float dPhi, dPhiMin, dPhiMax, dPhiChange, dPhiChangeMin, dPhiChangeMax;
   };
 
-  // Barrel-barrel segment (SDL/Segment.h:455-565).  dPhiMin/Max and
-  // dPhiChangeMin/Max keep their initial value 0.
-  LST_HD_BIG bool lsBarrel(const Modules& m,
-                       const MiniDoublets& md,
-                       uint16_t innerLM,
-                       uint16_t outerLM,
-                       unsigned int innerMD,
-                       unsigned int outerMD,
-                       LSValues& v) {
+  // The anchor positions and the dPhi cut of a segment candidate, computed
+  // by its first tests (lsBarrelWindow / lsEndcapWindow) for the rest.
+  struct LSWindow {
+    MDPos in, out;
+    float sdCut;
+  };
+
+  // The first tests of a barrel-barrel segment (SDL/Segment.h:455-500): the
+  // z window and the dPhi cut.  Cheap: no transcendental function.
+  LST_HD bool lsBarrelWindow(const Modules& m,
+                             const MiniDoublets& md,
+                             uint16_t innerLM,
+                             unsigned int innerMD,
+                             unsigned int outerMD,
+                             LSValues& v,
+                             LSWindow& w) {
     float sdMuls = (m.subdets[innerLM] == Barrel) ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / kPtCut
                                                   : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / kPtCut;
-    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
-    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
-    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
+    w.in = md.anchorPos[innerMD];
+    w.out = md.anchorPos[outerMD];
+    float zIn = w.in.z, rtIn = w.in.rt;
+    float zOut = w.out.z, rtOut = w.out.rt;
 
     float sdSlope = md.slope[outerMD];
     float sdPVoff = 0.1f / rtOut;
@@ -98,12 +106,27 @@ namespace lst {
     if (!((zOut >= zLo) && (zOut <= zHi)))
       return false;
 
-    float sdCut = sdSlope + fsqrt(sdMuls * sdMuls + sdPVoff * sdPVoff);
+    w.sdCut = sdSlope + fsqrt(sdMuls * sdMuls + sdPVoff * sdPVoff);
     v.dPhi = phiMpiPi(md.anchorPhi[outerMD] - md.anchorPhi[innerMD]);
-    if (!(fabs_(v.dPhi) <= sdCut))
+    return fabs_(v.dPhi) <= w.sdCut;
+  }
+
+  // Barrel-barrel segment (SDL/Segment.h:455-565).  dPhiMin/Max and
+  // dPhiChangeMin/Max keep their initial value 0.
+  LST_HD_BIG bool lsBarrel(const Modules& m,
+                       const MiniDoublets& md,
+                       uint16_t innerLM,
+                       uint16_t outerLM,
+                       unsigned int innerMD,
+                       unsigned int outerMD,
+                       LSValues& v) {
+    LSWindow w;
+    if (!lsBarrelWindow(m, md, innerLM, innerMD, outerMD, v, w))
       return false;
+    float xIn = w.in.x, yIn = w.in.y, zIn = w.in.z, rtIn = w.in.rt;
+    float xOut = w.out.x, yOut = w.out.y, zOut = w.out.z, rtOut = w.out.rt;
     v.dPhiChange = phiMpiPi(phiOf(xOut - xIn, yOut - yIn) - md.anchorPhi[innerMD]);
-    if (!(fabs_(v.dPhiChange) <= sdCut))
+    if (!(fabs_(v.dPhiChange) <= w.sdCut))
       return false;
 
     float thr[3];
@@ -120,17 +143,20 @@ namespace lst {
     return fabs_(dAlphaInnerMDOuterMD) < thr[2];
   }
 
-  // Segment with at least one endcap module (SDL/Segment.h:567-705).
-  LST_HD_BIG bool lsEndcap(const Modules& m,
-                       const MiniDoublets& md,
-                       uint16_t innerLM,
-                       uint16_t outerLM,
-                       unsigned int innerMD,
-                       unsigned int outerMD,
-                       LSValues& v) {
-    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
-    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
-    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
+  // The first tests of a segment with an endcap module (SDL/Segment.h:
+  // 567-660): z signs, the rt window, dPhi and dPhiChange.  Cheap: no
+  // transcendental function.
+  LST_HD bool lsEndcapWindow(const Modules& m,
+                             const MiniDoublets& md,
+                             uint16_t outerLM,
+                             unsigned int innerMD,
+                             unsigned int outerMD,
+                             LSValues& v,
+                             LSWindow& w) {
+    w.in = md.anchorPos[innerMD];
+    w.out = md.anchorPos[outerMD];
+    float zIn = w.in.z, rtIn = w.in.rt;
+    float zOut = w.out.z, rtOut = w.out.rt;
     bool outerLayerEndcapTwoS = (m.subdets[outerLM] == Endcap) && (m.moduleType[outerLM] == TwoS);
     float sdSlope = md.slope[outerMD];
     float disks2SMinRadius = 60.f;
@@ -150,6 +176,7 @@ namespace lst {
 
     v.dPhi = phiMpiPi(md.anchorPhi[outerMD] - md.anchorPhi[innerMD]);
     float sdCut = sdSlope;
+    w.sdCut = sdCut;
     if (outerLayerEndcapTwoS) {
       float dPhiPos_high = phiMpiPi(md.anchorHighEdgePhi[outerMD] - md.anchorPhi[innerMD]);
       float dPhiPos_low = phiMpiPi(md.anchorLowEdgePhi[outerMD] - md.anchorPhi[innerMD]);
@@ -166,9 +193,22 @@ namespace lst {
     v.dPhiChange = v.dPhi / dzFrac * (1.f + dzFrac);
     v.dPhiChangeMin = v.dPhiMin / dzFrac * (1.f + dzFrac);
     v.dPhiChangeMax = v.dPhiMax / dzFrac * (1.f + dzFrac);
-    if (!(fabs_(v.dPhiChange) <= sdCut))
-      return false;
+    return fabs_(v.dPhiChange) <= sdCut;
+  }
 
+  // Segment with at least one endcap module (SDL/Segment.h:567-705).
+  LST_HD_BIG bool lsEndcap(const Modules& m,
+                       const MiniDoublets& md,
+                       uint16_t innerLM,
+                       uint16_t outerLM,
+                       unsigned int innerMD,
+                       unsigned int outerMD,
+                       LSValues& v) {
+    LSWindow w;
+    if (!lsEndcapWindow(m, md, outerLM, innerMD, outerMD, v, w))
+      return false;
+    float xIn = w.in.x, yIn = w.in.y, zIn = w.in.z, rtIn = w.in.rt;
+    float xOut = w.out.x, yOut = w.out.y, zOut = w.out.z, rtOut = w.out.rt;
     float thr[3];
     lsDAlphaThresholds(m, md, xIn, yIn, zIn, rtIn, xOut, yOut, zOut, rtOut, innerLM, outerLM, innerMD, outerMD, thr);
     float innerMDAlpha = md.dphichanges[innerMD];
@@ -181,6 +221,21 @@ namespace lst {
     if (!(fabs_(dAlphaOuterMDSegment) < thr[1]))
       return false;
     return fabs_(dAlphaInnerMDOuterMD) < thr[2];
+  }
+
+  // The first tests of lsSelect alone (the windows and dPhi cuts): every
+  // candidate lsSelect accepts passes them, evaluated by the same code.
+  LST_HD bool lsPrefilter(const Modules& m,
+                          const MiniDoublets& md,
+                          uint16_t innerLM,
+                          uint16_t outerLM,
+                          unsigned int innerMD,
+                          unsigned int outerMD) {
+    LSValues v;
+    LSWindow w;
+    if (m.subdets[innerLM] == Barrel and m.subdets[outerLM] == Barrel)
+      return lsBarrelWindow(m, md, innerLM, innerMD, outerMD, v, w);
+    return lsEndcapWindow(m, md, outerLM, innerMD, outerMD, v, w);
   }
 
   LST_HD bool lsSelect(const Modules& m,

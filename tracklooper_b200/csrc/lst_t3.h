@@ -278,6 +278,22 @@ namespace lst {
     float betaIn, circleRadius, circleCenterX, circleCenterY;
   };
 
+  // The opening tests of t3Select alone (the shared mini-doublet and the r-z
+  // residual): every candidate t3Select accepts passes them, by the same code.
+  LST_HD bool t3Prefilter(const Modules& m,
+                          const MiniDoublets& md,
+                          const Segments& s,
+                          uint16_t lm1,
+                          uint16_t lm2,
+                          uint16_t lm3,
+                          unsigned int innerSeg,
+                          unsigned int outerSeg) {
+    if (s.mdIndices[2 * innerSeg + 1] != s.mdIndices[2 * outerSeg])
+      return false;
+    return t3PassRZ(m, md, lm1, lm2, lm3, s.mdIndices[2 * innerSeg], s.mdIndices[2 * outerSeg],
+                    s.mdIndices[2 * outerSeg + 1]);
+  }
+
   // SDL/Triplet.h:797-870
   LST_HD bool t3Select(const Modules& m,
                        const MiniDoublets& md,
