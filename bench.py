@@ -359,21 +359,39 @@ def run_ours(args, rank, world, local, events):
                   "cut_only": t5dnn.metrics(probe["cut"] != 0, lab)}
     eset.upload_packed(0, blob, offsets)
     k_m = max(2, args.steps // 2)
+    from tracklooper_b200 import performance
+
+    def tc_level():
+        # track-candidate efficiency / fake / duplicate rates of the slots'
+        # current outputs (the reference's definitions, performance.py)
+        eset.sync()
+        return performance.combine([performance.from_store(lambda f, i=i: eset.field(i, f), events[i])
+                                    for i in range(B)])
+
     ms_ref, _, _ = timed(batched_step, k_m)
+    tc_ref = tc_level()
     es.set_t5dnn_weights(w_new)
     es.set_t5dnn_threshold(wp_new)
     batched_step()
     ms_new, _, _ = timed(batched_step, k_m)
+    tc_new = tc_level()
     es.set_t5dnn_weights(t5dnn.reference_weights())
     es.set_t5dnn_threshold(t5dnn.REFERENCE_WP)
     eset.set_t5_method(lst.T5_CUTS)
     batched_step()
     ms_cut, _, _ = timed(batched_step, k_m)
+    tc_cut = tc_level()
     eset.set_t5_method(lst.T5_DNN)
-    for key, ms_ in (("reference_dnn", ms_ref), ("retrained_dnn", ms_new), ("cut_only", ms_cut)):
+    for key, ms_, tc in (("reference_dnn", ms_ref, tc_ref), ("retrained_dnn", ms_new, tc_new),
+                         ("cut_only", ms_cut, tc_cut)):
         classifier[key]["events_per_s"] = B * world * k_m / (ms_ * 1e-3)
+        classifier[key]["track_candidates"] = {
+            "fake_rate": tc["fake_rate"], "duplicate_rate": tc["duplicate_rate"],
+            "efficiency_hard": tc["hard"]["efficiency"], "efficiency_pileup": tc["pileup"]["efficiency"],
+            "t5_tc": tc["by_type"]["T5"]["tc"], "t5_tc_fake_rate": tc["by_type"]["T5"]["fake_rate"]}
     classifier["retrained_working_point"] = wp_new
-    classifier["level"] = "quintuplet candidates reaching the classifier decision, this step's events"
+    classifier["level"] = ("quintuplet candidates reaching the classifier decision, this step's events; "
+                           "track_candidates: the final track candidates (pT > 1 GeV, |eta| < 2.4 particles)")
 
     tot = sum(v[1] for v in prof.values())
     top = sorted(prof.items(), key=lambda kv: -kv[1][1])

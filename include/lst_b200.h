@@ -95,6 +95,8 @@ typedef struct lst_es_info {
   uint32_t nTotalSegments; /* LS arena length per event (incl. 50000 pLS) */
   uint32_t maxTriplets;    /* T3 arena length per event */
   uint32_t maxQuintuplets; /* T5 arena length per event */
+  float ptCut;             /* pt cut (GeV) of the module maps: from the geometry directory's
+                              "_pt<x>" suffix, 0.8 without one (SDL/Constants.h:102-105) */
 } lst_es_info;
 
 /* Last error message of the calling thread (empty if none). */

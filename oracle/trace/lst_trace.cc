@@ -305,7 +305,7 @@ namespace {
     if (mi < 0)
       return -1;
     S.hmod[i] = uint16_t(mi);
-    S.slope[i] = lst::mdMiniSlope(rt);
+    S.slope[i] = lst::mdMiniSlope(rt, m.ptCut);
     if (mi != H.es.pixelModuleIndex) {
       const bool isLowerHit = m.isLower[mi];
       const uint16_t lm = isLowerHit ? uint16_t(mi) : m.partnerModuleIndices[mi];
@@ -354,7 +354,7 @@ namespace {
                          S.zs[upper], S.rts[upper], S.phis[lower], S.phis[upper], pre, unsigned(lower), unsigned(upper), v);
     const int idx = nMD++;
     lst::storeMD(m, S.h, S.md, unsigned(lower), unsigned(upper), lm, v, unsigned(idx));
-    lst::storeMDDerived(S.md, unsigned(idx));
+    lst::storeMDDerived(S.md, unsigned(idx), H.m.ptCut);
     return idx;
   }
 
@@ -464,8 +464,8 @@ namespace {
     S.rg.segmentModuleIndices[pix] = kPlsSeg;
     lst::storePixelSegment(H.m, S.h, S.md, S.s, pix, kPlsMD, kPlsSeg, 0, unsigned(lh[0]), unsigned(lh[1]),
                            unsigned(lh[2]), unsigned(lh[3]), TFloat(in.dPhiChange[p]));
-    lst::storeMDDerived(S.md, kPlsMD);
-    lst::storeMDDerived(S.md, kPlsMD + 1);
+    lst::storeMDDerived(S.md, kPlsMD, H.m.ptCut);
+    lst::storeMDDerived(S.md, kPlsMD + 1, H.m.ptCut);
     return true;
   }
 
@@ -522,6 +522,7 @@ void* lsttr_create(const char* geometry_dir, const float* dnn_weights, float dnn
   m.nEndCapMap = unsigned(e.geoMapDetId.size());
   m.nModules = e.nModules;
   m.nLowerModules = e.nLowerModules;
+  m.ptCut = TFloat(e.ptCut);
   TFloat* w = reinterpret_cast<TFloat*>(&H->dnn);
   static_assert(sizeof(lst::T5DnnWeights) == lst::kT5DnnParams * sizeof(TFloat), "TFloat weight layout");
   for (int i = 0; i < lst::kT5DnnParams; ++i)

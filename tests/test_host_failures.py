@@ -87,14 +87,14 @@ def test_truncated_connection_map_loads_complete_records(tmp_path):
 
 
 def test_connection_map_with_too_many_connections(tmp_path):
-    """More than 40 connected modules (SDL/Constants.h:107) is an error, not
-    an overrun of the 40-slot module map."""
+    """More connected modules than a module-map row holds (80) is an error,
+    not an overrun of the row."""
     d = _copy_geometry(tmp_path)
     det = struct.unpack_from("<I", open(d / "sensor_centroids.bin", "rb").read(), 0)[0]
     with open(d / "module_connection_tracing_merged.bin", "ab") as f:
-        f.write(struct.pack("<II", det, 41) + struct.pack("<41I", *([det] * 41)))
+        f.write(struct.pack("<II", det, 81) + struct.pack("<81I", *([det] * 81)))
     rc, msg = _load_host(d)
-    assert rc < 0 and "40" in msg
+    assert rc < 0 and "more than 80 connected modules" in msg
 
 
 def test_corrupt_pixel_map_detid(tmp_path):

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <fstream>
 #include <map>
 
@@ -122,7 +123,25 @@ namespace lst {
     }
   }
 
+  // The pt cut a geometry directory is built for: the number after the last
+  // "_pt" of its name (OT800_IT615_pt0.6 -> 0.6), 0.8 when there is none.
+  float geometryPtCut(const std::string& dir) {
+    std::string name = dir;
+    while (!name.empty() && name.back() == '/')
+      name.pop_back();
+    const size_t slash = name.find_last_of('/');
+    if (slash != std::string::npos)
+      name = name.substr(slash + 1);
+    const size_t at = name.rfind("_pt");
+    if (at == std::string::npos)
+      return 0.8f;
+    char* end = nullptr;
+    const float v = std::strtof(name.c_str() + at + 3, &end);
+    return (end != name.c_str() + at + 3 && v > 0.f) ? v : 0.8f;
+  }
+
   std::string loadEsHost(const std::string& dir, EsHost& es) {
+    es.ptCut = geometryPtCut(dir);
     std::vector<CentroidRec> cents;
     if (!readRecords(dir + "/sensor_centroids.bin", cents) || cents.empty())
       return "unable to read " + dir + "/sensor_centroids.bin";
@@ -311,6 +330,9 @@ namespace lst {
         }
         auto& idxv = c == 0 ? es.connectedPixelsIndex : (c == 1 ? es.connectedPixelsIndexPos : es.connectedPixelsIndexNeg);
         auto& sizev = c == 0 ? es.connectedPixelsSizes : (c == 1 ? es.connectedPixelsSizesPos : es.connectedPixelsSizesNeg);
+        if (sizes > kMaxConnectedModules)
+          return "pixel map lists more than " + std::to_string(kMaxConnectedModules) + " modules for superbin " +
+                 std::to_string(sb);
         idxv[sb] = totals[c];
         sizev[sb] = sizes;
         totals[c] += sizes;
@@ -336,7 +358,8 @@ namespace lst {
       if (it == connections.end())
         continue;
       if (it->second.size() > kMaxConnectedModules)
-        return "more than 40 connected modules for detId " + std::to_string(detId);
+        return "more than " + std::to_string(kMaxConnectedModules) + " connected modules for detId " +
+               std::to_string(detId);
       es.nConnectedModules[idx] = static_cast<uint16_t>(it->second.size());
       for (size_t i = 0; i < it->second.size(); ++i) {
         uint16_t mi;

@@ -14,6 +14,9 @@ namespace lst {
     uint16_t nLowerModules = 0;
     uint16_t pixelModuleIndex = 0;
     unsigned int nPixels = 0;  // length of connectedPixels
+    // pt cut of the module and pixel maps: from the directory name's "_pt<x>"
+    // suffix (OT800_IT615_pt0.6 -> 0.6), 0.8 without one
+    float ptCut = 0.8f;
 
     // module arrays (index = re-assigned module index)
     std::vector<unsigned int> detIds;

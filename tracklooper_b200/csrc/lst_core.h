@@ -43,7 +43,13 @@ namespace lst {
 
   // ------------------------------------------------------------- capacities
   // SDL/Constants.h:107-121.
-  constexpr unsigned int kMaxConnectedModules = 40;
+  // Connected modules per module in the module map, and pixel-map modules per
+  // pLS superbin.  The reference's rows hold 40 (SDL/Constants.h:107), which
+  // the pt0.8 maps fill at most; the pt0.6 maps list up to 68 for 1328
+  // modules, more than the reference's rows hold (SDL/ModuleMethods.h:127-134
+  // would write past them), so the rows here hold 80.  Row length changes no
+  // object of the pt0.8 geometry.
+  constexpr unsigned int kMaxConnectedModules = 80;
   constexpr unsigned int kMaxPixelSegments = 50000;
   constexpr unsigned int kMaxPixelMDs = 2 * kMaxPixelSegments;
   constexpr unsigned int kMaxPixelTriplets = 5000;
@@ -58,6 +64,9 @@ namespace lst {
   constexpr float k2Rinv1GeVf = (2.99792458e-3 * 3.8) / 2;
   constexpr float kR1GeVf = 1. / (2.99792458e-3 * 3.8);
   constexpr float kSinAlphaMax = 0.95;
+  // The transverse-momentum cut the module and pixel maps are built for
+  // (SDL/Constants.h:102-105 sets it at compile time, PT_CUT, default 0.8
+  // GeV); here it is a property of the loaded geometry, Modules::ptCut.
   constexpr float kPtCut = 0.8f;
   constexpr float kDeltaZLum = 15.0;
   constexpr float kPixelPSZpitch = 0.15;
@@ -209,6 +218,7 @@ namespace lst {
     unsigned int nEndCapMap;
     uint16_t nModules;
     uint16_t nLowerModules;
+    float ptCut;  // the geometry's pt cut (GeV): 0.8 for OT800_IT615_pt0.8, 0.6 for _pt0.6
   };
 
   struct Hits {

@@ -247,6 +247,7 @@ namespace {
     m.nEndCapMap = static_cast<unsigned int>(h.geoMapDetId.size());
     m.nModules = h.nModules;
     m.nLowerModules = h.nLowerModules;
+    m.ptCut = h.ptCut;
     d.cpIndex = upload(c, h.connectedPixelsIndex, copies, sizes);
     d.cpSizes = upload(c, h.connectedPixelsSizes, copies, sizes);
     d.cpIndexPos = upload(c, h.connectedPixelsIndexPos, copies, sizes);
@@ -897,6 +898,7 @@ int lst_es_get_info(const lst_es* es, lst_es_info* out) {
   out->nTotalSegments = es->host.nTotalSegments;
   out->maxTriplets = es->host.maxTriplets;
   out->maxQuintuplets = es->host.maxQuintuplets;
+  out->ptCut = es->host.ptCut;
   return 0;
   LST_ABI_CATCH_INT
 }

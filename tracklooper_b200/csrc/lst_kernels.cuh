@@ -228,7 +228,7 @@ namespace lst {
       // Per-hit parts of the mini-doublet cuts of the module pair this hit
       // belongs to (lower module lm): the dphi-threshold slope, and the strip
       // shift of the hit it moves (tilted barrel and endcap modules).
-      ev.hitMiniSlope[ihit] = mdMiniSlope(rt);
+      ev.hitMiniSlope[ihit] = mdMiniSlope(rt, m.ptCut);
       if (mi != es.pixelModule) {
         const bool isLowerHit = m.isLower[mi];
         const uint16_t lm = isLowerHit ? mi : m.partnerModuleIndices[mi];
@@ -498,13 +498,13 @@ namespace lst {
         const unsigned int ownerN = __shfl_sync(kFullMask, n, owner);
         const unsigned int ownerBase = __shfl_sync(kFullMask, base, owner);
         if (f < total)
-          storeMDDerived(md, ownerBase + (f - (ownerIncl - ownerN)));
+          storeMDDerived(md, ownerBase + (f - (ownerIncl - ownerN)), es.m.ptCut);
       }
     }
     const unsigned int nPix = md.nMDs[es.nLowerModules];
     const unsigned int pixBase = es.mdOffset[es.nLowerModules];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < nPix; k += gridDim.x * blockDim.x)
-      storeMDDerived(md, pixBase + k);
+      storeMDDerived(md, pixBase + k, es.m.ptCut);
   }
 
   // SDL/MiniDoublet.h:1084-1104
@@ -525,67 +525,8 @@ namespace lst {
   // One warp per inner lower module walking (connected module, inner MD,
   // outer MD) in order (SDL/Segment.h:798-910).
   constexpr int kLSWarps = 4;
-  // One warp per inner module (SDL/Segment.h:798-885): the candidates are
-  // (connected module, inner MD, outer MD) in the reference's loop order,
-  // 32 per step.  Most fail the cheap window and dPhi tests that open the
-  // selection (lsPrefilter, the same code), so a step first runs only those;
-  // the survivors join a per-warp queue in shared memory in candidate order,
-  // and each time 32 are waiting the warp runs the full selection on them
-  // with every lane busy.  The queue is first in, first out, so the passing
-  // candidates are ranked in the reference's order.
-  // Walks candidates 0 .. total-1 of one warp in steps of 32: prefilter(f)
-  // runs the cheap opening tests of candidate f (every lane), the survivors
-  // wait in `queue` (64 entries of warp-private shared memory) in candidate
-  // order, and whenever 32 wait, select(n) runs the full selection on the
-  // first n of them (queue[lane] for lane < n) with every lane busy; the rest
-  // are drained at the end.  First in, first out: select sees the survivors
-  // in candidate order, so ranks taken in select follow the reference's loop
-  // order.
-  constexpr int kCandQueue = 64;
-  template <typename Prefilter, typename Select>
-  __device__ __forceinline__ void orderedQueueWalk(unsigned int total, unsigned int* queue, Prefilter prefilter,
-                                                   Select select) {
-    unsigned int queued = 0;  // the same in every lane
-    for (unsigned int start = 0; start < total; start += 32) {
-      const unsigned int f = start + laneId();
-      const bool pass = f < total && prefilter(f);
-      unsigned int tot;
-      const unsigned int r = warpRank(pass, tot);
-      if (pass)
-        queue[queued + r] = f;
-      queued += tot;
-      __syncwarp();
-      if (queued >= 32) {
-        select(32u);
-        __syncwarp();
-        const unsigned int left = queued - 32;
-        const unsigned int keep = laneId() < left ? queue[32 + laneId()] : 0u;
-        __syncwarp();
-        if (laneId() < left)
-          queue[laneId()] = keep;
-        queued = left;
-        __syncwarp();
-      }
-    }
-    if (queued > 0)
-      select(queued);
-    __syncwarp();
-  }
-
-  constexpr int kLSQueue = kCandQueue;
-  __device__ __forceinline__ void lsDecode(DeviceES const& es, const EventView& ev, const unsigned int* pre,
-                                          const uint16_t* outer, int nConn, unsigned int innerBase, unsigned int f,
-                                          uint16_t& outerLM, unsigned int& innerMD, unsigned int& outerMD) {
-    const int k = findSlot(pre, nConn, f);
-    outerLM = outer[k];
-    const unsigned int nOuterMDs = ev.md.nMDs[outerLM];
-    const unsigned int local = f - pre[k];
-    innerMD = innerBase + local / nOuterMDs;
-    outerMD = es.mdOffset[outerLM] + local % nOuterMDs;
-  }
-
-  __device__ __forceinline__ void lsModule(DeviceES const& es, const EventView& ev, uint16_t lm, unsigned int* pre,
-                                           uint16_t* outer, unsigned int* queue) {
+  __device__ __forceinline__ void lsModule(
+      DeviceES const& es, const EventView& ev, uint16_t lm, unsigned int* pre, uint16_t* outer) {
     const unsigned int nInnerMDs = ev.md.nMDs[lm];
     if (nInnerMDs == 0)
       return;
@@ -601,29 +542,27 @@ namespace lst {
     const unsigned int innerBase = es.mdOffset[lm];
     Segments ls = ev.ls;
     unsigned int count = 0;
-    orderedQueueWalk(
-        total, queue,
-        [&](unsigned int f) {
-          uint16_t outerLM;
-          unsigned int innerMD, outerMD;
-          lsDecode(es, ev, pre, outer, nConn, innerBase, f, outerLM, innerMD, outerMD);
-          return lsPrefilter(m, ev.md, lm, outerLM, innerMD, outerMD);
-        },
-        [&](unsigned int n) {
-          bool ok = false;
-          LSValues v;
-          unsigned int innerMD = 0, outerMD = 0;
-          uint16_t outerLM = 0;
-          if (laneId() < n) {
-            lsDecode(es, ev, pre, outer, nConn, innerBase, queue[laneId()], outerLM, innerMD, outerMD);
-            ok = lsSelect(m, ev.md, lm, outerLM, innerMD, outerMD, v);
-          }
-          unsigned int tot;
-          const unsigned int r = count + warpRank(ok, tot);
-          if (ok && int(r) < cap)
-            storeLS(ls, ev.md, innerMD, outerMD, lm, outerLM, v, base + r);
-          count += tot;
-        });
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      LSValues v;
+      unsigned int innerMD = 0, outerMD = 0;
+      uint16_t outerLM = 0;
+      if (f < total) {
+        int k = findSlot(pre, nConn, f);
+        outerLM = outer[k];
+        unsigned int nOuterMDs = ev.md.nMDs[outerLM];
+        unsigned int local = f - pre[k];
+        innerMD = innerBase + local / nOuterMDs;
+        outerMD = es.mdOffset[outerLM] + local % nOuterMDs;
+        ok = lsSelect(m, ev.md, lm, outerLM, innerMD, outerMD, v);
+      }
+      unsigned int tot;
+      unsigned int r = count + warpRank(ok, tot);
+      if (ok && int(r) < cap)
+        storeLS(ls, ev.md, innerMD, outerMD, lm, outerLM, v, base + r);
+      count += tot;
+    }
     if (laneId() == 0) {
       ls.nSegments[lm] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
       ls.totOccupancySegments[lm] = count;
@@ -635,13 +574,12 @@ namespace lst {
   __global__ void __launch_bounds__(LST_LB_LS) kCreateLS(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kLSWarps][kMaxConnectedModules + 1];
     __shared__ uint16_t sOuter[kLSWarps][kMaxConnectedModules];
-    __shared__ unsigned int sQueue[kLSWarps][kLSQueue];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;  // at most kLSWarps
     for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
       __syncwarp();
-      lsModule(es, ev, static_cast<uint16_t>(w), sPre[wib], sOuter[wib], sQueue[wib]);
+      lsModule(es, ev, static_cast<uint16_t>(w), sPre[wib], sOuter[wib]);
     }
   }
 
@@ -936,8 +874,7 @@ namespace lst {
   // segment of the middle module) in order (SDL/Triplet.h:874-1005).
   constexpr int kT3Warps = 4;
   constexpr int kT3MaxInner = 1024;
-  __device__ __forceinline__ void t3Module(DeviceES const& es, const EventView& ev, uint16_t lm1, unsigned int* pre,
-                                           unsigned int* queue) {
+  __device__ __forceinline__ void t3Module(DeviceES const& es, const EventView& ev, uint16_t lm1, unsigned int* pre) {
     const Modules& m = es.m;
     if (m.nConnectedModules[lm1] == 0)
       return;
@@ -960,40 +897,28 @@ namespace lst {
     const unsigned int base = ev.rg.tripletModuleIndices[lm1];
     Triplets t3 = ev.t3;
     unsigned int count = 0;
-    // candidate f: (inner segment, outer segment sharing its outer MD)
-    auto decode = [&](unsigned int f, unsigned int& innerSeg, unsigned int& outerSeg, uint16_t& middle,
-                      uint16_t& outerOuter) {
-      const int i = findSlot(pre, int(nInner), f);
-      innerSeg = segBase + i;
-      middle = ls.outerLowerModuleIndices[innerSeg];
-      const unsigned int mdMid = ls.mdIndices[2 * innerSeg + 1];
-      const unsigned int outerBase = es.lsOffset[middle];
-      outerSeg = outerBase + ev.lsByMD[outerBase + ev.mdLSStart[mdMid] + (f - pre[i])];
-      outerOuter = ls.outerLowerModuleIndices[outerSeg];
-    };
-    orderedQueueWalk(
-        total, queue,
-        [&](unsigned int f) {
-          unsigned int innerSeg, outerSeg;
-          uint16_t middle, outerOuter;
-          decode(f, innerSeg, outerSeg, middle, outerOuter);
-          return t3Prefilter(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg);
-        },
-        [&](unsigned int n) {
-          bool ok = false;
-          T3Values v;
-          unsigned int innerSeg = 0, outerSeg = 0;
-          uint16_t middle = 0, outerOuter = 0;
-          if (laneId() < n) {
-            decode(queue[laneId()], innerSeg, outerSeg, middle, outerOuter);
-            ok = t3Select(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg, v);
-          }
-          unsigned int tot;
-          const unsigned int r = count + warpRank(ok, tot);
-          if (ok && int(r) < cap)
-            storeT3(m, ev.md, ls, t3, innerSeg, outerSeg, lm1, middle, outerOuter, v, base + r);
-          count += tot;
-        });
+    for (unsigned int start = 0; start < total; start += 32) {
+      unsigned int f = start + laneId();
+      bool ok = false;
+      T3Values v;
+      unsigned int innerSeg = 0, outerSeg = 0;
+      uint16_t middle = 0, outerOuter = 0;
+      if (f < total) {
+        int i = findSlot(pre, int(nInner), f);
+        innerSeg = segBase + i;
+        middle = ls.outerLowerModuleIndices[innerSeg];
+        const unsigned int mdMid = ls.mdIndices[2 * innerSeg + 1];
+        const unsigned int outerBase = es.lsOffset[middle];
+        outerSeg = outerBase + ev.lsByMD[outerBase + ev.mdLSStart[mdMid] + (f - pre[i])];
+        outerOuter = ls.outerLowerModuleIndices[outerSeg];
+        ok = t3Select(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg, v);
+      }
+      unsigned int tot;
+      unsigned int r = count + warpRank(ok, tot);
+      if (ok && int(r) < cap)
+        storeT3(m, ev.md, ls, t3, innerSeg, outerSeg, lm1, middle, outerOuter, v, base + r);
+      count += tot;
+    }
     if (laneId() == 0) {
       t3.nTriplets[lm1] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
       t3.totOccupancyTriplets[lm1] = count;
@@ -1004,13 +929,12 @@ namespace lst {
 
   __global__ void __launch_bounds__(LST_LB_T3) kCreateT3(DeviceES es, const EventView* evs) {
     __shared__ unsigned int sPre[kT3Warps][kT3MaxInner + 1];
-    __shared__ unsigned int sQueue[kT3Warps][kCandQueue];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;  // at most kT3Warps
     for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
       __syncwarp();
-      t3Module(es, ev, static_cast<uint16_t>(w), sPre[wib], sQueue[wib]);
+      t3Module(es, ev, static_cast<uint16_t>(w), sPre[wib]);
     }
   }
 
@@ -1300,6 +1224,19 @@ namespace lst {
     }
   }
 
+  // Candidates of one block tile that reached the classifier, kept in shared
+  // memory until the tile's DNN pass (kT5Eval).
+  constexpr int kT5DnnTile = 64;
+  struct T5DnnSlot {
+    float feat[38];
+    T5Values v;
+    unsigned int mdIdx[5];
+    unsigned int cand;
+    float score;
+    uint16_t lm[5];
+    uint8_t tight;
+  };
+
   // t5DnnForward (SDL/NeuralNetwork.h:21-165) evaluated by one warp for one
   // candidate: lane j computes hidden unit j of each layer, summing its
   // inputs in the same order as the serial loops, so the score is
@@ -1339,19 +1276,21 @@ namespace lst {
   }
 
   // The T5 selection of the queued candidates, with the DNN classifier fused
-  // in (SDL/Quintuplet.h:2921-2941 evaluates it inline).  A warp takes 32
-  // candidates at a time, one per lane, and runs every test before the
-  // classifier; a lane whose candidate reaches the classifier leaves its 38
-  // DNN inputs in its row of the warp's shared-memory block.  The warp then
-  // classifies those candidates one after the other, a lane per hidden unit
-  // with the weights in shared memory (t5DnnForwardWarp), so the classifier
-  // runs on full warps although only a few candidates of a step reach it;
-  // each lane then finishes its own candidate.  Only warp barriers: the
-  // warps of a block do not wait for one another.
-  constexpr int kT5EvalWarps = 4;  // warps per block the kernel is launched with (at most)
+  // in (SDL/Quintuplet.h:2921-2941 evaluates it inline).  The block takes its
+  // candidates in tiles of blockDim.  Each thread runs every test before the
+  // classifier on one candidate; those that reach it leave their 38 DNN
+  // inputs and selection values in shared memory.  After a barrier each warp
+  // classifies the tile's waiting candidates one at a time, a lane per hidden
+  // unit, with the weights in shared memory (t5DnnForwardWarp); after a
+  // second, each thread finishes one classified candidate.  So the
+  // classifier runs on full warps although only some candidates of a warp
+  // reach it, and nothing goes through global memory.  A candidate that finds
+  // the tile's slots full is classified by its own thread at once; the
+  // arithmetic is the same in every case.
   __global__ void __launch_bounds__(LST_LB_T5EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
     __shared__ T5DnnWeights sW;
-    __shared__ float sFeat[kT5EvalWarps][32][38];
+    __shared__ T5DnnSlot sSlot[kT5DnnTile];
+    __shared__ unsigned int sCount;
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow)
       return;
@@ -1360,63 +1299,72 @@ namespace lst {
       float* dst = reinterpret_cast<float*>(&sW);
       for (int i = threadIdx.x; i < kT5DnnParams; i += blockDim.x)
         dst[i] = src[i];
-      __syncthreads();
     }
     const float wp = c_t5dnnWP;
     const unsigned int total = ev.sc->t5CandTotal;
     const unsigned int front = ev.sc->t5QueueCount, back = ev.sc->t5QueueBack;
     const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
     const unsigned int n = fromQueue ? front + back : total;
-    const unsigned int warp = threadIdx.x >> 5, lane = laneId();
-    const unsigned int nWarpsAll = gridDim.x * (blockDim.x >> 5);
-    float* feat = sFeat[warp][lane];
-    // warp-uniform loop: every lane of a warp runs the same steps
-    for (unsigned int step = blockIdx.x * (blockDim.x >> 5) + warp; step * 32u < n; step += nWarpsAll) {
-      const unsigned int q = step * 32u + lane;
-      bool atClassifier = false;
-      unsigned int c = 0;
-      uint16_t lm[5];
-      unsigned int innerT3 = 0, outerT3 = 0;
-      T5Values v;
-      T5Stage st;
+    const unsigned int tileStride = gridDim.x * blockDim.x;
+    const unsigned int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    // every thread of the block runs the same number of tiles (barriers inside)
+    for (unsigned int tile = blockIdx.x * blockDim.x; tile < n; tile += tileStride) {
+      if (threadIdx.x == 0)
+        sCount = 0;
+      __syncthreads();
+      const unsigned int q = tile + threadIdx.x;
       if (q < n) {
-        c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
+        const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
+        unsigned int innerT3, outerT3;
+        uint16_t lm[5];
         t5Decode(ev, c, innerT3, outerT3, lm);
+        T5Values v;
+        T5Stage st;
         if (!t5SelectPre(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st)) {
           ev.t5CandFlag[c] = 0;
-        } else if (!useDnn) {
-          if (t5Classify(es.m, ev.md, ev.ls, ev.t3, sW, false, wp, lm, innerT3, v, st))
+        } else {
+          const unsigned int k = useDnn ? atomicAdd(&sCount, 1u) : unsigned(kT5DnnTile);
+          if (k < unsigned(kT5DnnTile)) {
+            T5DnnSlot& sl = sSlot[k];
+            t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius,
+                          v.outerRadius, v.bridgeRadius, sl.feat);
+            sl.v = v;
+            for (int i = 0; i < 5; ++i) {
+              sl.mdIdx[i] = st.mdIdx[i];
+              sl.lm[i] = lm[i];
+            }
+            sl.cand = c;
+            sl.tight = st.tight ? 1 : 0;
+          } else if (t5Classify(es.m, ev.md, ev.ls, ev.t3, sW, useDnn, wp, lm, innerT3, v, st)) {
             t5Keep(ev, c, v);
-          else
+          } else {
             ev.t5CandFlag[c] = 0;
-        } else {
-          t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius,
-                        v.outerRadius, v.bridgeRadius, feat);
-          atClassifier = true;
+          }
         }
       }
-      unsigned int waiting = __ballot_sync(kFullMask, atClassifier);
-      if (waiting == 0u)
-        continue;
-      __syncwarp();
-      float myScore = 0.f;
-      while (waiting) {
-        const int owner = __ffs(waiting) - 1;
-        waiting &= waiting - 1;
-        const float score = t5DnnForwardWarp(sW, sFeat[warp][owner]);
-        if (int(lane) == owner)
-          myScore = score;
+      __syncthreads();
+      const unsigned int m = sCount < unsigned(kT5DnnTile) ? sCount : unsigned(kT5DnnTile);
+      if (m == 0)
+        continue;  // uniform over the block: no candidate of the tile waits
+      for (unsigned int k = warp; k < m; k += nWarps) {
+        const float score = t5DnnForwardWarp(sW, sSlot[k].feat);
+        if (laneId() == 0)
+          sSlot[k].score = score;
       }
-      if (atClassifier) {
-        if (!(myScore > wp)) {
-          ev.t5CandFlag[c] = 0;
-        } else {
-          t5NonAnchor(es.m, ev.md, lm, st.mdIdx, v);
-          v.tightCutFlag = st.tight and (myScore > wp);
-          t5Keep(ev, c, v);
+      __syncthreads();
+      for (unsigned int k = threadIdx.x; k < m; k += blockDim.x) {
+        const T5DnnSlot& sl = sSlot[k];
+        const float inference = sl.score;
+        if (!(inference > wp)) {
+          ev.t5CandFlag[sl.cand] = 0;
+          continue;
         }
+        T5Values v = sl.v;
+        t5NonAnchor(es.m, ev.md, sl.lm, sl.mdIdx, v);
+        v.tightCutFlag = sl.tight != 0 and (inference > wp);
+        t5Keep(ev, sl.cand, v);
       }
-      __syncwarp();
+      __syncthreads();
     }
   }
 

@@ -26,10 +26,10 @@ namespace lst {
                                  float* thr) {
     const bool innerBarrel = m.subdets[innerLM] == Barrel;
     const bool outerBarrel = m.subdets[outerLM] == Barrel;
-    float sdMuls = innerBarrel ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / kPtCut
-                               : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / kPtCut;
+    float sdMuls = innerBarrel ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / m.ptCut
+                               : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / m.ptCut;
     float segmentDr = fsqrt((yOut - yIn) * (yOut - yIn) + (xOut - xIn) * (xOut - xIn));
-    const float dAlpha_Bfield = fasin(fmin_(segmentDr * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    const float dAlpha_Bfield = fasin(fmin_(segmentDr * k2Rinv1GeVf / m.ptCut, kSinAlphaMax));
     bool isInnerTilted = innerBarrel and m.sides[innerLM] != Center;
     bool isOuterTilted = outerBarrel and m.sides[outerLM] != Center;
     const float drdzInner = m.drdzs[innerLM];
@@ -74,28 +74,20 @@ namespace lst {
     float dPhi, dPhiMin, dPhiMax, dPhiChange, dPhiChangeMin, dPhiChangeMax;
   };
 
-  // The anchor positions and the dPhi cut of a segment candidate, computed
-  // by its first tests (lsBarrelWindow / lsEndcapWindow) for the rest.
-  struct LSWindow {
-    MDPos in, out;
-    float sdCut;
-  };
-
-  // The first tests of a barrel-barrel segment (SDL/Segment.h:455-500): the
-  // z window and the dPhi cut.  Cheap: no transcendental function.
-  LST_HD bool lsBarrelWindow(const Modules& m,
-                             const MiniDoublets& md,
-                             uint16_t innerLM,
-                             unsigned int innerMD,
-                             unsigned int outerMD,
-                             LSValues& v,
-                             LSWindow& w) {
-    float sdMuls = (m.subdets[innerLM] == Barrel) ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / kPtCut
-                                                  : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / kPtCut;
-    w.in = md.anchorPos[innerMD];
-    w.out = md.anchorPos[outerMD];
-    float zIn = w.in.z, rtIn = w.in.rt;
-    float zOut = w.out.z, rtOut = w.out.rt;
+  // Barrel-barrel segment (SDL/Segment.h:455-565).  dPhiMin/Max and
+  // dPhiChangeMin/Max keep their initial value 0.
+  LST_HD_BIG bool lsBarrel(const Modules& m,
+                       const MiniDoublets& md,
+                       uint16_t innerLM,
+                       uint16_t outerLM,
+                       unsigned int innerMD,
+                       unsigned int outerMD,
+                       LSValues& v) {
+    float sdMuls = (m.subdets[innerLM] == Barrel) ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / m.ptCut
+                                                  : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / m.ptCut;
+    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
+    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
+    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
 
     float sdSlope = md.slope[outerMD];
     float sdPVoff = 0.1f / rtOut;
@@ -106,27 +98,12 @@ namespace lst {
     if (!((zOut >= zLo) && (zOut <= zHi)))
       return false;
 
-    w.sdCut = sdSlope + fsqrt(sdMuls * sdMuls + sdPVoff * sdPVoff);
+    float sdCut = sdSlope + fsqrt(sdMuls * sdMuls + sdPVoff * sdPVoff);
     v.dPhi = phiMpiPi(md.anchorPhi[outerMD] - md.anchorPhi[innerMD]);
-    return fabs_(v.dPhi) <= w.sdCut;
-  }
-
-  // Barrel-barrel segment (SDL/Segment.h:455-565).  dPhiMin/Max and
-  // dPhiChangeMin/Max keep their initial value 0.
-  LST_HD_BIG bool lsBarrel(const Modules& m,
-                       const MiniDoublets& md,
-                       uint16_t innerLM,
-                       uint16_t outerLM,
-                       unsigned int innerMD,
-                       unsigned int outerMD,
-                       LSValues& v) {
-    LSWindow w;
-    if (!lsBarrelWindow(m, md, innerLM, innerMD, outerMD, v, w))
+    if (!(fabs_(v.dPhi) <= sdCut))
       return false;
-    float xIn = w.in.x, yIn = w.in.y, zIn = w.in.z, rtIn = w.in.rt;
-    float xOut = w.out.x, yOut = w.out.y, zOut = w.out.z, rtOut = w.out.rt;
     v.dPhiChange = phiMpiPi(phiOf(xOut - xIn, yOut - yIn) - md.anchorPhi[innerMD]);
-    if (!(fabs_(v.dPhiChange) <= w.sdCut))
+    if (!(fabs_(v.dPhiChange) <= sdCut))
       return false;
 
     float thr[3];
@@ -143,20 +120,17 @@ namespace lst {
     return fabs_(dAlphaInnerMDOuterMD) < thr[2];
   }
 
-  // The first tests of a segment with an endcap module (SDL/Segment.h:
-  // 567-660): z signs, the rt window, dPhi and dPhiChange.  Cheap: no
-  // transcendental function.
-  LST_HD bool lsEndcapWindow(const Modules& m,
-                             const MiniDoublets& md,
-                             uint16_t outerLM,
-                             unsigned int innerMD,
-                             unsigned int outerMD,
-                             LSValues& v,
-                             LSWindow& w) {
-    w.in = md.anchorPos[innerMD];
-    w.out = md.anchorPos[outerMD];
-    float zIn = w.in.z, rtIn = w.in.rt;
-    float zOut = w.out.z, rtOut = w.out.rt;
+  // Segment with at least one endcap module (SDL/Segment.h:567-705).
+  LST_HD_BIG bool lsEndcap(const Modules& m,
+                       const MiniDoublets& md,
+                       uint16_t innerLM,
+                       uint16_t outerLM,
+                       unsigned int innerMD,
+                       unsigned int outerMD,
+                       LSValues& v) {
+    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
+    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
+    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
     bool outerLayerEndcapTwoS = (m.subdets[outerLM] == Endcap) && (m.moduleType[outerLM] == TwoS);
     float sdSlope = md.slope[outerMD];
     float disks2SMinRadius = 60.f;
@@ -176,7 +150,6 @@ namespace lst {
 
     v.dPhi = phiMpiPi(md.anchorPhi[outerMD] - md.anchorPhi[innerMD]);
     float sdCut = sdSlope;
-    w.sdCut = sdCut;
     if (outerLayerEndcapTwoS) {
       float dPhiPos_high = phiMpiPi(md.anchorHighEdgePhi[outerMD] - md.anchorPhi[innerMD]);
       float dPhiPos_low = phiMpiPi(md.anchorLowEdgePhi[outerMD] - md.anchorPhi[innerMD]);
@@ -193,22 +166,9 @@ namespace lst {
     v.dPhiChange = v.dPhi / dzFrac * (1.f + dzFrac);
     v.dPhiChangeMin = v.dPhiMin / dzFrac * (1.f + dzFrac);
     v.dPhiChangeMax = v.dPhiMax / dzFrac * (1.f + dzFrac);
-    return fabs_(v.dPhiChange) <= sdCut;
-  }
-
-  // Segment with at least one endcap module (SDL/Segment.h:567-705).
-  LST_HD_BIG bool lsEndcap(const Modules& m,
-                       const MiniDoublets& md,
-                       uint16_t innerLM,
-                       uint16_t outerLM,
-                       unsigned int innerMD,
-                       unsigned int outerMD,
-                       LSValues& v) {
-    LSWindow w;
-    if (!lsEndcapWindow(m, md, outerLM, innerMD, outerMD, v, w))
+    if (!(fabs_(v.dPhiChange) <= sdCut))
       return false;
-    float xIn = w.in.x, yIn = w.in.y, zIn = w.in.z, rtIn = w.in.rt;
-    float xOut = w.out.x, yOut = w.out.y, zOut = w.out.z, rtOut = w.out.rt;
+
     float thr[3];
     lsDAlphaThresholds(m, md, xIn, yIn, zIn, rtIn, xOut, yOut, zOut, rtOut, innerLM, outerLM, innerMD, outerMD, thr);
     float innerMDAlpha = md.dphichanges[innerMD];
@@ -221,21 +181,6 @@ namespace lst {
     if (!(fabs_(dAlphaOuterMDSegment) < thr[1]))
       return false;
     return fabs_(dAlphaInnerMDOuterMD) < thr[2];
-  }
-
-  // The first tests of lsSelect alone (the windows and dPhi cuts): every
-  // candidate lsSelect accepts passes them, evaluated by the same code.
-  LST_HD bool lsPrefilter(const Modules& m,
-                          const MiniDoublets& md,
-                          uint16_t innerLM,
-                          uint16_t outerLM,
-                          unsigned int innerMD,
-                          unsigned int outerMD) {
-    LSValues v;
-    LSWindow w;
-    if (m.subdets[innerLM] == Barrel and m.subdets[outerLM] == Barrel)
-      return lsBarrelWindow(m, md, innerLM, innerMD, outerMD, v, w);
-    return lsEndcapWindow(m, md, outerLM, innerMD, outerMD, v, w);
   }
 
   LST_HD bool lsSelect(const Modules& m,

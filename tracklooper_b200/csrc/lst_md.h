@@ -71,7 +71,7 @@ namespace lst {
   // dPhi acceptance of a mini-doublet (SDL/MiniDoublet.h:340-402).
   // The slope term of mdDPhiThreshold, a function of the hit's rt alone
   // (computed once per hit by kHitPrep).
-  LST_HD float mdMiniSlope(float rt) { return fasin(fmin_(rt * k2Rinv1GeVf / kPtCut, kSinAlphaMax)); }
+  LST_HD float mdMiniSlope(float rt, float ptCut) { return fasin(fmin_(rt * k2Rinv1GeVf / ptCut, kSinAlphaMax)); }
 
   LST_HD float mdDPhiThresholdFromSlope(const Modules& m, float miniSlope, uint16_t mi, float dPhi = 0, float dz = 0) {
     unsigned int iL = m.layers[mi] - 1;
@@ -79,7 +79,7 @@ namespace lst {
     const float rLayNominal = barrel ? miniRminMeanBarrel(iL) : miniRminMeanEndcap(iL);
     const float miniPVoff = 0.1f / rLayNominal;
     const float miniMuls =
-        barrel ? miniMulsPtScaleBarrel(iL) * 3.f / kPtCut : miniMulsPtScaleEndcap(iL) * 3.f / kPtCut;
+        barrel ? miniMulsPtScaleBarrel(iL) * 3.f / m.ptCut : miniMulsPtScaleEndcap(iL) * 3.f / m.ptCut;
     const bool isTilted = barrel and m.sides[mi] != Center;
     float drdz;
     if (isTilted) {
@@ -101,7 +101,7 @@ namespace lst {
   }
 
   LST_HD float mdDPhiThreshold(const Modules& m, float rt, uint16_t mi, float dPhi = 0, float dz = 0) {
-    return mdDPhiThresholdFromSlope(m, mdMiniSlope(rt), mi, dPhi, dz);
+    return mdDPhiThresholdFromSlope(m, mdMiniSlope(rt, m.ptCut), mi, dPhi, dz);
   }
 
   // Moves the strip hit along the strip so that it lines up with the
@@ -198,9 +198,9 @@ namespace lst {
   }
 
   // The derived per-MD values of MiniDoublets (slope, tanSlope, slope3).
-  LST_HD void storeMDDerived(MiniDoublets& md, unsigned int idx) {
+  LST_HD void storeMDDerived(MiniDoublets& md, unsigned int idx, float ptCut) {
     const float rt = md.anchorRt[idx];
-    const float slope = fasin(fmin_(rt * k2Rinv1GeVf / kPtCut, kSinAlphaMax));
+    const float slope = fasin(fmin_(rt * k2Rinv1GeVf / ptCut, kSinAlphaMax));
     md.slope[idx] = slope;
     md.tanSlope[idx] = ftan(slope);
     md.slope3[idx] = fasin(fmin_(rt * k2Rinv1GeVf / 3.0f, kSinAlphaMax));

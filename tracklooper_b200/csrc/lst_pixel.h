@@ -62,7 +62,7 @@ namespace lst {
     const float r3_InUp = fsqrt(z_InUp * z_InUp + rt_InUp * rt_InUp);
     float drt_InSeg = rt_InOut - rt_InLo;
     const float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rt_OutLo - rt_InUp) / 50.f) * fsqrt(r3_InUp / rt_InUp);
-    const float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    const float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     float dzErr = drt_OutLo_InUp * etaErr * coshEta;
     dzErr *= dzErr;
     dzErr += 0.03f * 0.03f;
@@ -150,7 +150,7 @@ namespace lst {
                   sinDPhi / drt_tl_axis;
     }
     const float dBetaROut2 = dBetaROut * dBetaROut;
-    float betaOutCut = fasin(fmin_(drt_tl_axis * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
+    float betaOutCut = fasin(fmin_(drt_tl_axis * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
                        fsqrt(dBetaLum2 + dBetaMuls * dBetaMuls);
     if (!(fabs_(betaOut) < betaOutCut))
       return false;
@@ -208,7 +208,7 @@ namespace lst {
     const float multDzDr = dzOutInAbs * coshEta / (coshEta * coshEta - 1.f);
     const float r3_InUp = fsqrt(z_InUp * z_InUp + rt_InUp * rt_InUp);
     const float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rt_OutLo - rt_InUp) / 50.f) * fsqrt(r3_InUp / rt_InUp);
-    const float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    const float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     float drtErr = etaErr * multDzDr;
     drtErr *= drtErr;
     drtErr += 0.03f * 0.03f;
@@ -297,7 +297,7 @@ namespace lst {
                   sinDPhi / drt_tl_axis;
     }
     const float dBetaROut2 = dBetaROut * dBetaROut;
-    float betaOutCut = fasin(fmin_(drt_tl_axis * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
+    float betaOutCut = fasin(fmin_(drt_tl_axis * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
                        fsqrt(dBetaLum2 + dBetaMuls * dBetaMuls);
     if (!(fabs_(betaOut) < betaOutCut))
       return false;

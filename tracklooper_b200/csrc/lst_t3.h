@@ -92,7 +92,7 @@ namespace lst {
     float coshEta = dr3_InSeg / drt_InSeg;
     float dzErr = (zpitchIn + zpitchOut) * (zpitchIn + zpitchOut) * 2.f;
     float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rtOut - rtIn) / 50.f) * fsqrt(r3In / rtIn);
-    float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     dzErr += sdlMuls * sdlMuls * drt_OutIn * drt_OutIn / 3.f * coshEta * coshEta;
     dzErr = fsqrt(dzErr);
     const float dzMean = dz_InSeg / drt_InSeg * drt_OutIn;
@@ -107,7 +107,7 @@ namespace lst {
     betaIn = alpha_InLo - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
     float drt_tl_axis = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
     const float rt_InSeg = segmentDr(md, md1, md2);
-    float betaInCut = fasin(fmin_((-rt_InSeg + drt_tl_axis) * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / drt_InSeg);
+    float betaInCut = fasin(fmin_((-rt_InSeg + drt_tl_axis) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / drt_InSeg);
     return pass and (fabs_(betaIn) < betaInCut);
   }
 
@@ -160,7 +160,7 @@ namespace lst {
     // The reference evaluates 0.1f + 0.2 * (...) / 50.f in double here.
     const float sdlThetaMulsF =
         0.015f * dsqrt(0.1f + 0.2 * (rtOut - rtIn) / 50.f) * fsqrt(rIn / rtIn);
-    const float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    const float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     drtErr += sdlMuls * sdlMuls * multDzDr * multDzDr / 3.f * coshEta * coshEta;
     drtErr = fsqrt(drtErr);
     bool pass = (kZ >= 0) && (rtOut >= rtLo) && (rtOut <= rtHi);
@@ -181,7 +181,7 @@ namespace lst {
     float sdIn_dr = segmentDr(md, md1, md2);
     float sdIn_d = rt_InOut - rt_InLo;
     float dr = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
-    float betaInCut = fasin(fmin_((-sdIn_dr + dr) * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdIn_d);
+    float betaInCut = fasin(fmin_((-sdIn_dr + dr) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdIn_d);
     return pass and (fabs_(betaInRHmin) < betaInCut);
   }
 
@@ -223,7 +223,7 @@ namespace lst {
     float multDzDr = dzOutInAbs * coshEta / (coshEta * coshEta - 1.f);
     float kZ = (zOut - zIn) / dzSDIn;
     float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rtOut - rtIn) / 50.f);
-    float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     float drtErr = fsqrt(kPixelPSZpitch * kPixelPSZpitch * 2.f / (dzSDIn * dzSDIn) * (dzOutInAbs * dzOutInAbs) +
                          sdlMuls * sdlMuls * multDzDr * multDzDr / 3.f * coshEta * coshEta);
     float drtMean = drtSDIn * dzOutInAbs / fabs_(dzSDIn);
@@ -252,7 +252,7 @@ namespace lst {
     float sdIn_dr = segmentDr(md, md1, md2);
     float sdIn_d = rt_InOut - rt_InLo;
     float dr = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
-    float betaInCut = fasin(fmin_((-sdIn_dr + dr) * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdIn_d);
+    float betaInCut = fasin(fmin_((-sdIn_dr + dr) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdIn_d);
     return pass and (fabs_(betaInRHmin) < betaInCut);
   }
 
@@ -277,22 +277,6 @@ namespace lst {
   struct T3Values {
     float betaIn, circleRadius, circleCenterX, circleCenterY;
   };
-
-  // The opening tests of t3Select alone (the shared mini-doublet and the r-z
-  // residual): every candidate t3Select accepts passes them, by the same code.
-  LST_HD bool t3Prefilter(const Modules& m,
-                          const MiniDoublets& md,
-                          const Segments& s,
-                          uint16_t lm1,
-                          uint16_t lm2,
-                          uint16_t lm3,
-                          unsigned int innerSeg,
-                          unsigned int outerSeg) {
-    if (s.mdIndices[2 * innerSeg + 1] != s.mdIndices[2 * outerSeg])
-      return false;
-    return t3PassRZ(m, md, lm1, lm2, lm3, s.mdIndices[2 * innerSeg], s.mdIndices[2 * outerSeg],
-                    s.mdIndices[2 * outerSeg + 1]);
-  }
 
   // SDL/Triplet.h:797-870
   LST_HD bool t3Select(const Modules& m,

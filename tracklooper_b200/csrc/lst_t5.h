@@ -109,7 +109,7 @@ namespace lst {
     float coshEta = dr3_InSeg / drt_InSeg;
     float dzErr = (zpitch_InLo + zpitch_OutLo) * (zpitch_InLo + zpitch_OutLo) * 2.f;
     float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rt_OutLo - rt_InLo) / 50.f) * fsqrt(r3_InLo / rt_InLo);
-    float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     dzErr += sdlMuls * sdlMuls * drt_OutLo_InLo * drt_OutLo_InLo / 3.f * coshEta * coshEta;
     dzErr = fsqrt(dzErr);
     const float dzMean = dz_InSeg / drt_InSeg * drt_OutLo_InLo;
@@ -165,7 +165,7 @@ namespace lst {
     float drt_tl_axis = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
     float corrF = 1.f;
     const float rt_InSeg = segmentDr(md, q.md1, q.md2);
-    float betaInCut = fasin(fmin_((-rt_InSeg * corrF + drt_tl_axis) * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) +
+    float betaInCut = fasin(fmin_((-rt_InSeg * corrF + drt_tl_axis) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) +
                       (0.02f / drt_InSeg);
     if (!(fabs_(betaInRHmin) < betaInCut))
       return false;
@@ -204,7 +204,7 @@ namespace lst {
                   sinDPhi / drt_tl_axis;
     }
     const float dBetaROut2 = dBetaROut * dBetaROut;
-    float betaOutCut = fasin(fmin_(drt_tl_axis * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
+    float betaOutCut = fasin(fmin_(drt_tl_axis * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
                        fsqrt(dBetaLum2 + dBetaMuls * dBetaMuls);
     if (!(fabs_(betaOut) < betaOutCut))
       return false;
@@ -255,7 +255,7 @@ namespace lst {
     float drtErr =
         zGeom1_another * zGeom1_another * drtSDIn * drtSDIn / dzSDIn / dzSDIn * (1.f - 2.f * kZ + 2.f * kZ * kZ);
     const float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rt_OutLo - rt_InLo) / 50.f) * fsqrt(rIn / rt_InLo);
-    const float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    const float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     drtErr += sdlMuls * sdlMuls * multDzDr * multDzDr / 3.f * coshEta * coshEta;
     drtErr = fsqrt(drtErr);
     if (!((kZ >= 0) && (rtOut >= rtLo) && (rtOut <= rtHi)))
@@ -313,7 +313,7 @@ namespace lst {
     float dr = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
     const float corrF = 1.f;
     float betaInCut =
-        fasin(fmin_((-sdIn_dr * corrF + dr) * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdIn_d);
+        fasin(fmin_((-sdIn_dr * corrF + dr) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdIn_d);
     if (!(fabs_(betaInRHmin) < betaInCut))
       return false;
 
@@ -351,7 +351,7 @@ namespace lst {
                   sinDPhi / dr;
     }
     const float dBetaROut2 = dBetaROut * dBetaROut;
-    float betaOutCut = fasin(fmin_(dr * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
+    float betaOutCut = fasin(fmin_(dr * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
                        fsqrt(dBetaLum2 + dBetaMuls * dBetaMuls);
     if (!(fabs_(betaOut) < betaOutCut))
       return false;
@@ -390,7 +390,7 @@ namespace lst {
     float multDzDr = dzOutInAbs * coshEta / (coshEta * coshEta - 1.f);
     float kZ = (z_OutLo - z_InLo) / dzSDIn;
     float sdlThetaMulsF = 0.015f * fsqrt(0.1f + 0.2f * (rt_OutLo - rt_InLo) / 50.f);
-    float sdlMuls = sdlThetaMulsF * 3.f / kPtCut * 4.f;
+    float sdlMuls = sdlThetaMulsF * 3.f / m.ptCut * 4.f;
     float drtErr = fsqrt(kPixelPSZpitch * kPixelPSZpitch * 2.f / (dzSDIn * dzSDIn) * (dzOutInAbs * dzOutInAbs) +
                          sdlMuls * sdlMuls * multDzDr * multDzDr / 3.f * coshEta * coshEta);
     float drtMean = drtSDIn * dzOutInAbs / fabs_(dzSDIn);
@@ -450,7 +450,7 @@ namespace lst {
     float dr = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
     const float corrF = 1.f;
     float betaInCut =
-        fasin(fmin_((-sdIn_dr * corrF + dr) * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdIn_d);
+        fasin(fmin_((-sdIn_dr * corrF + dr) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdIn_d);
     if (!(fabs_(betaInRHmin) < betaInCut))
       return false;
 
@@ -479,7 +479,7 @@ namespace lst {
     const float dBetaLum2 = (dBetaInLum + dBetaOutLum) * (dBetaInLum + dBetaOutLum);
     const float dBetaRIn2 = 0;
     float dBetaROut2 = 0;
-    float betaOutCut = fasin(fmin_(dr * k2Rinv1GeVf / kPtCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
+    float betaOutCut = fasin(fmin_(dr * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / sdOut_d) +
                        fsqrt(dBetaLum2 + dBetaMuls * dBetaMuls);
     if (!(fabs_(betaOut) < betaOutCut))
       return false;
@@ -1284,7 +1284,7 @@ namespace lst {
     // so they run cheapest first: the radius tests of
     // SDL/Quintuplet.h:2740-2906 before the two beta algorithms of :2555-2622
     // and the rz test of :2715-2735.
-    const bool pass = (v.innerRadius >= 0.95f * kPtCut / (2.f * k2Rinv1GeVf));
+    const bool pass = (v.innerRadius >= 0.95f * m.ptCut / (2.f * k2Rinv1GeVf));
     if (!pass)
       return false;
     short s1 = m.subdets[lm[0]], s2 = m.subdets[lm[1]], s3 = m.subdets[lm[2]], s4 = m.subdets[lm[3]],

@@ -33,13 +33,20 @@ ES_BASE = PKG_DIR  # plays the role of $LST_BASE: <ES_BASE>/data/<GEOMETRY_NAME>
 _lock = threading.Lock()
 
 
-def geometry_dir() -> str:
-    """Returns the unpacked geometry directory, unpacking the tarball if needed."""
-    out = os.path.join(DATA_DIR, GEOMETRY_NAME)
+# The geometries shipped (data/<name>.tar.xz): the pt0.8 module and pixel maps
+# the reference loads (SDL/LSTESData.cc:46-57), and the pt0.6 ones beside them
+# in the reference's data/, which it hard-codes away.  The event setup takes
+# the pt cut of its cuts from the directory name (lst_es_info.ptCut).
+GEOMETRIES = ("OT800_IT615_pt0.8", "OT800_IT615_pt0.6")
+
+
+def geometry_dir(name: str = GEOMETRY_NAME) -> str:
+    """Returns the unpacked geometry directory `name`, unpacking its tarball if needed."""
+    out = os.path.join(DATA_DIR, name)
     marker = os.path.join(out, "sensor_centroids.bin")
     with _lock:
         if not os.path.exists(marker):
-            tarball = os.path.join(DATA_DIR, GEOMETRY_NAME + ".tar.xz")
+            tarball = os.path.join(DATA_DIR, name + ".tar.xz")
             if not os.path.exists(tarball):
                 raise FileNotFoundError(f"geometry tarball missing: {tarball}")
             with lzma.open(tarball) as xz, tarfile.open(fileobj=xz) as tar:

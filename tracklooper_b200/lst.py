@@ -246,6 +246,7 @@ class EsInfo(ctypes.Structure):
         ("nTotalSegments", ctypes.c_uint32),
         ("maxTriplets", ctypes.c_uint32),
         ("maxQuintuplets", ctypes.c_uint32),
+        ("ptCut", ctypes.c_float),
     ]
 
 
@@ -390,7 +391,7 @@ class ES:
         self.device = device
         info = EsInfo()
         _check(lib.lst_es_get_info(h, ctypes.byref(info)), "lst_es_get_info")
-        self.info = {n: int(getattr(info, n)) for n, _ in EsInfo._fields_}
+        self.info = {n: (float if n == "ptCut" else int)(getattr(info, n)) for n, _ in EsInfo._fields_}
 
     @property
     def handle(self):
@@ -440,7 +441,7 @@ class HostES:
         self._h = h
         info = EsInfo()
         _check(lib.lst_es_get_info(h, ctypes.byref(info)), "lst_es_get_info")
-        self.info = {n: int(getattr(info, n)) for n, _ in EsInfo._fields_}
+        self.info = {n: (float if n == "ptCut" else int)(getattr(info, n)) for n, _ in EsInfo._fields_}
 
     def array(self, name: str, dtype) -> np.ndarray:
         lib = library()

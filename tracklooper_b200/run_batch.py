@@ -1,11 +1,14 @@
 """Runs a batch of seeded synthetic events through the CUDA chain and prints
 per-event object counts and the batch time.
 
-  python -m tracklooper_b200.run_batch --config 2 --events 8 [--repeat 3] [--cuts]
+  python -m tracklooper_b200.run_batch --config 2 --events 8 [--repeat 3] [--cuts] [--tune-cache PATH]
 
 --config selects the generator configuration (1 muon gun, 2 PU200-shaped,
 3 PU140-250, 5 PU250 with displaced tracks); the events are generated with
 seeds (config << 32) | index, uploaded packed, and run once per --repeat.
+With --tune-cache the launch shapes come from the autotuner's cache for this
+geometry, device, batch size and build, or from a sweep that is then stored
+there (lst_autotune_load / lst_autotune).
 """
 from __future__ import annotations
 
@@ -26,6 +29,7 @@ def main(argv=None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--cuts", action="store_true", help="cut-only T5 selection instead of the DNN")
     ap.add_argument("--json", action="store_true")
+    ap.add_argument("--tune-cache", default=None, help="autotuner cache file (load, or sweep and store)")
     args = ap.parse_args(argv)
 
     with ThreadPoolExecutor(max_workers=16) as pool:
@@ -35,6 +39,10 @@ def main(argv=None):
     if args.cuts:
         eset.set_t5_method(lst.T5_CUTS)
     blob, offsets = lst.pack_events(inputs)
+    if args.tune_cache:
+        if not eset.autotune_load(args.events, args.tune_cache):
+            eset.upload_packed(0, blob, offsets)
+            eset.autotune(0, args.events, args.tune_cache)
     times = []
     for r in range(args.repeat):
         t0 = time.perf_counter()
