@@ -140,6 +140,7 @@ namespace {
     std::vector<uint16_t> mdMod;
     std::vector<TFloat> mdF[40];
     std::vector<lst::MDPos> mdPos;
+    std::vector<lst::MDRec> mdRec;
     lst::MiniDoublets md{};
     // segments
     std::vector<TFloat> lsF[6];
@@ -194,6 +195,7 @@ namespace {
 
       mdA.resize(kMDn); mdO.resize(kMDn); mdMod.resize(kMDn); mdN.resize(nModules + 1); mdTot.resize(nModules + 1);
       mdPos.resize(kMDn);
+      mdRec.resize(kMDn);
       TFloat* f[40];
       for (int i = 0; i < 40; ++i)
         f[i] = F(mdF[i], kMDn);
@@ -209,6 +211,7 @@ namespace {
       md.outerHighEdgeX = f[k++]; md.outerHighEdgeY = f[k++]; md.outerLowEdgeX = f[k++]; md.outerLowEdgeY = f[k++];
       md.slope = f[k++]; md.tanSlope = f[k++]; md.slope3 = f[k++];
       md.anchorPos = mdPos.data();
+      md.rec = mdRec.data();
 
       TFloat* g[6];
       for (int i = 0; i < 6; ++i)

@@ -201,9 +201,12 @@ def test_nan_hit_coordinates(ref, es):
         for st, r in d.items():
             assert r["only_a"] == 0 and r["only_b"] == 0 and r["state_differ"] == 0, (st, r)
         bad_set = set(int(i) for i in bad)
-        skip = {"ls": 0, "t3": 0, "t5": 0, "pt3": 1, "pt5": 1, "tc": 2}  # key entries before the hits
+        skip = {"ls": 0, "t3": 0, "t5": 0, "pt3": 1, "pt5": 1}  # key entries before the hits
         for st, n0 in skip.items():
             assert not any(h in bad_set for k in a.keys[st] for h in k[n0:]), st
+        # track candidates built of outer-tracker objects (a pLS candidate's
+        # slots hold pixel ntuple indices, another index space)
+        assert not any(h in bad_set for k in a.keys["tc"] if k[0] in (4, 5, 7) for h in k[2:])
         assert ev.counts()["nTrackCandidates"] > 1000
     finally:
         ev.event_set.close()

@@ -290,10 +290,19 @@ namespace lst {
     // The anchor hit's x, y, z, rt in one 16-byte record: the segment, triplet
     // and pixel kernels gather them together for mini-doublets chosen by index.
     struct MDPos* anchorPos;
+    // Everything the segment cuts read of a mini-doublet, in one 48-byte
+    // record (three 16-byte loads instead of a dozen scattered ones).
+    struct MDRec* rec;
   };
 
   struct alignas(16) MDPos {
     float x, y, z, rt;
+  };
+
+  struct alignas(16) MDRec {
+    float x, y, z, rt;                         // anchor hit
+    float phi, slope, tanSlope, dphichange;    // anchorPhi, slope, tanSlope, dphichanges
+    float dphi, dz, highEdgePhi, lowEdgePhi;   // dphis, dzs, anchorHighEdgePhi, anchorLowEdgePhi
   };
 
   struct Segments {

@@ -139,6 +139,7 @@ namespace {
     v.md.tanSlope = c.take<float>(MD);
     v.md.slope3 = c.take<float>(MD);
     v.md.anchorPos = c.take<lst::MDPos>(MD);
+    v.md.rec = c.take<lst::MDRec>(MD);
     v.sc = c.take<lst::EventScalars>(1);
   }
 
@@ -493,12 +494,17 @@ namespace {
     const size_t P = lst::kMaxPixelSegments;
     const dim3 one(1, count);
     switch (stage) {
-      case LST_STAGE_MINI_DOUBLETS:
-        LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, 32), count), tunedThreads(ev, kTuMD), d, v);
+      case LST_STAGE_MINI_DOUBLETS: {
+        // modules per warp task: 32 when a launch holds many events, fewer
+        // for a few events, so that a single event still fills the GPU
+        const unsigned int mpt = count >= 16 ? 32u : (count >= 4 ? 8u : 4u);
+        LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, mpt), count), tunedThreads(ev, kTuMD), d, v,
+                   mpt);
         LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kMDDerived, tunedWarpGrid(ev, kTuMDDerived, nLower + 1, count), tunedThreads(ev, kTuMDDerived),
                    d, v);
         break;
+      }
       case LST_STAGE_SEGMENTS:
         LST_LAUNCH(lst::kCreateLS, tunedWarpGrid(ev, kTuLS, nLower, count), tunedThreads(ev, kTuLS), d, v);
         LST_LAUNCH(lst::kLSRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);

@@ -333,9 +333,9 @@ namespace lst {
   // their rank in the reference's serial loop order (lower hit outer, upper
   // hit inner), the first mdCap of them.
   //
-  // A warp takes 32 consecutive lower modules at a time (most hold fewer
-  // than 32 pairs, the median 14) and deals their pairs out in order, 32 per
-  // step, across module boundaries: lane l of step s takes the task's pair
+  // A warp takes up to 32 consecutive lower modules at a time (most hold
+  // fewer than 32 pairs, the median 14) and deals their pairs out in order, 32
+  // per step, across module boundaries: lane l of step s takes the task's pair
   // 32 s + l, finds its module by a binary search over the lanes' exclusive
   // prefix of pair counts, and its hits by dividing by the module's upper
   // hit count.  A passing pair's rank is the module's running count (one
@@ -344,11 +344,11 @@ namespace lst {
   // modules, and a large module simply spans several steps.
   constexpr int kMDMaxWarps = 8;  // warps per block the kernel is launched with (at most)
   __device__ __forceinline__ void mdTask(DeviceES const& es, const EventView& ev, unsigned int task,
-                                         unsigned int* count) {
+                                         unsigned int modulesPerTask, unsigned int* count) {
     const Hits& h = ev.hits;
     const unsigned int lane = laneId();
-    const unsigned int lmU = task * 32u + lane;
-    const bool valid = lmU < es.nLowerModules && h.hitRangesLower[lmU] != -1;
+    const unsigned int lmU = task * modulesPerTask + lane;
+    const bool valid = lane < modulesPerTask && lmU < es.nLowerModules && h.hitRangesLower[lmU] != -1;
     const int nL = valid ? int(h.hitRangesnLower[lmU]) : 0;
     const int nU = valid ? int(h.hitRangesnUpper[lmU]) : 0;
     const int loHit0 = valid ? h.hitRangesLower[lmU] : 0;
@@ -390,7 +390,7 @@ namespace lst {
       bool ok = false;
       MDValues v;
       unsigned int lowerIdx = 0, upperIdx = 0;
-      const uint16_t lm = static_cast<uint16_t>(task * 32u + unsigned(j));
+      const uint16_t lm = static_cast<uint16_t>(task * modulesPerTask + unsigned(j));
       if (g < total) {
         const int local = g - exj;
         lowerIdx = unsigned(loj + local / nUj);
@@ -450,14 +450,16 @@ namespace lst {
 #define LST_LB_EVAL 128, LST_LB_EVAL_B
 #define LST_LB_T5EVAL 128, LST_LB_T5EVAL_B
 #define LST_LB_PIXMID 128, LST_LB_PIXMID_B
-  __global__ void __launch_bounds__(LST_LB_MD) kCreateMD(DeviceES es, const EventView* evs) {
+  // modulesPerTask (1..32): 32 for batches; fewer for a single event, whose
+  // 13 000 lower modules would otherwise make only ~400 warp tasks.
+  __global__ void __launch_bounds__(LST_LB_MD) kCreateMD(DeviceES es, const EventView* evs, unsigned int modulesPerTask) {
     __shared__ unsigned int sCount[kMDMaxWarps][32];
     const EventView& ev = evs[blockIdx.y];
     const int wpb = blockDim.x >> 5;
     const int w = threadIdx.x >> 5;
-    const unsigned int nTasks = (es.nLowerModules + 31u) / 32u;
+    const unsigned int nTasks = (es.nLowerModules + modulesPerTask - 1u) / modulesPerTask;
     for (unsigned int task = blockIdx.x * wpb + w; task < nTasks; task += gridDim.x * wpb)
-      mdTask(es, ev, task, sCount[w]);
+      mdTask(es, ev, task, modulesPerTask, sCount[w]);
   }
 
   // Derived per-MD values for every stored MD (lower modules and the pixel

@@ -47,11 +47,11 @@ namespace lst {
     if (innerBarrel)
       sdLumForInnerMini = innerminiTilt * dAlpha_Bfield;
     else
-      sdLumForInnerMini = md.dphis[innerMD] * 15.0f / md.dzs[innerMD];
+      sdLumForInnerMini = md.rec[innerMD].dphi * 15.0f / md.rec[innerMD].dz;
     if (outerBarrel)
       sdLumForOuterMini = outerminiTilt * dAlpha_Bfield;
     else
-      sdLumForOuterMini = md.dphis[outerMD] * 15.0f / md.dzs[outerMD];
+      sdLumForOuterMini = md.rec[outerMD].dphi * 15.0f / md.rec[outerMD].dz;
 
     float dAlpha_res_inner = 0.02f / miniDelta * (innerBarrel ? 1.0f : fabs_(zIn) / rtIn);
     float dAlpha_res_outer = 0.02f / miniDelta * (outerBarrel ? 1.0f : fabs_(zOut) / rtOut);
@@ -85,13 +85,14 @@ namespace lst {
                        LSValues& v) {
     float sdMuls = (m.subdets[innerLM] == Barrel) ? miniMulsPtScaleBarrel(m.layers[innerLM] - 1) * 3.f / m.ptCut
                                                   : miniMulsPtScaleEndcap(m.layers[innerLM] - 1) * 3.f / m.ptCut;
-    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
-    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
-    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
+    const MDRec& rIn = md.rec[innerMD];
+    const MDRec& rOut = md.rec[outerMD];
+    float xIn = rIn.x, yIn = rIn.y, zIn = rIn.z, rtIn = rIn.rt;
+    float xOut = rOut.x, yOut = rOut.y, zOut = rOut.z, rtOut = rOut.rt;
 
-    float sdSlope = md.slope[outerMD];
+    float sdSlope = rOut.slope;
     float sdPVoff = 0.1f / rtOut;
-    float dzDrtScale = md.tanSlope[outerMD] / sdSlope;
+    float dzDrtScale = rOut.tanSlope / sdSlope;
     const float zGeom = m.layers[innerLM] <= 2 ? 2.f * kPixelPSZpitch : 2.f * kStrip2SZpitch;
     float zLo = zIn + (zIn - kDeltaZLum) * (rtOut / rtIn - 1.f) * (zIn > 0.f ? 1.f : dzDrtScale) - zGeom;
     float zHi = zIn + (zIn + kDeltaZLum) * (rtOut / rtIn - 1.f) * (zIn < 0.f ? 1.f : dzDrtScale) + zGeom;
@@ -99,17 +100,17 @@ namespace lst {
       return false;
 
     float sdCut = sdSlope + fsqrt(sdMuls * sdMuls + sdPVoff * sdPVoff);
-    v.dPhi = phiMpiPi(md.anchorPhi[outerMD] - md.anchorPhi[innerMD]);
+    v.dPhi = phiMpiPi(rOut.phi - rIn.phi);
     if (!(fabs_(v.dPhi) <= sdCut))
       return false;
-    v.dPhiChange = phiMpiPi(phiOf(xOut - xIn, yOut - yIn) - md.anchorPhi[innerMD]);
+    v.dPhiChange = phiMpiPi(phiOf(xOut - xIn, yOut - yIn) - rIn.phi);
     if (!(fabs_(v.dPhiChange) <= sdCut))
       return false;
 
     float thr[3];
     lsDAlphaThresholds(m, md, xIn, yIn, zIn, rtIn, xOut, yOut, zOut, rtOut, innerLM, outerLM, innerMD, outerMD, thr);
-    float innerMDAlpha = md.dphichanges[innerMD];
-    float outerMDAlpha = md.dphichanges[outerMD];
+    float innerMDAlpha = rIn.dphichange;
+    float outerMDAlpha = rOut.dphichange;
     float dAlphaInnerMDSegment = innerMDAlpha - v.dPhiChange;
     float dAlphaOuterMDSegment = outerMDAlpha - v.dPhiChange;
     float dAlphaInnerMDOuterMD = innerMDAlpha - outerMDAlpha;
@@ -128,11 +129,12 @@ namespace lst {
                        unsigned int innerMD,
                        unsigned int outerMD,
                        LSValues& v) {
-    const MDPos pIn = md.anchorPos[innerMD], pOut = md.anchorPos[outerMD];
-    float xIn = pIn.x, yIn = pIn.y, zIn = pIn.z, rtIn = pIn.rt;
-    float xOut = pOut.x, yOut = pOut.y, zOut = pOut.z, rtOut = pOut.rt;
+    const MDRec& rIn = md.rec[innerMD];
+    const MDRec& rOut = md.rec[outerMD];
+    float xIn = rIn.x, yIn = rIn.y, zIn = rIn.z, rtIn = rIn.rt;
+    float xOut = rOut.x, yOut = rOut.y, zOut = rOut.z, rtOut = rOut.rt;
     bool outerLayerEndcapTwoS = (m.subdets[outerLM] == Endcap) && (m.moduleType[outerLM] == TwoS);
-    float sdSlope = md.slope[outerMD];
+    float sdSlope = rOut.slope;
     float disks2SMinRadius = 60.f;
     float rtGeom = ((rtIn < disks2SMinRadius && rtOut < disks2SMinRadius)
                         ? (2.f * kPixelPSZpitch)
@@ -142,17 +144,17 @@ namespace lst {
       return false;
     float dz = zOut - zIn;
     float dLum = signTransfer(kDeltaZLum, zIn);
-    float drtDzScale = sdSlope / md.tanSlope[outerMD];
+    float drtDzScale = sdSlope / rOut.tanSlope;
     float rtLo = fmax_(rtIn * (1.f + dz / (zIn + dLum) * drtDzScale) - rtGeom, rtIn - 0.5f * rtGeom);
     float rtHi = rtIn * (zOut - dLum) / (zIn - dLum) + rtGeom;
     if (!((rtOut >= rtLo) && (rtOut <= rtHi)))
       return false;
 
-    v.dPhi = phiMpiPi(md.anchorPhi[outerMD] - md.anchorPhi[innerMD]);
+    v.dPhi = phiMpiPi(rOut.phi - rIn.phi);
     float sdCut = sdSlope;
     if (outerLayerEndcapTwoS) {
-      float dPhiPos_high = phiMpiPi(md.anchorHighEdgePhi[outerMD] - md.anchorPhi[innerMD]);
-      float dPhiPos_low = phiMpiPi(md.anchorLowEdgePhi[outerMD] - md.anchorPhi[innerMD]);
+      float dPhiPos_high = phiMpiPi(rOut.highEdgePhi - rIn.phi);
+      float dPhiPos_low = phiMpiPi(rOut.lowEdgePhi - rIn.phi);
       v.dPhiMax = fabs_(dPhiPos_high) > fabs_(dPhiPos_low) ? dPhiPos_high : dPhiPos_low;
       v.dPhiMin = fabs_(dPhiPos_high) > fabs_(dPhiPos_low) ? dPhiPos_low : dPhiPos_high;
     } else {
@@ -171,8 +173,8 @@ namespace lst {
 
     float thr[3];
     lsDAlphaThresholds(m, md, xIn, yIn, zIn, rtIn, xOut, yOut, zOut, rtOut, innerLM, outerLM, innerMD, outerMD, thr);
-    float innerMDAlpha = md.dphichanges[innerMD];
-    float outerMDAlpha = md.dphichanges[outerMD];
+    float innerMDAlpha = rIn.dphichange;
+    float outerMDAlpha = rOut.dphichange;
     float dAlphaInnerMDSegment = innerMDAlpha - v.dPhiChange;
     float dAlphaOuterMDSegment = outerMDAlpha - v.dPhiChange;
     float dAlphaInnerMDOuterMD = innerMDAlpha - outerMDAlpha;

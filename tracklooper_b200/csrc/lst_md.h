@@ -198,12 +198,17 @@ namespace lst {
   }
 
   // The derived per-MD values of MiniDoublets (slope, tanSlope, slope3).
+  // Also fills the mini-doublet's record of segment-cut inputs (MDRec).
   LST_HD void storeMDDerived(MiniDoublets& md, unsigned int idx, float ptCut) {
     const float rt = md.anchorRt[idx];
     const float slope = fasin(fmin_(rt * k2Rinv1GeVf / ptCut, kSinAlphaMax));
+    const float tanSlope = ftan(slope);
     md.slope[idx] = slope;
-    md.tanSlope[idx] = ftan(slope);
+    md.tanSlope[idx] = tanSlope;
     md.slope3[idx] = fasin(fmin_(rt * k2Rinv1GeVf / 3.0f, kSinAlphaMax));
+    const MDPos p = md.anchorPos[idx];
+    md.rec[idx] = MDRec{p.x, p.y, p.z, p.rt, md.anchorPhi[idx], slope, tanSlope, md.dphichanges[idx],
+                        md.dphis[idx], md.dzs[idx], md.anchorHighEdgePhi[idx], md.anchorLowEdgePhi[idx]};
   }
 
   struct MDValues {

@@ -16,8 +16,8 @@ namespace lst {
                        unsigned int md1,
                        unsigned int md2,
                        unsigned int md3) {
-    const float r1 = md.anchorPos[md1].rt, r2 = md.anchorPos[md2].rt, r3 = md.anchorPos[md3].rt;
-    const float z1 = md.anchorPos[md1].z, z2 = md.anchorPos[md2].z, z3 = md.anchorPos[md3].z;
+    const float r1 = md.rec[md1].rt, r2 = md.rec[md2].rt, r3 = md.rec[md3].rt;
+    const float z1 = md.rec[md1].z, z2 = md.rec[md2].z, z3 = md.rec[md3].z;
     const int layer1 = m.sdlLayers[lm1], layer2 = m.sdlLayers[lm2], layer3 = m.sdlLayers[lm3];
     const float residual = z2 - ((z3 - z1) / (r3 - r1) * (r2 - r1) + z1);
     const float ar = fabs_(residual);
@@ -53,8 +53,8 @@ namespace lst {
   }
 
   LST_HD float segmentDr(const MiniDoublets& md, unsigned int a, unsigned int b) {
-    return fsqrt((md.anchorPos[b].x - md.anchorPos[a].x) * (md.anchorPos[b].x - md.anchorPos[a].x) +
-                 (md.anchorPos[b].y - md.anchorPos[a].y) * (md.anchorPos[b].y - md.anchorPos[a].y));
+    return fsqrt((md.rec[b].x - md.rec[a].x) * (md.rec[b].x - md.rec[a].x) +
+                 (md.rec[b].y - md.rec[a].y) * (md.rec[b].y - md.rec[a].y));
   }
 
   // Barrel-barrel-barrel pointing and first beta cut (SDL/Triplet.h:301-402).
@@ -70,11 +70,11 @@ namespace lst {
                             float& betaIn) {
     bool isPSIn = (m.moduleType[lm1] == PS);
     bool isPSOut = (m.moduleType[lm3] == PS);
-    float rtIn = md.anchorPos[md1].rt, rtMid = md.anchorPos[md2].rt, rtOut = md.anchorPos[md3].rt;
-    float zIn = md.anchorPos[md1].z, zMid = md.anchorPos[md2].z, zOut = md.anchorPos[md3].z;
-    float alpha1GeVOut = md.slope[md3];
+    float rtIn = md.rec[md1].rt, rtMid = md.rec[md2].rt, rtOut = md.rec[md3].rt;
+    float zIn = md.rec[md1].z, zMid = md.rec[md2].z, zOut = md.rec[md3].z;
+    float alpha1GeVOut = md.rec[md3].slope;
     float rtRatio_OutIn = rtOut / rtIn;
-    float dzDrtScale = md.tanSlope[md3] / alpha1GeVOut;
+    float dzDrtScale = md.rec[md3].tanSlope / alpha1GeVOut;
     float zpitchIn = (isPSIn ? kPixelPSZpitch : kStrip2SZpitch);
     float zpitchOut = (isPSOut ? kPixelPSZpitch : kStrip2SZpitch);
     const float zHi =
@@ -102,9 +102,9 @@ namespace lst {
     bool pass = ((zOut >= zLoPointed) && (zOut <= zHiPointed));
 
     float alpha_InLo = s.dPhiChanges[innerSeg];
-    float tl_axis_x = md.anchorPos[md3].x - md.anchorPos[md1].x;
-    float tl_axis_y = md.anchorPos[md3].y - md.anchorPos[md1].y;
-    betaIn = alpha_InLo - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
+    float tl_axis_x = md.rec[md3].x - md.rec[md1].x;
+    float tl_axis_y = md.rec[md3].y - md.rec[md1].y;
+    betaIn = alpha_InLo - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.rec[md1].phi);
     float drt_tl_axis = fsqrt(tl_axis_x * tl_axis_x + tl_axis_y * tl_axis_y);
     const float rt_InSeg = segmentDr(md, md1, md2);
     float betaInCut = fasin(fmin_((-rt_InSeg + drt_tl_axis) * k2Rinv1GeVf / m.ptCut, kSinAlphaMax)) + (0.02f / drt_InSeg);
@@ -124,10 +124,10 @@ namespace lst {
                             float& betaIn) {
     bool isPSIn = (m.moduleType[lm1] == PS);
     bool isPSOut = (m.moduleType[lm3] == PS);
-    float rtIn = md.anchorPos[md1].rt, rtMid = md.anchorPos[md2].rt, rtOut = md.anchorPos[md3].rt;
-    float zIn = md.anchorPos[md1].z, zMid = md.anchorPos[md2].z, zOut = md.anchorPos[md3].z;
-    float alpha1GeV_OutLo = md.slope[md3];
-    float dzDrtScale = md.tanSlope[md3] / alpha1GeV_OutLo;
+    float rtIn = md.rec[md1].rt, rtMid = md.rec[md2].rt, rtOut = md.rec[md3].rt;
+    float zIn = md.rec[md1].z, zMid = md.rec[md2].z, zOut = md.rec[md3].z;
+    float alpha1GeV_OutLo = md.rec[md3].slope;
+    float dzDrtScale = md.rec[md3].tanSlope / alpha1GeV_OutLo;
     float zpitchIn = (isPSIn ? kPixelPSZpitch : kStrip2SZpitch);
     float zpitchOut = (isPSOut ? kPixelPSZpitch : kStrip2SZpitch);
     float zGeom = zpitchIn + zpitchOut;
@@ -165,12 +165,12 @@ namespace lst {
     drtErr = fsqrt(drtErr);
     bool pass = (kZ >= 0) && (rtOut >= rtLo) && (rtOut <= rtHi);
 
-    float rt_InLo = md.anchorPos[md1].rt;
-    float rt_InOut = md.anchorPos[md2].rt;
+    float rt_InLo = md.rec[md1].rt;
+    float rt_InOut = md.rec[md2].rt;
     float sdIn_alpha = s.dPhiChanges[innerSeg];
-    float tl_axis_x = md.anchorPos[md3].x - md.anchorPos[md1].x;
-    float tl_axis_y = md.anchorPos[md3].y - md.anchorPos[md1].y;
-    betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
+    float tl_axis_x = md.rec[md3].x - md.rec[md1].x;
+    float tl_axis_y = md.rec[md3].y - md.rec[md1].y;
+    betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.rec[md1].phi);
     float betaInRHmin = betaIn;
     float betaInRHmax = betaIn;
     if (fabs_(betaInRHmin) > fabs_(betaInRHmax)) {
@@ -196,10 +196,10 @@ namespace lst {
                             unsigned int md3,
                             unsigned int innerSeg,
                             float& betaIn) {
-    float rtIn = md.anchorPos[md1].rt, rtMid = md.anchorPos[md2].rt, rtOut = md.anchorPos[md3].rt;
-    float zIn = md.anchorPos[md1].z, zMid = md.anchorPos[md2].z, zOut = md.anchorPos[md3].z;
-    float alpha1GeV_Out = md.slope[md3];
-    float dzDrtScale = md.tanSlope[md3] / alpha1GeV_Out;
+    float rtIn = md.rec[md1].rt, rtMid = md.rec[md2].rt, rtOut = md.rec[md3].rt;
+    float zIn = md.rec[md1].z, zMid = md.rec[md2].z, zOut = md.rec[md3].z;
+    float alpha1GeV_Out = md.rec[md3].slope;
+    float dzDrtScale = md.rec[md3].tanSlope / alpha1GeV_Out;
     if (!(zIn * zOut > 0))
       return false;
     float dLum = signTransfer(kDeltaZLum, zIn);
@@ -234,12 +234,12 @@ namespace lst {
     if (isInSgInnerMDPS and isInSgOuterMDPS)
       pass = ((kZ >= 0) && (rtOut >= rtLo_point) && (rtOut <= rtHi_point));
 
-    float rt_InLo = md.anchorPos[md1].rt;
-    float rt_InOut = md.anchorPos[md2].rt;
+    float rt_InLo = md.rec[md1].rt;
+    float rt_InOut = md.rec[md2].rt;
     float sdIn_alpha = s.dPhiChanges[innerSeg];
-    float tl_axis_x = md.anchorPos[md3].x - md.anchorPos[md1].x;
-    float tl_axis_y = md.anchorPos[md3].y - md.anchorPos[md1].y;
-    betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.anchorPhi[md1]);
+    float tl_axis_x = md.rec[md3].x - md.rec[md1].x;
+    float tl_axis_y = md.rec[md3].y - md.rec[md1].y;
+    betaIn = sdIn_alpha - phiMpiPi(phiOf(tl_axis_x, tl_axis_y) - md.rec[md1].phi);
     float sdIn_alphaRHmin = s.dPhiChangeMins[innerSeg];
     float sdIn_alphaRHmax = s.dPhiChangeMaxs[innerSeg];
     float betaInRHmin = betaIn + sdIn_alphaRHmin - sdIn_alpha;
@@ -309,12 +309,12 @@ namespace lst {
       pass = false;
     if (!pass)
       return false;
-    v.circleRadius = circleFrom3(md.anchorPos[md1].x,
-                                 md.anchorPos[md1].y,
-                                 md.anchorPos[md2].x,
-                                 md.anchorPos[md2].y,
-                                 md.anchorPos[md3].x,
-                                 md.anchorPos[md3].y,
+    v.circleRadius = circleFrom3(md.rec[md1].x,
+                                 md.rec[md1].y,
+                                 md.rec[md2].x,
+                                 md.rec[md2].y,
+                                 md.rec[md3].x,
+                                 md.rec[md3].y,
                                  v.circleCenterX,
                                  v.circleCenterY);
     return true;
