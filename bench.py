@@ -450,6 +450,11 @@ def run_ours(args, rank, world, local, events):
         "clocks": clocks,
         "roofline": roofline,
         "kernels": kernel_table,
+        # device time of all of a step's kernels (CUDA events around each,
+        # direct launches) beside the graph-replayed step: the difference is
+        # what the step's launch boundaries cost
+        "kernels_sum_ms_per_step": round(tot / args.steps, 4),
+        "launches_per_step": round(sum(v[0] for v in prof.values()) / args.steps, 1),
         "objects_per_event": {k: round(v / B, 1) for k, v in agg.items() if k != "nLower"},
         "device_memory_gb": round(eset.memory_bytes() / 1e9, 2),
         "autotune": tune_info,

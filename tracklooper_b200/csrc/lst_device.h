@@ -116,6 +116,8 @@ namespace lst {
     unsigned int* t5CandFlag;   // per candidate: 0 = fails, else 1 + slot of its values in t5PassValues
     T5Values* t5PassValues;     // selection values of passing candidates
     unsigned int* t5PassC;      //   and their candidate index
+    float* t5DnnFeat;           // candidates staged for the classifier (kT5Eval): 38 inputs each
+    struct T5DnnSlotG* t5DnnSlot;  //   and their selection state
     unsigned int* plsModPre;    // per pLS: candidate prefix over its connected modules (41 entries)
     unsigned int* plsCand;      // per pLS: candidates
     unsigned int* plsCandOff;   // per pLS: first candidate (nPLS + 1 entries)

@@ -237,6 +237,8 @@
   X(t5CandFlag, unsigned int, lst::kT5CandCap)        \
   X(t5PassValues, lst::T5Values, lst::kT5PassCap)     \
   X(t5PassC, unsigned int, lst::kT5PassCap)           \
+  X(t5DnnFeat, float, 38 * lst::kT5DnnCap)            \
+  X(t5DnnSlot, lst::T5DnnSlotG, lst::kT5DnnCap)      \
   X(plsModPre, unsigned int, P * (lst::kMaxConnectedModules + 1)) \
   X(plsCand, unsigned int, P)                         \
   X(plsCandOff, unsigned int, P + 1)                  \

@@ -427,7 +427,7 @@ namespace lst {
   // the fastest of a sweep over 2..14 blocks on B200 (PU200 batches, launch
   // shapes autotuned for each setting).
 #ifndef LST_LB_MD_B
-#define LST_LB_MD_B 3
+#define LST_LB_MD_B 4
 #endif
 #ifndef LST_LB_LS_B
 #define LST_LB_LS_B 12
@@ -1226,43 +1226,6 @@ namespace lst {
     }
   }
 
-  // Candidates of one block tile that reached the classifier, kept in shared
-  // memory until the tile's DNN pass (kT5Eval).
-  constexpr int kT5DnnTile = 64;
-  struct T5DnnSlot {
-    float feat[38];
-    T5Values v;
-    unsigned int mdIdx[5];
-    unsigned int cand;
-    float score;
-    uint16_t lm[5];
-    uint8_t tight;
-  };
-
-  // t5DnnForward (SDL/NeuralNetwork.h:21-165) evaluated by one warp for one
-  // candidate: lane j computes hidden unit j of each layer, summing its
-  // inputs in the same order as the serial loops, so the score is
-  // bit-identical; the layer-1 outputs reach the other lanes by shuffles.
-  // Every lane returns the score.
-  __device__ __forceinline__ float t5DnnForwardWarp(const T5DnnWeights& w, const float* x) {
-    const unsigned int lane = laneId();
-    float acc = 0;
-    for (int in = 0; in < 38; ++in)
-      acc += x[in] * w.w0[in * 32 + lane];
-    acc += w.b0[lane];
-    const float h1 = (acc > 0.f) ? acc : 0.f;
-    acc = 0;
-    for (int in = 0; in < 32; ++in)
-      acc += __shfl_sync(kFullMask, h1, in) * w.w2[in * 32 + lane];
-    acc += w.b2[lane];
-    const float h2 = (acc > 0.f) ? acc : 0.f;
-    float out = 0;
-    for (int in = 0; in < 32; ++in)
-      out += __shfl_sync(kFullMask, h2, in) * w.w4[in];
-    out += w.b4[0];
-    return fexp(out) / (fexp(out) + 1);
-  }
-
   // Records a candidate that passes the T5 selection: its values go to the
   // pass buffer (flag = slot + 1), or, when the buffer is full, the flag asks
   // for re-evaluation at emission (flag = kT5PassCap + 1).
@@ -1277,21 +1240,20 @@ namespace lst {
     }
   }
 
-  // The T5 selection of the queued candidates, with the DNN classifier fused
-  // in (SDL/Quintuplet.h:2921-2941 evaluates it inline).  The block takes its
-  // candidates in tiles of blockDim.  Each thread runs every test before the
-  // classifier on one candidate; those that reach it leave their 38 DNN
-  // inputs and selection values in shared memory.  After a barrier each warp
-  // classifies the tile's waiting candidates one at a time, a lane per hidden
-  // unit, with the weights in shared memory (t5DnnForwardWarp); after a
-  // second, each thread finishes one classified candidate.  So the
-  // classifier runs on full warps although only some candidates of a warp
-  // reach it, and nothing goes through global memory.  A candidate that finds
-  // the tile's slots full is classified by its own thread at once; the
-  // arithmetic is the same in every case.
+  // The T5 selection of the queued candidates with the DNN classifier in the
+  // same kernel (SDL/Quintuplet.h:2921-2941 evaluates it inline).  Each
+  // thread runs every test before the classifier on its candidates; a
+  // candidate that reaches the classifier leaves its 38 inputs and its
+  // selection state in the block's slice of the event's staging area (its
+  // own rows, in L2) instead of running the 38-32-32-1 forward pass there
+  // and then, on a few lanes of its warp.  When the block has evaluated all
+  // of its candidates, its threads classify the block's staged candidates,
+  // one per thread with the weights in shared memory, so that the forward
+  // passes run on full warps.  A candidate that finds its block's slice full
+  // is classified at once by its own thread; the arithmetic is the same
+  // either way.
   __global__ void __launch_bounds__(LST_LB_T5EVAL) kT5Eval(DeviceES es, const EventView* evs, bool useDnn) {
     __shared__ T5DnnWeights sW;
-    __shared__ T5DnnSlot sSlot[kT5DnnTile];
     __shared__ unsigned int sCount;
     const EventView& ev = evs[blockIdx.y];
     if (ev.sc->t5CandOverflow)
@@ -1302,71 +1264,64 @@ namespace lst {
       for (int i = threadIdx.x; i < kT5DnnParams; i += blockDim.x)
         dst[i] = src[i];
     }
+    if (threadIdx.x == 0)
+      sCount = 0;
+    __syncthreads();
     const float wp = c_t5dnnWP;
+    const unsigned int slice = kT5DnnCap / gridDim.x;
+    const unsigned int base = blockIdx.x * slice;
     const unsigned int total = ev.sc->t5CandTotal;
     const unsigned int front = ev.sc->t5QueueCount, back = ev.sc->t5QueueBack;
     const bool fromQueue = front <= kCandQueueCap && back <= kCandQueueCap - front;
     const unsigned int n = fromQueue ? front + back : total;
-    const unsigned int tileStride = gridDim.x * blockDim.x;
-    const unsigned int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
-    // every thread of the block runs the same number of tiles (barriers inside)
-    for (unsigned int tile = blockIdx.x * blockDim.x; tile < n; tile += tileStride) {
-      if (threadIdx.x == 0)
-        sCount = 0;
-      __syncthreads();
-      const unsigned int q = tile + threadIdx.x;
-      if (q < n) {
-        const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
-        unsigned int innerT3, outerT3;
-        uint16_t lm[5];
-        t5Decode(ev, c, innerT3, outerT3, lm);
-        T5Values v;
-        T5Stage st;
-        if (!t5SelectPre(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st)) {
-          ev.t5CandFlag[c] = 0;
-        } else {
-          const unsigned int k = useDnn ? atomicAdd(&sCount, 1u) : unsigned(kT5DnnTile);
-          if (k < unsigned(kT5DnnTile)) {
-            T5DnnSlot& sl = sSlot[k];
-            t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius,
-                          v.outerRadius, v.bridgeRadius, sl.feat);
-            sl.v = v;
-            for (int i = 0; i < 5; ++i) {
-              sl.mdIdx[i] = st.mdIdx[i];
-              sl.lm[i] = lm[i];
-            }
-            sl.cand = c;
-            sl.tight = st.tight ? 1 : 0;
-          } else if (t5Classify(es.m, ev.md, ev.ls, ev.t3, sW, useDnn, wp, lm, innerT3, v, st)) {
-            t5Keep(ev, c, v);
-          } else {
-            ev.t5CandFlag[c] = 0;
-          }
+    for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+      const unsigned int c = fromQueue ? ev.candQueue[q < front ? q : kCandQueueCap - 1 - (q - front)] : q;
+      unsigned int innerT3, outerT3;
+      uint16_t lm[5];
+      t5Decode(ev, c, innerT3, outerT3, lm);
+      T5Values v;
+      T5Stage st;
+      if (!t5SelectPre(es.m, ev.md, ev.ls, ev.t3, lm, innerT3, outerT3, v, st)) {
+        ev.t5CandFlag[c] = 0;
+        continue;
+      }
+      const unsigned int k = useDnn ? atomicAdd(&sCount, 1u) : slice;
+      if (k < slice) {
+        float feat[38];
+        t5DnnFeatures(es.m, ev.md, ev.ls, ev.t3, st.xs, st.ys, st.mdIdx, lm, innerT3, v.innerRadius, v.outerRadius,
+                      v.bridgeRadius, feat);
+        for (int i = 0; i < 38; ++i)
+          ev.t5DnnFeat[size_t(base + k) * 38 + i] = feat[i];
+        T5DnnSlotG& sl = ev.t5DnnSlot[base + k];
+        sl.v = v;
+        for (int i = 0; i < 5; ++i) {
+          sl.mdIdx[i] = st.mdIdx[i];
+          sl.lm[i] = lm[i];
         }
+        sl.cand = c;
+        sl.tight = st.tight ? 1 : 0;
+      } else if (t5Classify(es.m, ev.md, ev.ls, ev.t3, sW, useDnn, wp, lm, innerT3, v, st)) {
+        t5Keep(ev, c, v);
+      } else {
+        ev.t5CandFlag[c] = 0;
       }
-      __syncthreads();
-      const unsigned int m = sCount < unsigned(kT5DnnTile) ? sCount : unsigned(kT5DnnTile);
-      if (m == 0)
-        continue;  // uniform over the block: no candidate of the tile waits
-      for (unsigned int k = warp; k < m; k += nWarps) {
-        const float score = t5DnnForwardWarp(sW, sSlot[k].feat);
-        if (laneId() == 0)
-          sSlot[k].score = score;
+    }
+    __syncthreads();
+    const unsigned int m = sCount < slice ? sCount : slice;
+    for (unsigned int k = threadIdx.x; k < m; k += blockDim.x) {
+      float feat[38];
+      for (int i = 0; i < 38; ++i)
+        feat[i] = ev.t5DnnFeat[size_t(base + k) * 38 + i];
+      const float inference = t5DnnForward(sW, feat);
+      const T5DnnSlotG& sl = ev.t5DnnSlot[base + k];
+      if (!(inference > wp)) {
+        ev.t5CandFlag[sl.cand] = 0;
+        continue;
       }
-      __syncthreads();
-      for (unsigned int k = threadIdx.x; k < m; k += blockDim.x) {
-        const T5DnnSlot& sl = sSlot[k];
-        const float inference = sl.score;
-        if (!(inference > wp)) {
-          ev.t5CandFlag[sl.cand] = 0;
-          continue;
-        }
-        T5Values v = sl.v;
-        t5NonAnchor(es.m, ev.md, sl.lm, sl.mdIdx, v);
-        v.tightCutFlag = sl.tight != 0 and (inference > wp);
-        t5Keep(ev, sl.cand, v);
-      }
-      __syncthreads();
+      T5Values v = sl.v;
+      t5NonAnchor(es.m, ev.md, sl.lm, sl.mdIdx, v);
+      v.tightCutFlag = sl.tight != 0 and (inference > wp);
+      t5Keep(ev, sl.cand, v);
     }
   }
 

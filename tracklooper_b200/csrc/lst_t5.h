@@ -1228,6 +1228,17 @@ namespace lst {
     bool tightCutFlag;
   };
 
+  // A candidate staged for the classifier pass at the end of kT5Eval's
+  // block (the event's kT5DnnCap slots are split among the blocks).
+  constexpr unsigned int kT5DnnCap = 1u << 14;
+  struct T5DnnSlotG {
+    T5Values v;
+    unsigned int mdIdx[5];
+    unsigned int cand;
+    uint16_t lm[5];
+    uint8_t tight;
+  };
+
   // T5 selection for one (inner T3, outer T3) pair
   // (SDL/Quintuplet.h:2508-2984).  useDnn selects the DNN method
   // (USE_RZCHI2 + USE_T5_DNN) with working point dnnWP (the reference's is
