@@ -24,7 +24,10 @@
 //    point of closest approach to the beam line, and the state at the last seed
 //    hit taken at a nominal inner-tracker radius of 16 cm (or where |z| reaches
 //    30 cm, whichever comes first); a quadruplet with probability 0.75, else a
-//    triplet; a fraction of tracks gets a second seed sharing 3 pixel hits;
+//    triplet; duplicate seeds sharing 3 pixel hits with the first (half of the
+//    seeded tracks, and half of the quadruplets once more) and fake seeds (half
+//    as many as seeded tracks, see generate()) bring a PU200 event to about
+//    1.4e4 pLS after the reference's pLS pT cut;
 //  * noise: extra hits, 1% of the signal hit count, uniformly over OT sensors.
 #include <algorithm>
 #include <cmath>
@@ -643,19 +646,44 @@ namespace {
     }
     ev->nOT = static_cast<uint32_t>(ev->x.size());
 
-    // Pixel seeds.
+    // Pixel seeds.  Every particle above 0.6 GeV inside the pixel acceptance
+    // seeds a pLS from its first 3 or 4 inner-tracker hits.  As pixel seeding
+    // does, a particle is often seeded more than once: a triplet ending one
+    // layer earlier (half of the particles) and, for quadruplets, the outer
+    // triplet (half of them), each sharing three pixel hits with the first
+    // seed.  Fake seeds, hits of different particles that happen to line up,
+    // come in at half the rate of seeded particles: a seeded particle's
+    // direction turned by a few mrad, a pT off by a log-normal factor and a
+    // random charge, on pixel hits of their own, with no particle (-1).
+    // Seeds below the reference's pLS pT cut are dropped by addSeed.
     uint32_t pixHit = 0;
+    std::vector<int> seeded;
     for (int i = 0; i < (int)ev->particles.size(); ++i) {
       auto& p = ev->particles[i];
       if (p.pt < 0.6 || std::fabs(p.eta) > 2.6)
         continue;
+      seeded.push_back(i);
       Helix h(p.pt, p.eta, p.phi, p.vx, p.vy, p.vz, p.q);
       int nHits = r.uniform() < 0.75 ? 4 : 3;
       uint32_t base = pixHit;
       pixHit += 4;
       addSeed(*ev, h, p, i, r, base, nHits, false);
-      if (r.uniform() < 0.3)  // duplicate seed sharing three pixel hits
+      if (r.uniform() < 0.5)  // duplicate: the first three hits, last one a layer earlier
         addSeed(*ev, h, p, i, r, base, 3, true);
+      if (nHits == 4 && r.uniform() < 0.5)  // duplicate: the outer three hits of the quadruplet
+        addSeed(*ev, h, p, i, r, base + 1, 3, false);
+    }
+    size_t nFake = seeded.size() / 2;
+    for (size_t k = 0; k < nFake; ++k) {
+      Particle f = ev->particles[seeded[size_t(r.uniform() * seeded.size()) % seeded.size()]];
+      f.phi += 0.005 * r.normal();
+      f.eta += 0.005 * r.normal();
+      f.pt *= std::exp(0.3 * r.normal());
+      f.q = r.uniform() < 0.5 ? -1.0 : 1.0;
+      Helix h(f.pt, f.eta, f.phi, f.vx, f.vy, f.vz, f.q);
+      uint32_t base = pixHit;
+      pixHit += 4;
+      addSeed(*ev, h, f, -1, r, base, r.uniform() < 0.5 ? 4 : 3, false);
     }
     return ev;
   }
