@@ -527,18 +527,30 @@ namespace lst {
   // One warp per inner lower module walking (connected module, inner MD,
   // outer MD) in order (SDL/Segment.h:798-910).
   constexpr int kLSWarps = 4;
-  __device__ __forceinline__ void lsModule(
-      DeviceES const& es, const EventView& ev, uint16_t lm, unsigned int* pre, uint16_t* outer) {
+  // Per-warp scratch of the walk: the prefix of the candidates over the
+  // connected modules, and per connected module its index, MD count and
+  // first MD, so that a candidate finds its MDs without a global load.
+  struct LSScratch {
+    unsigned int pre[kMaxConnectedModules + 1];
+    unsigned int nOuterMDs[kMaxConnectedModules];
+    unsigned int outerBase[kMaxConnectedModules];
+    uint16_t outer[kMaxConnectedModules];
+  };
+  __device__ __forceinline__ void lsModule(DeviceES const& es, const EventView& ev, uint16_t lm, LSScratch& sc) {
     const unsigned int nInnerMDs = ev.md.nMDs[lm];
     if (nInnerMDs == 0)
       return;
     const Modules& m = es.m;
     const int nConn = m.nConnectedModules[lm];
-    for (int k = laneId(); k < nConn; k += 32)
-      outer[k] = m.moduleMap[lm * kMaxConnectedModules + k];
-    __syncwarp();
-    const unsigned int total =
-        warpPrefix(pre, nConn, [&](int k) { return nInnerMDs * ev.md.nMDs[outer[k]]; });
+    uint16_t* outer = sc.outer;
+    const unsigned int total = warpPrefix(sc.pre, nConn, [&](int k) {
+      const uint16_t o = m.moduleMap[lm * kMaxConnectedModules + k];
+      const unsigned int n = ev.md.nMDs[o];
+      outer[k] = o;
+      sc.nOuterMDs[k] = n;
+      sc.outerBase[k] = static_cast<unsigned int>(es.mdOffset[o]);
+      return nInnerMDs * n;
+    });
     const int cap = es.lsCap[lm];
     const unsigned int base = es.lsOffset[lm];
     const unsigned int innerBase = es.mdOffset[lm];
@@ -551,12 +563,12 @@ namespace lst {
       unsigned int innerMD = 0, outerMD = 0;
       uint16_t outerLM = 0;
       if (f < total) {
-        int k = findSlot(pre, nConn, f);
+        int k = findSlot(sc.pre, nConn, f);
         outerLM = outer[k];
-        unsigned int nOuterMDs = ev.md.nMDs[outerLM];
-        unsigned int local = f - pre[k];
+        unsigned int nOuterMDs = sc.nOuterMDs[k];
+        unsigned int local = f - sc.pre[k];
         innerMD = innerBase + local / nOuterMDs;
-        outerMD = es.mdOffset[outerLM] + local % nOuterMDs;
+        outerMD = sc.outerBase[k] + local % nOuterMDs;
         ok = lsSelect(m, ev.md, lm, outerLM, innerMD, outerMD, v);
       }
       unsigned int tot;
@@ -574,14 +586,13 @@ namespace lst {
   }
 
   __global__ void __launch_bounds__(LST_LB_LS) kCreateLS(DeviceES es, const EventView* evs) {
-    __shared__ unsigned int sPre[kLSWarps][kMaxConnectedModules + 1];
-    __shared__ uint16_t sOuter[kLSWarps][kMaxConnectedModules];
+    __shared__ LSScratch sScratch[kLSWarps];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;  // at most kLSWarps
     for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
       __syncwarp();
-      lsModule(es, ev, static_cast<uint16_t>(w), sPre[wib], sOuter[wib]);
+      lsModule(es, ev, static_cast<uint16_t>(w), sScratch[wib]);
     }
   }
 
@@ -874,9 +885,19 @@ namespace lst {
 
   // One warp per inner-inner lower module walking (inner segment, outer
   // segment of the middle module) in order (SDL/Triplet.h:874-1005).
+  //
+  // The inner segments are taken kT3Chunk at a time.  For each the warp
+  // keeps in shared memory the prefix of its candidates and where its outer
+  // segments are listed (the MD-keyed segment index of the middle module),
+  // so that a candidate reaches its outer segment with one global load.
   constexpr int kT3Warps = 4;
-  constexpr int kT3MaxInner = 1024;
-  __device__ __forceinline__ void t3Module(DeviceES const& es, const EventView& ev, uint16_t lm1, unsigned int* pre) {
+  constexpr int kT3Chunk = 128;
+  struct T3Scratch {
+    unsigned int pre[kT3Chunk + 1];
+    unsigned int listStart[kT3Chunk];  // first entry of the inner segment's outer segments in lsByMD
+    unsigned int outerBase[kT3Chunk];  // first segment of the middle module
+  };
+  __device__ __forceinline__ void t3Module(DeviceES const& es, const EventView& ev, uint16_t lm1, T3Scratch& sc) {
     const Modules& m = es.m;
     if (m.nConnectedModules[lm1] == 0)
       return;
@@ -885,41 +906,48 @@ namespace lst {
       return;
     const unsigned int segBase = es.lsOffset[lm1];
     const Segments& ls = ev.ls;
-    // Only outer segments whose inner MD is the inner segment's outer MD can
-    // pass (the first test of the reference's triplet algorithm); they are
-    // enumerated through the MD-keyed segment index in storage order, so
-    // candidates keep the reference's (inner, outer) order.
-    const unsigned int total = warpPrefix(pre, int(nInner), [&](int i) {
-      uint16_t middle = ls.outerLowerModuleIndices[segBase + i];
-      if (ls.nSegments[middle] == 0)
-        return 0u;
-      return static_cast<unsigned int>(ev.mdLSCount[ls.mdIndices[2 * (segBase + i) + 1]]);
-    });
     const int cap = ev.rg.tripletModuleOccupancy[lm1];
     const unsigned int base = ev.rg.tripletModuleIndices[lm1];
     Triplets t3 = ev.t3;
     unsigned int count = 0;
-    for (unsigned int start = 0; start < total; start += 32) {
-      unsigned int f = start + laneId();
-      bool ok = false;
-      T3Values v;
-      unsigned int innerSeg = 0, outerSeg = 0;
-      uint16_t middle = 0, outerOuter = 0;
-      if (f < total) {
-        int i = findSlot(pre, int(nInner), f);
-        innerSeg = segBase + i;
-        middle = ls.outerLowerModuleIndices[innerSeg];
-        const unsigned int mdMid = ls.mdIndices[2 * innerSeg + 1];
+    for (unsigned int c0 = 0; c0 < nInner; c0 += kT3Chunk) {
+      const int n = int(min(nInner - c0, unsigned(kT3Chunk)));
+      __syncwarp();  // the previous chunk's scratch has been read
+      // Only outer segments whose inner MD is the inner segment's outer MD
+      // can pass (the first test of the reference's triplet algorithm); they
+      // are enumerated through the MD-keyed segment index in storage order,
+      // so candidates keep the reference's (inner, outer) order.
+      const unsigned int total = warpPrefix(sc.pre, n, [&](int i) {
+        const unsigned int seg = segBase + c0 + unsigned(i);
+        const uint16_t middle = ls.outerLowerModuleIndices[seg];
+        if (ls.nSegments[middle] == 0)
+          return 0u;
+        const unsigned int mdMid = ls.mdIndices[2 * seg + 1];
         const unsigned int outerBase = es.lsOffset[middle];
-        outerSeg = outerBase + ev.lsByMD[outerBase + ev.mdLSStart[mdMid] + (f - pre[i])];
-        outerOuter = ls.outerLowerModuleIndices[outerSeg];
-        ok = t3Select(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg, v);
+        sc.outerBase[i] = outerBase;
+        sc.listStart[i] = outerBase + ev.mdLSStart[mdMid];
+        return static_cast<unsigned int>(ev.mdLSCount[mdMid]);
+      });
+      for (unsigned int start = 0; start < total; start += 32) {
+        unsigned int f = start + laneId();
+        bool ok = false;
+        T3Values v;
+        unsigned int innerSeg = 0, outerSeg = 0;
+        uint16_t middle = 0, outerOuter = 0;
+        if (f < total) {
+          int i = findSlot(sc.pre, n, f);
+          innerSeg = segBase + c0 + unsigned(i);
+          middle = ls.outerLowerModuleIndices[innerSeg];
+          outerSeg = sc.outerBase[i] + ev.lsByMD[sc.listStart[i] + (f - sc.pre[i])];
+          outerOuter = ls.outerLowerModuleIndices[outerSeg];
+          ok = t3Select(m, ev.md, ls, lm1, middle, outerOuter, innerSeg, outerSeg, v);
+        }
+        unsigned int tot;
+        unsigned int r = count + warpRank(ok, tot);
+        if (ok && int(r) < cap)
+          storeT3(m, ev.md, ls, t3, innerSeg, outerSeg, lm1, middle, outerOuter, v, base + r);
+        count += tot;
       }
-      unsigned int tot;
-      unsigned int r = count + warpRank(ok, tot);
-      if (ok && int(r) < cap)
-        storeT3(m, ev.md, ls, t3, innerSeg, outerSeg, lm1, middle, outerOuter, v, base + r);
-      count += tot;
     }
     if (laneId() == 0) {
       t3.nTriplets[lm1] = (int(count) < cap) ? count : (cap > 0 ? unsigned(cap) : 0u);
@@ -930,13 +958,13 @@ namespace lst {
   }
 
   __global__ void __launch_bounds__(LST_LB_T3) kCreateT3(DeviceES es, const EventView* evs) {
-    __shared__ unsigned int sPre[kT3Warps][kT3MaxInner + 1];
+    __shared__ T3Scratch sScratch[kT3Warps];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;  // at most kT3Warps
     for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
       __syncwarp();
-      t3Module(es, ev, static_cast<uint16_t>(w), sPre[wib]);
+      t3Module(es, ev, static_cast<uint16_t>(w), sScratch[wib]);
     }
   }
 
