@@ -117,6 +117,15 @@ int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_thre
  * Replaces SDL::loadAndFillESHost + SDL::loadAndFillESDevice
  * (SDL/LSTESData.h:79-80, SDL/LSTESData.cc:79-126). */
 int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out);
+/* lst_es_load with options.  LST_ES_BUILD_ON_DEVICE builds the event setup on
+ * `device` from the files' raw records (module re-indexing, detId hash,
+ * orientations, partners, module and pixel maps, occupancy caps) instead of
+ * on the host; the arrays, and the error messages, are the same.  The host
+ * copy of the event setup (lst_es_host_array) is then read back from the
+ * device. */
+#define LST_ES_BUILD_ON_DEVICE 1u
+int lst_es_load_ex(const char* geometry_dir, const char* t5dnn_weights_path, int device, unsigned int flags,
+                   lst_es** out);
 void lst_es_free(lst_es* es);
 /* Loads the geometry on the host only (no device, no upload): for inspecting
  * the event setup.  Such a handle cannot create event sets. */

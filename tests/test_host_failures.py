@@ -154,3 +154,14 @@ def test_null_arguments_are_errors():
     assert lib.lst_es_load_host(None, ctypes.byref(h)) < 0
     assert lib.lst_es_get_info(None, None) < 0
     assert lib.lst_event_create(None, 1, 1, None, ctypes.byref(h)) < 0
+
+
+def test_es_load_ex_flags():
+    """lst_es_load_ex rejects unknown flags before touching a file or the
+    device; without a usable device the device build reports an error."""
+    lib = lst.library()
+    h = ctypes.c_void_p()
+    assert lib.lst_es_load_ex(geometry.geometry_dir().encode(), None, 0, 0x80, ctypes.byref(h)) < 0
+    assert "unknown flags" in lib.lst_last_error().decode()
+    assert not h.value
+    assert lib.lst_es_load_ex(None, None, 0, lst.ES_BUILD_ON_DEVICE, ctypes.byref(h)) < 0

@@ -28,7 +28,7 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-LIB_SOURCES = ["lst_event.cu", "lst_dnn.cu", "es.cc"]
+LIB_SOURCES = ["lst_event.cu", "lst_dnn.cu", "es.cc", "es_device.cu"]
 LIB_DEPS = ["lst_core.h", "lst_md.h", "lst_ls.h", "lst_t3.h", "lst_t5.h", "lst_pixel.h", "lst_device.h",
             "lst_kernels.cuh", "lst_fields.h", "lst_seed.h", "es.h"]
 

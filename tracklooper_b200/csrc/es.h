@@ -65,4 +65,13 @@ namespace lst {
   // empty string on success, else an error message.
   std::string loadEsHost(const std::string& geometryDir, EsHost& es);
 
+  // The same event setup built by kernels on `device` from the files' raw
+  // records, then copied into `es` (csrc/es_device.cu).  Same arrays, same
+  // error messages.
+  std::string buildEsOnDevice(const std::string& geometryDir, int device, EsHost& es);
+
+  // The pt cut a geometry directory is built for (the number after its
+  // name's last "_pt", 0.8 without one).
+  float geometryPtCut(const std::string& dir);
+
 }  // namespace lst

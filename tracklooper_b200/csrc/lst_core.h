@@ -84,7 +84,7 @@ namespace lst {
   // cut algorithms call them from dozens of sites, and an inlined copy per
   // site multiplies the code the diverging warps of one SM fetch.
 #if defined(__CUDACC__)
-#define LST_HD_MATH __host__ __device__ __noinline__
+#define LST_HD_MATH static __host__ __device__ __noinline__  // one copy per translation unit
 #else
 #define LST_HD_MATH inline
 #endif

@@ -760,26 +760,44 @@ int lst_kernel_attributes(int i, const char** name, int* num_regs, int* max_thre
 }
 
 int lst_es_load(const char* geometry_dir, const char* t5dnn_weights_path, int device, lst_es** out) {
+  return lst_es_load_ex(geometry_dir, t5dnn_weights_path, device, 0u, out);
+}
+
+int lst_es_load_ex(const char* geometry_dir, const char* t5dnn_weights_path, int device, unsigned int flags,
+                   lst_es** out) {
   LST_ABI_TRY
   if (!geometry_dir || !out)
     return setError("lst_es_load: null argument");
   *out = nullptr;
+  if (flags & ~LST_ES_BUILD_ON_DEVICE)
+    return setError("lst_es_load_ex: unknown flags");
   std::unique_ptr<lst_es> es(new (std::nothrow) lst_es());
   if (!es)
     return setError("out of host memory");
   es->device = device;
-  std::string err = lst::loadEsHost(geometry_dir, es->host);
-  if (!err.empty())
-    return setError(err);
-  for (int v : es->host.t5CapIfEligible)
-    if (v >= 0)
-      es->nEligibleMax++;
-  // Every input file is read and checked before the first CUDA call.
+  // Every input file is read and checked before the first CUDA call: the
+  // geometry, then the weights on the host path; the weights, then the
+  // geometry (whose files the device build reads before its first CUDA
+  // call) on the device path.
+  const bool onDevice = (flags & LST_ES_BUILD_ON_DEVICE) != 0;
+  if (!onDevice) {
+    std::string err = lst::loadEsHost(geometry_dir, es->host);
+    if (!err.empty())
+      return setError(err);
+  }
   if (t5dnn_weights_path) {
     int rc = loadWeightsFile(t5dnn_weights_path, es->dnn);
     if (rc)
       return rc;
   }
+  if (onDevice) {
+    std::string err = lst::buildEsOnDevice(geometry_dir, device, es->host);
+    if (!err.empty())
+      return setError(err);
+  }
+  for (int v : es->host.t5CapIfEligible)
+    if (v >= 0)
+      es->nEligibleMax++;
   LST_CUDA(cudaSetDevice(device));
   std::vector<std::pair<void*, const void*>> copies;
   std::vector<size_t> sizes;
@@ -868,6 +886,9 @@ int lst_es_host_array(const lst_es* es, const char* name, const void** data, siz
   LST_ES_ARRAY("pixelmap.", connectedPixelsSizesNeg)
   LST_ES_ARRAY("endcap.", geoMapDetId)
   LST_ES_ARRAY("endcap.", geoMapPhi)
+  LST_ES_ARRAY("endcap.", geoMapIndex)
+  LST_ES_ARRAY("hash.", detHashKey)
+  LST_ES_ARRAY("hash.", detHashVal)
   LST_ES_ARRAY("caps.", mdOffset)
   LST_ES_ARRAY("caps.", mdCap)
   LST_ES_ARRAY("caps.", lsOffset)

@@ -67,12 +67,15 @@ STATUS_BITS = {
     0x40: "invalid input",
 }
 
+ES_BUILD_ON_DEVICE = 1  # LST_ES_BUILD_ON_DEVICE
+
 # Exported symbols of include/lst_b200.h.
 EXPORTS = (
     "lst_last_error",
     "lst_kernel_count",
     "lst_kernel_attributes",
     "lst_es_load",
+    "lst_es_load_ex",
     "lst_es_free",
     "lst_es_load_host",
     "lst_es_host_array",
@@ -269,6 +272,7 @@ def library(path: str = LIB_PATH) -> ctypes.CDLL:
         lib.lst_kernel_attributes.argtypes = [i32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(i32),
                                               ctypes.POINTER(i32), ctypes.POINTER(sz), ctypes.POINTER(sz)]
         lib.lst_es_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, ctypes.POINTER(vp)]
+        lib.lst_es_load_ex.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, u32, ctypes.POINTER(vp)]
         lib.lst_es_free.argtypes = [vp]
         lib.lst_es_free.restype = None
         lib.lst_es_get_info.argtypes = [vp, ctypes.POINTER(EsInfo)]
@@ -381,12 +385,15 @@ def field_dtypes() -> dict:
 class ES:
     """Event setup on one device (SDL::LSTESDeviceData)."""
 
-    def __init__(self, device: int = 0, weights: str | None = DNN_WEIGHTS, geometry_dir: str | None = None):
+    def __init__(self, device: int = 0, weights: str | None = DNN_WEIGHTS, geometry_dir: str | None = None,
+                 build_on_device: bool = False):
+        """build_on_device: build the event setup with kernels on `device`
+        (LST_ES_BUILD_ON_DEVICE) instead of on the host; same arrays."""
         lib = library()
         gdir = geometry_dir or geometry.geometry_dir()
         h = ctypes.c_void_p()
-        _check(lib.lst_es_load(gdir.encode(), weights.encode() if weights else None, device, ctypes.byref(h)),
-               "lst_es_load")
+        _check(lib.lst_es_load_ex(gdir.encode(), weights.encode() if weights else None, device,
+                                  ES_BUILD_ON_DEVICE if build_on_device else 0, ctypes.byref(h)), "lst_es_load")
         self._h = h
         self.device = device
         info = EsInfo()
@@ -396,6 +403,10 @@ class ES:
     @property
     def handle(self):
         return self._h
+
+    def array(self, name: str, dtype) -> np.ndarray:
+        """The host copy of an event-setup array (lst_es_host_array)."""
+        return _es_array(self._h, name, dtype)
 
     def geometry_hash(self) -> int:
         return int(library().lst_es_geometry_hash(self._h))
@@ -430,6 +441,21 @@ class ES:
             pass
 
 
+def _es_array(h, name: str, dtype) -> np.ndarray:
+    """Copy of the event-setup array `name` of handle h (lst_es_host_array)."""
+    lib = library()
+    p, n, esz = ctypes.c_void_p(), ctypes.c_size_t(), ctypes.c_size_t()
+    _check(lib.lst_es_host_array(h, name.encode(), ctypes.byref(p), ctypes.byref(n), ctypes.byref(esz)),
+           f"es array {name}")
+    dt = np.dtype(dtype)
+    if dt.itemsize != esz.value:
+        raise LSTError(f"{name}: element size {esz.value}, asked for {dt}")
+    if n.value == 0:
+        return np.zeros(0, dt)
+    buf = (ctypes.c_char * (n.value * esz.value)).from_address(p.value)
+    return np.frombuffer(buf, dtype=dt).copy()
+
+
 class HostES:
     """Event setup loaded on the host only (lst_es_load_host), for inspection."""
 
@@ -444,17 +470,7 @@ class HostES:
         self.info = {n: (float if n == "ptCut" else int)(getattr(info, n)) for n, _ in EsInfo._fields_}
 
     def array(self, name: str, dtype) -> np.ndarray:
-        lib = library()
-        p, n, esz = ctypes.c_void_p(), ctypes.c_size_t(), ctypes.c_size_t()
-        _check(lib.lst_es_host_array(self._h, name.encode(), ctypes.byref(p), ctypes.byref(n), ctypes.byref(esz)),
-               f"es array {name}")
-        dt = np.dtype(dtype)
-        if dt.itemsize != esz.value:
-            raise LSTError(f"{name}: element size {esz.value}, asked for {dt}")
-        if n.value == 0:
-            return np.zeros(0, dt)
-        buf = (ctypes.c_char * (n.value * esz.value)).from_address(p.value)
-        return np.frombuffer(buf, dtype=dt).copy()
+        return _es_array(self._h, name, dtype)
 
     def close(self):
         if self._h:
