@@ -259,10 +259,27 @@ def run_ours(args, rank, world, local, events):
                  "shapes": {k: list(v) for k, v in eset.launch_shapes().items()},
                  "geometry_hash": f"{es.geometry_hash():016x}"}
     eset.upload_packed(0, blob, offsets)
+    # a second event set with the same resident inputs and launch shapes: the
+    # batched steps go to the two sets in turn, so that one batch's kernels
+    # fill the SMs that the other batch's kernel tails and small stages leave
+    # idle (two batches in flight, on two streams)
+    eset2 = lst.EventSet(es, n_slots=B, max_hits=max_hits)
+    if not eset2.autotune_load(B, tune_cache):
+        raise RuntimeError("the second event set could not load the launch shapes of the first")
+    eset2.upload_packed(0, blob, offsets)
+    sets = (eset, eset2)
+    stream2 = torch.cuda.ExternalStream(eset2.stream(), device=dev)
+    turn = [0]
 
     def batched_step():
         eset.ingest(0, B)
         eset.run_graph(0, B)
+
+    def pipelined_step():
+        s_ = sets[turn[0] % 2]
+        turn[0] += 1
+        s_.ingest(0, B)
+        s_.run_graph(0, B)
 
     def dropin_step():
         for i in range(B):
@@ -278,13 +295,15 @@ def run_ours(args, rank, world, local, events):
         torch.cuda.synchronize()
         if sampler:
             sampler.start()
-        l0 = eset.launches()
+        l0 = eset.launches() + eset2.launches()
         start.record(stream)
+        stream2.wait_stream(stream)  # the second set's work starts after the start mark
         for _ in range(k):
             step()
+        stream.wait_stream(stream2)  # and the stop mark comes after both sets' work
         stop.record(stream)
         stop.synchronize()
-        l1 = eset.launches()
+        l1 = eset.launches() + eset2.launches()
         clocks = sampler.stop() if sampler else None
         torch.cuda.synchronize()
         ms = reduce_max(start.elapsed_time(stop), world, dev)
@@ -293,12 +312,14 @@ def run_ours(args, rank, world, local, events):
     # warm-up
     for _ in range(args.warmup):
         batched_step()
+        pipelined_step()
     for _ in range(max(1, args.warmup // 2)):
         dropin_step()
     torch.cuda.synchronize()
 
     sampler = ClockSampler(local)
-    ms_b, launches_b, clocks = timed(batched_step, args.steps, sampler)
+    ms_b, launches_b, clocks = timed(pipelined_step, args.steps, sampler)
+    ms_b1, _, _ = timed(batched_step, args.steps)  # one set: the steps one after the other
     ms_d, _, _ = timed(dropin_step, max(1, args.steps // 2))
     steps_d = max(1, args.steps // 2)
     # the slots now hold the per-event (drop-in) results: the same lists?
@@ -307,20 +328,46 @@ def run_ours(args, rank, world, local, events):
     dropin_out = (out_hits[:n_h1], out_len[:n_tc1], out_seed[:n_tc1], out_type[:n_tc1], tco, hco)
     same_lists = all(np.array_equal(a, b) for a, b in zip(batched_out, dropin_out))
 
-    # e2e batched: host packed inputs -> device -> stages -> track-candidate output on host
-    # every step copies its inputs in and its outputs back; the next step's
-    # input copy (lst_batch_stage, copy stream) overlaps this step's stages
+    # e2e batched: host packed inputs -> device -> stages -> track-candidate
+    # output on host.  Every step copies its inputs in and its outputs back.
+    # Two event sets take the steps in turn, as a serving loop would: a step's
+    # input copy (lst_batch_stage, on its set's copy stream) and the reading of
+    # the previous step's output (lst_batch_get_output, on the other set's
+    # stream) overlap the stages running on the GPU.
+    def get_output_of(s):
+        lst._check(lib.lst_batch_get_output(s.handle, 0, B, ctypes.byref(outs)), "lst_batch_get_output")
+
     def e2e_run(k):
-        eset.stage(0, blob, offsets)
+        sets[0].stage(0, blob, offsets)
+        prev = None
         for i in range(k):
-            eset.ingest_staged()
-            eset.run_graph(0, B)
+            cur = sets[i % 2]
+            cur.ingest_staged()
+            cur.run_graph(0, B)
             if i + 1 < k:
-                eset.stage(0, blob, offsets)
-            get_output()
+                sets[(i + 1) % 2].stage(0, blob, offsets)
+            if prev is not None:
+                get_output_of(prev)
+            prev = cur
+        get_output_of(prev)
 
     e2e_run(2)
     ms_e, _, _ = timed(lambda: e2e_run(args.steps), 1)
+    mem_bytes = eset.memory_bytes()
+    # the host -> device copy of one step's packed inputs alone, for the e2e
+    # bound (the copies of consecutive steps cannot overlap one another)
+    dev_in = torch.empty(in_bytes, dtype=torch.uint8, device=dev)
+    h2d_ms = []
+    for _ in range(4):
+        a_ = torch.cuda.Event(enable_timing=True)
+        b_ = torch.cuda.Event(enable_timing=True)
+        a_.record()
+        dev_in.copy_(pinned, non_blocking=True)
+        b_.record()
+        b_.synchronize()
+        h2d_ms.append(a_.elapsed_time(b_))
+    del dev_in
+    h2d_gbs = in_bytes / (min(h2d_ms[1:]) * 1e-3) / 1e9
 
     # e2e drop-in: per-event C ABI calls with host arrays, event by event
     ev1 = lst.Event(es, event_set=eset, slot=0)
@@ -434,15 +481,23 @@ def run_ours(args, rank, world, local, events):
     res = {
         "value": value,
         "ms_per_step": ms_b / args.steps,
+        "one_set": {"value": events_all * args.steps / (ms_b1 * 1e-3), "unit": "events/s",
+                    "ms_per_step": ms_b1 / args.steps,
+                    "mode": "one event set, each step's stages after the previous step's"},
+        "pipelining": "two event sets with the same resident inputs take the steps in turn on two streams; "
+                      "ms_per_step is the timed region over the steps",
         "drop_in": {"value": events_all * steps_d / (ms_d * 1e-3), "unit": "events/s",
                     "ms_per_event": ms_d / steps_d / B},
         "batched_over_drop_in": (ms_d / steps_d) / (ms_b / args.steps),
         "batched_equals_drop_in": same_lists,
         "e2e": {"value": events_all * args.steps / (ms_e * 1e-3), "unit": "events/s",
                 "h2d_bytes_per_step": in_bytes + 8 * B, "d2h_bytes_per_step": d2h_bytes,
-                "mode": "batched C ABI from pinned host buffers: each step's packed inputs copied in (lst_batch_stage on the "
-                        "copy stream, overlapping the previous step's stages), lst_batch_ingest_staged, "
-                        "lst_batch_run_graph, lst_batch_get_output"},
+                "mode": "batched C ABI from pinned host buffers, two event sets taking the steps in turn: each "
+                        "step's packed inputs copied in (lst_batch_stage on its set's copy stream), "
+                        "lst_batch_ingest_staged, lst_batch_run_graph, and its output read back "
+                        "(lst_batch_get_output) while the next step's stages run",
+                "h2d_gbs": round(h2d_gbs, 1),
+                "h2d_bound_events_per_s": round(events_all / (in_bytes / (h2d_gbs * 1e9)), 1)},
         "e2e_drop_in": {"value": events_all * n_dropin_e2e / (ms_de * 1e-3), "unit": "events/s",
                         "mode": "per-event C ABI from host arrays (add_hits, add_pixel_segments, stages, output)"},
         "t5_classifier": classifier,
@@ -456,10 +511,11 @@ def run_ours(args, rank, world, local, events):
         "kernels_sum_ms_per_step": round(tot / args.steps, 4),
         "launches_per_step": round(sum(v[0] for v in prof.values()) / args.steps, 1),
         "objects_per_event": {k: round(v / B, 1) for k, v in agg.items() if k != "nLower"},
-        "device_memory_gb": round(eset.memory_bytes() / 1e9, 2),
+        "device_memory_gb": round(2 * mem_bytes / 1e9, 2),
         "autotune": tune_info,
         "l2": f"inputs larger than L2: {in_bytes / 1e6:.0f} MB of packed inputs per step plus the object arenas",
     }
+    eset2.close()
     eset.close()
     es.close()
     return res
