@@ -259,16 +259,18 @@ def run_ours(args, rank, world, local, events):
                  "shapes": {k: list(v) for k, v in eset.launch_shapes().items()},
                  "geometry_hash": f"{es.geometry_hash():016x}"}
     eset.upload_packed(0, blob, offsets)
-    # a second event set with the same resident inputs and launch shapes: the
-    # batched steps go to the two sets in turn, so that one batch's kernels
-    # fill the SMs that the other batch's kernel tails and small stages leave
-    # idle (two batches in flight, on two streams)
-    eset2 = lst.EventSet(es, n_slots=B, max_hits=max_hits)
-    if not eset2.autotune_load(B, tune_cache):
-        raise RuntimeError("the second event set could not load the launch shapes of the first")
-    eset2.upload_packed(0, blob, offsets)
-    sets = (eset, eset2)
-    stream2 = torch.cuda.ExternalStream(eset2.stream(), device=dev)
+    # more event sets with the same resident inputs and launch shapes: the
+    # batched steps go to the sets in turn, so that one batch's kernels fill
+    # the SMs that another batch's kernel tails and small stages leave idle
+    # (args.sets batches in flight, each set on its own stream)
+    sets = [eset]
+    for _ in range(args.sets - 1):
+        e_ = lst.EventSet(es, n_slots=B, max_hits=max_hits)
+        if not e_.autotune_load(B, tune_cache):
+            raise RuntimeError("an added event set could not load the launch shapes of the first")
+        e_.upload_packed(0, blob, offsets)
+        sets.append(e_)
+    streams = [torch.cuda.ExternalStream(e_.stream(), device=dev) for e_ in sets]
     turn = [0]
 
     def batched_step():
@@ -276,7 +278,7 @@ def run_ours(args, rank, world, local, events):
         eset.run_graph(0, B)
 
     def pipelined_step():
-        s_ = sets[turn[0] % 2]
+        s_ = sets[turn[0] % len(sets)]
         turn[0] += 1
         s_.ingest(0, B)
         s_.run_graph(0, B)
@@ -295,15 +297,17 @@ def run_ours(args, rank, world, local, events):
         torch.cuda.synchronize()
         if sampler:
             sampler.start()
-        l0 = eset.launches() + eset2.launches()
+        l0 = sum(e_.launches() for e_ in sets)
         start.record(stream)
-        stream2.wait_stream(stream)  # the second set's work starts after the start mark
+        for st_ in streams[1:]:
+            st_.wait_stream(stream)  # the other sets' work starts after the start mark
         for _ in range(k):
             step()
-        stream.wait_stream(stream2)  # and the stop mark comes after both sets' work
+        for st_ in streams[1:]:
+            stream.wait_stream(st_)  # and the stop mark comes after every set's work
         stop.record(stream)
         stop.synchronize()
-        l1 = eset.launches() + eset2.launches()
+        l1 = sum(e_.launches() for e_ in sets)
         clocks = sampler.stop() if sampler else None
         torch.cuda.synchronize()
         ms = reduce_max(start.elapsed_time(stop), world, dev)
@@ -341,11 +345,11 @@ def run_ours(args, rank, world, local, events):
         sets[0].stage(0, blob, offsets)
         prev = None
         for i in range(k):
-            cur = sets[i % 2]
+            cur = sets[i % len(sets)]
             cur.ingest_staged()
             cur.run_graph(0, B)
             if i + 1 < k:
-                sets[(i + 1) % 2].stage(0, blob, offsets)
+                sets[(i + 1) % len(sets)].stage(0, blob, offsets)
             if prev is not None:
                 get_output_of(prev)
             prev = cur
@@ -484,15 +488,15 @@ def run_ours(args, rank, world, local, events):
         "one_set": {"value": events_all * args.steps / (ms_b1 * 1e-3), "unit": "events/s",
                     "ms_per_step": ms_b1 / args.steps,
                     "mode": "one event set, each step's stages after the previous step's"},
-        "pipelining": "two event sets with the same resident inputs take the steps in turn on two streams; "
-                      "ms_per_step is the timed region over the steps",
+        "pipelining": f"{len(sets)} event sets with the same resident inputs take the steps in turn, each on its "
+                      "own stream; ms_per_step is the timed region over the steps",
         "drop_in": {"value": events_all * steps_d / (ms_d * 1e-3), "unit": "events/s",
                     "ms_per_event": ms_d / steps_d / B},
         "batched_over_drop_in": (ms_d / steps_d) / (ms_b / args.steps),
         "batched_equals_drop_in": same_lists,
         "e2e": {"value": events_all * args.steps / (ms_e * 1e-3), "unit": "events/s",
                 "h2d_bytes_per_step": in_bytes + 8 * B, "d2h_bytes_per_step": d2h_bytes,
-                "mode": "batched C ABI from pinned host buffers, two event sets taking the steps in turn: each "
+                "mode": f"batched C ABI from pinned host buffers, {len(sets)} event sets taking the steps in turn: each "
                         "step's packed inputs copied in (lst_batch_stage on its set's copy stream), "
                         "lst_batch_ingest_staged, lst_batch_run_graph, and its output read back "
                         "(lst_batch_get_output) while the next step's stages run",
@@ -511,11 +515,12 @@ def run_ours(args, rank, world, local, events):
         "kernels_sum_ms_per_step": round(tot / args.steps, 4),
         "launches_per_step": round(sum(v[0] for v in prof.values()) / args.steps, 1),
         "objects_per_event": {k: round(v / B, 1) for k, v in agg.items() if k != "nLower"},
-        "device_memory_gb": round(2 * mem_bytes / 1e9, 2),
+        "device_memory_gb": round(len(sets) * mem_bytes / 1e9, 2),
         "autotune": tune_info,
         "l2": f"inputs larger than L2: {in_bytes / 1e6:.0f} MB of packed inputs per step plus the object arenas",
     }
-    eset2.close()
+    for e_ in sets[1:]:
+        e_.close()
     eset.close()
     es.close()
     return res
@@ -618,6 +623,8 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--sets", type=int, default=2, choices=range(1, 5), metavar="{1..4}",
+                    help="event sets taking the batched steps in turn")
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--cpu-events", type=int, default=0, help="reference CPU sample size (0: 2 per thread)")
     args = ap.parse_args(argv)
@@ -643,7 +650,8 @@ def main(argv=None, runner=None, backend: str = "nccl"):
 
     config = {"workload": f"PU200-shaped events (generator configuration {args.config}), batch of {args.batch} per GPU",
               "events_per_step_per_gpu": args.batch, "geometry": "OT800_IT615_pt0.8",
-              "t5_selection": "reference-weight DNN", "parallelism": f"replicas x{world}"}
+              "t5_selection": "reference-weight DNN", "parallelism": f"replicas x{world}",
+              "event_sets_per_gpu": args.sets}
     base = {"metric": METRIC, "unit": "events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator, PU200-shaped)", "config": config}
