@@ -497,7 +497,10 @@ namespace {
       case LST_STAGE_MINI_DOUBLETS: {
         // modules per warp task: 32 when a launch holds many events, fewer
         // for a few events, so that a single event still fills the GPU
-        const unsigned int mpt = count >= 16 ? 32u : (count >= 4 ? 8u : 4u);
+#ifndef LST_MD_MPT
+#define LST_MD_MPT 32u
+#endif
+        const unsigned int mpt = count >= 16 ? LST_MD_MPT : (count >= 4 ? 8u : 4u);
         LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, mpt), count), tunedThreads(ev, kTuMD), d, v,
                    mpt);
         LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
