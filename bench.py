@@ -284,9 +284,11 @@ def run_ours(args, rank, world, local, events):
         s_.run_graph(0, B)
 
     def dropin_step():
+        # one event per launch sequence: each event's stages replayed as that
+        # event's own CUDA graph
         for i in range(B):
             eset.ingest(i, 1)
-            eset.run(i, 1)
+            eset.run_graph(i, 1)
 
     def timed(step, k, sampler=None):
         start = torch.cuda.Event(enable_timing=True)
@@ -494,7 +496,9 @@ def run_ours(args, rank, world, local, events):
         "pipelining": f"{len(sets)} event sets with the same resident inputs take the steps in turn, each on its "
                       "own stream; ms_per_step is the timed region over the steps",
         "drop_in": {"value": events_all * steps_d / (ms_d * 1e-3), "unit": "events/s",
-                    "ms_per_event": ms_d / steps_d / B},
+                    "ms_per_event": ms_d / steps_d / B,
+                    "mode": "one event per launch sequence (lst_batch_ingest, then lst_batch_run_graph of that "
+                            "event's slot: its stages as one CUDA graph)"},
         "batched_over_drop_in": (ms_d / steps_d) / (ms_b / args.steps),
         "batched_equals_drop_in": same_lists,
         "e2e": {"value": events_all * args.steps / (ms_e * 1e-3), "unit": "events/s",
