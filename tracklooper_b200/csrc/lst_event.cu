@@ -498,7 +498,7 @@ namespace {
         // modules per warp task: 32 when a launch holds many events, fewer
         // for a few events, so that a single event still fills the GPU
 #ifndef LST_MD_MPT
-#define LST_MD_MPT 32u
+#define LST_MD_MPT 16u
 #endif
         const unsigned int mpt = count >= 16 ? LST_MD_MPT : (count >= 4 ? 8u : 4u);
         LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, mpt), count), tunedThreads(ev, kTuMD), d, v,
