@@ -174,6 +174,26 @@ def hbm_peak():
         return HBM_FALLBACK_GBS, "fallback"
 
 
+def committed_issue_slots(kernel: str):
+    """(IPC, fraction of the 4 issue slots per SM, how it was captured) of
+    `kernel` from the committed ncu summary (profiles/issue_slots.txt), or
+    (None, None, None)."""
+    path = os.path.join(ROOT, "profiles", "issue_slots.txt")
+    note = []
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("#"):
+                    note.append(line[1:].strip())
+                    continue
+                parts = line.split()
+                if len(parts) >= 3 and parts[0] == kernel:
+                    return float(parts[1]), float(parts[2]), " ".join(note)
+    except OSError:
+        pass
+    return None, None, None
+
+
 def committed_traffic(kernel: str):
     """(DRAM bytes per launch of `kernel`, how they were captured) from the
     committed ncu summary (profiles/dram_traffic.txt: '# ' comment lines
@@ -479,6 +499,7 @@ def run_ours(args, rank, world, local, events):
         "traffic": committed_traffic(dominant)[0],
         "traffic_source": committed_traffic(dominant)[1],
         "algorithmic_bytes_per_launch": algo,
+        "issue_slots": dict(zip(("ipc", "frac", "source"), committed_issue_slots(dominant))),
         "launch_ms": round(dms / dlaunches, 4),
         "share_of_device_time": round(dms / tot, 4) if tot else None,
     }
