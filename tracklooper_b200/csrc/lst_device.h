@@ -69,7 +69,9 @@ namespace lst {
     unsigned int t5QueueBack;     // quintuplet candidates queued from the back (modules not all barrel)
     unsigned int pixQueue2Count;  // pixel candidates passing the first pixel tracklet as well
     unsigned int t5SortCount;     // quintuplets binned by eta for the cross-module cleaning
-    unsigned int pad[1];
+    unsigned int mdNext;          // next task for kCreateMD's warps
+    unsigned int lsNext;          // next lower module for kCreateLS's warps
+    unsigned int t3Next;          // next lower module for kCreateT3's warps
   };
 
   // All device pointers of one event.

@@ -501,6 +501,7 @@ namespace {
 #define LST_MD_MPT 16u
 #endif
         const unsigned int mpt = count >= 16 ? LST_MD_MPT : (count >= 4 ? 8u : 4u);
+        LST_LAUNCH(lst::kTaskCountersReset, dim3(1, count), 32, v);
         LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, mpt), count), tunedThreads(ev, kTuMD), d, v,
                    mpt);
         LST_LAUNCH(lst::kMDRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
@@ -509,12 +510,14 @@ namespace {
         break;
       }
       case LST_STAGE_SEGMENTS:
+        LST_LAUNCH(lst::kTaskCountersReset, dim3(1, count), 32, v);
         LST_LAUNCH(lst::kCreateLS, tunedWarpGrid(ev, kTuLS, nLower, count), tunedThreads(ev, kTuLS), d, v);
         LST_LAUNCH(lst::kLSRanges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kLSByMD, warpGrid(ceilDiv(nLower, 32), lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
         break;
       case LST_STAGE_TRIPLETS:
         LST_LAUNCH(lst::kT3Offsets, one, 1024, d, v);
+        LST_LAUNCH(lst::kTaskCountersReset, dim3(1, count), 32, v);
         LST_LAUNCH(lst::kCreateT3, tunedWarpGrid(ev, kTuT3, nLower, count), tunedThreads(ev, kTuT3), d, v);
         LST_LAUNCH(lst::kT3Ranges, dim3(blocksFor(nLower, count), count), kThreads, d, v);
         LST_LAUNCH(lst::kT3ByMD, warpGrid(ceilDiv(nLower, 32), lst::kIdxWarps, count), 32 * lst::kIdxWarps, d, v);
@@ -660,6 +663,7 @@ namespace {
         {"kCreateMD", (const void*)lst::kCreateMD},
         {"kMDRanges", (const void*)lst::kMDRanges},
         {"kMDDerived", (const void*)lst::kMDDerived},
+        {"kTaskCountersReset", (const void*)lst::kTaskCountersReset},
         {"kCreateLS", (const void*)lst::kCreateLS},
         {"kLSRanges", (const void*)lst::kLSRanges},
         {"kT3Offsets", (const void*)lst::kT3Offsets},

@@ -327,6 +327,27 @@ namespace lst {
     }
   }
 
+  // Work counters of the kernels whose warps take their next task from the
+  // event's counter (kCreateMD, kCreateLS, kCreateT3), so that a warp that
+  // drew light tasks takes more: the work per module is very uneven.  Zeroed
+  // before each of those kernels runs.
+  __global__ void kTaskCountersReset(const EventView* evs) {
+    if (threadIdx.x == 0) {
+      EventScalars* sc = evs[blockIdx.y].sc;
+      sc->mdNext = 0;
+      sc->lsNext = 0;
+      sc->t3Next = 0;
+    }
+  }
+  // The next task of the calling warp from counter *next (the same value on
+  // every lane).
+  __device__ __forceinline__ unsigned int warpNextTask(unsigned int* next) {
+    unsigned int t = 0;
+    if (laneId() == 0)
+      t = atomicAdd(next, 1u);
+    return __shfl_sync(kFullMask, t, 0);
+  }
+
   // ======================================================== mini-doublets
   // SDL/MiniDoublet.h:896-992: every (lower hit, upper hit) pair of a lower
   // module is a candidate; passing ones are stored in the module's arena at
@@ -455,10 +476,10 @@ namespace lst {
   __global__ void __launch_bounds__(LST_LB_MD) kCreateMD(DeviceES es, const EventView* evs, unsigned int modulesPerTask) {
     __shared__ unsigned int sCount[kMDMaxWarps][32];
     const EventView& ev = evs[blockIdx.y];
-    const int wpb = blockDim.x >> 5;
     const int w = threadIdx.x >> 5;
     const unsigned int nTasks = (es.nLowerModules + modulesPerTask - 1u) / modulesPerTask;
-    for (unsigned int task = blockIdx.x * wpb + w; task < nTasks; task += gridDim.x * wpb)
+    // tasks from the event's counter (kTaskCountersReset zeroes it before)
+    for (unsigned int task = warpNextTask(&ev.sc->mdNext); task < nTasks; task = warpNextTask(&ev.sc->mdNext))
       mdTask(es, ev, task, modulesPerTask, sCount[w]);
   }
 
@@ -589,8 +610,8 @@ namespace lst {
     __shared__ LSScratch sScratch[kLSWarps];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
-    const int wpb = blockDim.x >> 5;  // at most kLSWarps
-    for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
+    // modules from the event's counter (kTaskCountersReset zeroes it before)
+    for (unsigned int w = warpNextTask(&ev.sc->lsNext); w < es.nLowerModules; w = warpNextTask(&ev.sc->lsNext)) {
       __syncwarp();
       lsModule(es, ev, static_cast<uint16_t>(w), sScratch[wib]);
     }
@@ -961,8 +982,8 @@ namespace lst {
     __shared__ T3Scratch sScratch[kT3Warps];
     const EventView& ev = evs[blockIdx.y];
     const int wib = threadIdx.x >> 5;
-    const int wpb = blockDim.x >> 5;  // at most kT3Warps
-    for (int w = blockIdx.x * wpb + wib; w < es.nLowerModules; w += gridDim.x * wpb) {
+    // modules from the event's counter (kTaskCountersReset zeroes it before)
+    for (unsigned int w = warpNextTask(&ev.sc->t3Next); w < es.nLowerModules; w = warpNextTask(&ev.sc->t3Next)) {
       __syncwarp();
       t3Module(es, ev, static_cast<uint16_t>(w), sScratch[wib]);
     }
