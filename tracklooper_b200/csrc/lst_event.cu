@@ -498,7 +498,7 @@ namespace {
         // modules per warp task: 32 when a launch holds many events, fewer
         // for a few events, so that a single event still fills the GPU
 #ifndef LST_MD_MPT
-#define LST_MD_MPT 16u
+#define LST_MD_MPT 8u
 #endif
         const unsigned int mpt = count >= 16 ? LST_MD_MPT : (count >= 4 ? 8u : 4u);
         LST_LAUNCH(lst::kTaskCountersReset, dim3(1, count), 32, v);

@@ -471,7 +471,7 @@ namespace lst {
 #define LST_LB_EVAL 128, LST_LB_EVAL_B
 #define LST_LB_T5EVAL 128, LST_LB_T5EVAL_B
 #define LST_LB_PIXMID 128, LST_LB_PIXMID_B
-  // modulesPerTask (1..32): 16 for batches; fewer for a single event, whose
+  // modulesPerTask (1..32): 8 for batches; fewer for a single event, whose
   // 13 000 lower modules would otherwise make only ~400 warp tasks.
   __global__ void __launch_bounds__(LST_LB_MD) kCreateMD(DeviceES es, const EventView* evs, unsigned int modulesPerTask) {
     __shared__ unsigned int sCount[kMDMaxWarps][32];
