@@ -495,12 +495,12 @@ namespace {
     const dim3 one(1, count);
     switch (stage) {
       case LST_STAGE_MINI_DOUBLETS: {
-        // modules per warp task: 32 when a launch holds many events, fewer
-        // for a few events, so that a single event still fills the GPU
+        // modules per warp task: 8 from 4 events per launch, 4 for fewer, so
+        // that a single event still makes enough tasks to fill the GPU
 #ifndef LST_MD_MPT
 #define LST_MD_MPT 8u
 #endif
-        const unsigned int mpt = count >= 16 ? LST_MD_MPT : (count >= 4 ? 8u : 4u);
+        const unsigned int mpt = count >= 4 ? LST_MD_MPT : 4u;
         LST_LAUNCH(lst::kTaskCountersReset, dim3(1, count), 32, v);
         LST_LAUNCH(lst::kCreateMD, tunedWarpGrid(ev, kTuMD, ceilDiv(nLower, mpt), count), tunedThreads(ev, kTuMD), d, v,
                    mpt);
